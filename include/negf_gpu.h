@@ -1,0 +1,146 @@
+/*
+ * negf_gpu.h -- C ABI of the B200 NEGF engine (libnegfgpu.so).
+ *
+ * Drop-in for the hot path of NEGFtrans: src/negf.f90 (the per-job drivers)
+ * and src/math_kernel.f90 (the RGF solver), called from Fortran through
+ * iso_c_binding or from C/C++/Python directly.
+ *
+ * Conventions
+ *  - Plain C types only.  Complex numbers are interleaved (re, im) doubles,
+ *    the memory layout of Fortran complex*16 and C double _Complex.
+ *  - Arrays are column-major (Fortran order): element (i,j,k) of an
+ *    (N,N,Nz) array is at i + N*j + N*N*k, 0-based.  No copies are needed on
+ *    the Fortran side.
+ *  - Units are the reference's "atomic" units after main.f90:184-205:
+ *    energies and potentials in Hartree, lengths in bohr.
+ *  - Every entry returns an int status: 0 = NEGF_OK, < 0 = an argument or
+ *    CUDA error (never exit()); > 0 = LAPACK-style singular pivot, i.e. a
+ *    block had a zero pivot (the 1-based column), results of that job are not
+ *    trusted.  The reference ignores INFO (math_kernel.f90:31-32); this
+ *    library reports it.
+ *  - Ownership: the caller owns every host buffer; a context owns its device
+ *    buffers.  One context per host thread; different contexts may be used
+ *    concurrently.  Host-pointer entries are synchronous.
+ */
+#ifndef NEGF_GPU_H
+#define NEGF_GPU_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NEGF_OK 0
+#define NEGF_ERR_ARG (-1)
+#define NEGF_ERR_CUDA (-2)
+#define NEGF_ERR_NOMEM (-3)
+#define NEGF_ERR_UNSUPPORTED (-4)
+
+#define NEGF_FP64 0 /* complex128 throughout */
+
+typedef struct negf_ctx negf_ctx;
+
+/* The inputs that main.f90 hands to the negf.f90 job drivers
+ * (V_reciprocal_all, nx_grid, ny_grid, atomic%..., kpoint). */
+typedef struct negf_problem {
+    int32_t N;            /* plane-wave basis size, size(nx_grid)                */
+    int32_t Nz;           /* z slices, size(V_reciprocal_all, 3); must be >= 2   */
+    int32_t ngx, ngy;     /* V_reciprocal_all bounds (-ngx:ngx, -ngy:ngy)        */
+    const int32_t *nx;    /* [N] nx_grid                                         */
+    const int32_t *ny;    /* [N] ny_grid                                         */
+    const double *vhat;   /* complex (2ngx+1)*(2ngy+1)*Nz, V_reciprocal_all      */
+    double Lx, Ly, Lz;    /* atomic%LX, LY, LZ (bohr)                            */
+    double V_L, V_R;      /* atomic%V_L, V_R (Hartree)                           */
+    double eta;           /* atomic%ETA (Hartree)                                */
+    int32_t nk;           /* size(kpoint)                                        */
+    const double *kpt;    /* [nk][3] = kpoint(i)%kx, %ky, %weight                */
+} negf_problem;
+
+typedef struct negf_stats {
+    int32_t n_jobs;        /* (E,k) RGF sweeps run                                */
+    int32_t n_singular;    /* jobs that met a zero pivot                          */
+    int32_t first_bad_job; /* 0-based job index of the first such job, or -1      */
+    int32_t info;          /* LAPACK-style info of that job, 0 if none            */
+    double device_ms;      /* device time of the sweeps (CUDA events)             */
+} negf_stats;
+
+/* ---------------------------------------------------------------- setup
+ * Host-side mirrors of the set-up that main.f90 / grid.f90 do once. */
+
+/* PlaneWaveBasis_construction_findsize, grid.f90:387-408 */
+int negf_basis_size(double encut, double lx, double ly, int32_t *n);
+/* PlaneWaveBasis_construction, grid.f90:410-431; nx, ny have room for n */
+int negf_basis(double encut, double lx, double ly, int32_t n, int32_t *nx, int32_t *ny);
+/* Kpoint_mesh_construction, grid.f90:433-448; out[3*i] = kx, ky, weight */
+int negf_kmesh(int32_t nkx, int32_t nky, double lx, double ly, double *out);
+/* LocalPotential_RealToPlanewave per slice + the truncated copy of
+ * main.f90:239-247: vreal (Nx,Ny,Nz) Hartree -> vhat (2ngx+1,2ngy+1,Nz)
+ * complex, zero where |i|>ngx/2 or |j|>ngy/2 (left uninitialised by the
+ * reference).  Errors if 2*ngx > Nx or 2*ngy > Ny (grid.f90:33-37). */
+int negf_vhat(const double *vreal, int32_t Nx, int32_t Ny, int32_t Nz, int32_t ngx, int32_t ngy,
+              double *vhat);
+
+/* -------------------------------------------------------------- context */
+
+/* Uploads V_reciprocal_all, the basis and the k-points to `device`.
+ * Replaces the per-job Hamiltonian_construction/E_minus_H_construction
+ * inputs of negf.f90:145-150 (blocks are generated on chip). */
+int negf_ctx_create(const negf_problem *prob, int32_t device, negf_ctx **ctx);
+int negf_ctx_destroy(negf_ctx *ctx);
+
+/* ---------------------------------------------------------- kernel level */
+
+/* GreensFunction_tri_solver(G_inv_D, G_Function, DFL), math_kernel.f90:44-165.
+ * D: (N,N,Nz) complex, the scaled E-H blocks with +I couplings.
+ * dfl: any of "D", "F", "L"; diag / first / last receive the diagonal, first
+ * column and last column blocks ((N,N,Nz) complex each; NULL when not
+ * requested; zero-filled like the reference when requested but not in dfl).
+ * The reference's t_gfunc array-of-structs becomes three planes. */
+int negf_tri_solve(negf_ctx *ctx, const double *D, int32_t N, int32_t Nz, const char *dfl,
+                   double *diag, double *first, double *last);
+
+/* ------------------------------------------------------------- job level */
+
+/* Transmission_Coefficient, negf.f90:115-174, for all nE*nk jobs at once
+ * (the job loop of main.f90:384-407).  energies[nE] = Transmission(:)%energy
+ * (Hartree, real; the solve uses E + i*eta).  On return
+ * tau[e] = sum_k weight_k * tau(E_e, k), the reduced Transmission(:)%tau. */
+int negf_transmission(negf_ctx *ctx, const double *energies, int32_t nE, int32_t precision,
+                      double *tau, negf_stats *stats);
+
+/* Same computation on device-resident buffers, enqueued on `stream`
+ * (a cudaStream_t; NULL = legacy default stream), no synchronisation.
+ * d_tau_jobs (optional, [nk*nE], job order of negf.f90:131-133) receives the
+ * unweighted per-job tau; d_info (optional, [nk*nE] int32) the per-job info. */
+int negf_transmission_device(negf_ctx *ctx, const double *d_energies, int32_t nE,
+                             int32_t precision, double *d_tau, double *d_tau_jobs,
+                             int32_t *d_info, void *stream);
+
+/* Equilibrium_Density, negf.f90:9-113, for all (N_circle+N_line)*nk jobs
+ * (main.f90:258-297).  gap = atomic%GAP (Hartree), min_v = minval(V_real)
+ * (Hartree), mu = atomic%MU (Hartree), temperature in K.  dm (N,N,Nz)
+ * complex receives Density_Matrix (overwritten, not accumulated). */
+int negf_density(negf_ctx *ctx, int32_t n_circle, int32_t n_line, double min_v, double mu,
+                 double gap, double temperature, double *dm, negf_stats *stats);
+
+/* Local_Density_Of_State, negf.f90:176-236, summed over k-points for the
+ * energies i_e0 .. i_e0+n_chunk-1 (0-based) of the grid
+ * E_i = e_lo + (e_hi-e_lo)*i/n_e.  ldos receives n_chunk consecutive
+ * (N,N,Nz) complex LDOS_Matrix arrays (overwritten). */
+int negf_ldos_matrix(negf_ctx *ctx, double e_lo, double e_hi, int32_t n_e, int32_t i_e0,
+                     int32_t n_chunk, double *ldos, negf_stats *stats);
+
+/* Greensfunction_PlanewaveToReal, grid.f90:71-135, for Nz_s slices:
+ * g (N,N,Nz_s) complex -> out (Nx,Ny,Nz_s) complex, the unnormalised
+ * real-space diagonal.  Computed by binning G(a,b) on n_a-n_b and one 2-D
+ * DFT per slice instead of the reference's 2*Nx*Ny 2-D FFTs. */
+int negf_ptor(const double *g, const int32_t *nx, const int32_t *ny, int32_t N, int32_t Nz_s,
+              int32_t Nx, int32_t Ny, double *out);
+
+/* Library version string. */
+const char *negf_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

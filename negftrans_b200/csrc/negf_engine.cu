@@ -1,0 +1,806 @@
+// negf_engine.cu -- kernels and C ABI of the FP64 RGF engine (sm_100a).
+//
+// Replaces the per-job drivers of src/negf.f90 and the solver of
+// src/math_kernel.f90.  Three kernels carry the hot path:
+//   k_transmission  F-mode streaming sweep + transmission epilogue, one CTA
+//                   per (E,k) job, O(N^2) state per job (negf.f90:115-174)
+//   k_rgf_slab      sweeps that keep every generator block, for the diagonal
+//                   (density, LDOS) and first/last-column (tri_solve) blocks
+//                   (negf.f90:9-113, 176-236; math_kernel.f90:44-165)
+//   k_accumulate    weighted sum of the diagonal blocks over the jobs of a
+//                   chunk (the accumulation loops of negf.f90:86-111,226-234)
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "negf_gpu.h"
+#include "rgf_device.cuh"
+
+using namespace negf;
+
+namespace {
+
+constexpr double PI = 3.141592653589793;           // global.f90:28
+constexpr double HARTREE = 27.211386245988;        // global.f90:24
+constexpr double K_B = 8.617333262e-5 / HARTREE;   // global.f90:26
+
+struct RgfJob {
+    double e_re, e_im;  // complex energy of the solve, E + i*eta already added
+    double e_t;         // real energy of the transmission weights
+    int ik;             // k-point
+    int pad;
+};
+
+// ------------------------------------------------------------------ kernels
+template <int NB, int RPT>
+__global__ void __launch_bounds__(NT, 1)
+    k_transmission(Geo g, const double *__restrict__ energies, int nE, int njobs, double2 *ws,
+                   size_t wstride, double *tau_jobs, int *info_jobs) {
+    extern __shared__ __align__(256) unsigned char smem[];
+    Smem s = carve<NB>(smem, g.N);
+    const int N = g.N, ld = g.ld, Nz = g.Nz;
+    for (int i = threadIdx.x; i < N; i += NT) { s.nx[i] = g.nx[i]; s.ny[i] = g.ny[i]; }
+    __syncthreads();
+    double2 *A0 = ws + (size_t)blockIdx.x * wstride;
+    double2 *A1 = A0 + (size_t)ld * N;
+    double2 *P0 = A1 + (size_t)ld * N;
+    double2 *P1 = P0 + (size_t)ld * N;
+    for (int job = blockIdx.x; job < njobs; job += gridDim.x) {
+        // job -> (energy, k-point), energy fastest: negf.f90:131-133
+        const int ie = job % nE, ik = job / nE;
+        const double e = energies[ie];
+        const double2 E = make_double2(e, g.eta);
+        job_vectors(g, s, E, e, ik);
+        __syncthreads();
+        double2 *cur = A0, *oth = A1, *P = P0, *Pn = P1;
+        // generator_r(N_z-1) = inv(D_Nz)          math_kernel.f90:82
+        form_block(cur, g, s, Nz - 1, E, ik, nullptr, nullptr);
+        __syncthreads();
+        int info = gj_invert<NB, RPT>(cur, N, ld, s);
+        unpermute(P, ld, cur, ld, N, s, 1.0);
+        __syncthreads();
+        // generator_r(m) = inv(D_{m+1} - generator_r(m+1)), with the running
+        // product P = gR(Nz-1) ... gR(m) of the first-column chain
+        // G_{Nz,1} = (-1)^(Nz-1) gR(Nz-1) ... gR(1) G_11 (math_kernel.f90:83-90,120-128)
+        for (int m = Nz - 3; m >= 0; --m) {
+            form_block(oth, g, s, m + 1, E, ik, cur, nullptr);
+            __syncthreads();
+            const int r = gj_invert<NB, RPT>(oth, N, ld, s);
+            if (r && !info) info = r;
+            GemmArgs ga{Pn, ld, P, ld, s.iprow, oth, ld, s.iprow, N, N, N};
+            cta_gemm(ga, s, GEMM_STORE, g.delta);
+            __syncthreads();
+            double2 *t = cur; cur = oth; oth = t;
+            t = P; P = Pn; Pn = t;
+        }
+        // G_11 = inv(D_1 - generator_r(1))          math_kernel.f90:113-118
+        form_block(oth, g, s, 0, E, ik, cur, nullptr);
+        __syncthreads();
+        const int r = gj_invert<NB, RPT>(oth, N, ld, s);
+        if (r && !info) info = r;
+        // tau = sum_ij gamma_L,i gamma_R,j |2 dz^2 G_{Nz,1}(i,j)|^2   grid.f90:362-383
+        GemmArgs ga{nullptr, 0, P, ld, s.iprow, oth, ld, s.iprow, N, N, N};
+        double t = cta_gemm(ga, s, GEMM_TAU, g.delta);
+        t = block_sum(t, s);
+        if (threadIdx.x == 0) {
+            tau_jobs[job] = t;
+            if (info_jobs) info_jobs[job] = info;
+        }
+        __syncthreads();
+    }
+}
+
+// tau(E) = sum_k w_k tau(E,k)   negf.f90:172
+__global__ void k_tau_reduce(const double *__restrict__ tau_jobs, const double *__restrict__ kw, int nE,
+                             int nk, double *__restrict__ tau) {
+    const int ie = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ie >= nE) return;
+    double t = 0.0;
+    for (int ik = 0; ik < nk; ++ik) t += tau_jobs[(size_t)ik * nE + ie] * kw[ik];
+    tau[ie] = t;
+}
+
+enum { WANT_D = 1, WANT_F = 2, WANT_L = 4 };
+
+// One job per CTA.  slab (Nz blocks, leading dimension ld) first receives
+// the generator_r blocks; with WANT_D it ends up holding G_kk in block k.
+// out_first / out_last (leading dimension N) receive G_k1 / G_kNz.
+template <int NB, int RPT>
+__global__ void __launch_bounds__(NT, 1)
+    k_rgf_slab(Geo g, const RgfJob *__restrict__ jobs, int njobs, const double2 *__restrict__ Dexp,
+               double2 *ws, size_t wstride, double2 *slabs, size_t sstride, int want,
+               double2 *out_first, double2 *out_last, int *info_jobs) {
+    extern __shared__ __align__(256) unsigned char smem[];
+    Smem s = carve<NB>(smem, g.N);
+    const int N = g.N, ld = g.ld, Nz = g.Nz;
+    const size_t NB2 = (size_t)ld * N;  // one workspace block
+    const size_t NN = (size_t)N * N;    // one output block
+    for (int i = threadIdx.x; i < N; i += NT) { s.nx[i] = g.nx[i]; s.ny[i] = g.ny[i]; }
+    __syncthreads();
+    const int job = blockIdx.x;
+    if (job >= njobs) return;
+    double2 *A0 = ws + (size_t)blockIdx.x * wstride;
+    double2 *A1 = A0 + NB2, *T0 = A1 + NB2, *T1 = T0 + NB2, *T2 = T1 + NB2;
+    double2 *slab = slabs + (size_t)blockIdx.x * sstride;
+    const RgfJob jb = jobs[job];
+    const double2 E = make_double2(jb.e_re, jb.e_im);
+    const int ik = jb.ik;
+    if (!Dexp) job_vectors(g, s, E, jb.e_t, ik);
+    __syncthreads();
+    int info = 0, r;
+    double2 *cur = A0, *oth = A1;
+
+    if (want & (WANT_D | WANT_F)) {
+        // generator_r, math_kernel.f90:81-91
+        form_block(cur, g, s, Nz - 1, E, ik, nullptr, Dexp);
+        __syncthreads();
+        info = gj_invert<NB, RPT>(cur, N, ld, s);
+        unpermute(slab + NB2 * (Nz - 2), ld, cur, ld, N, s, 1.0);
+        __syncthreads();
+        for (int m = Nz - 3; m >= 0; --m) {
+            form_block(oth, g, s, m + 1, E, ik, cur, Dexp);
+            __syncthreads();
+            r = gj_invert<NB, RPT>(oth, N, ld, s);
+            if (r && !info) info = r;
+            unpermute(slab + NB2 * m, ld, oth, ld, N, s, 1.0);
+            __syncthreads();
+            double2 *t = cur; cur = oth; oth = t;
+        }
+        form_block(oth, g, s, 0, E, ik, cur, Dexp);
+        __syncthreads();
+        r = gj_invert<NB, RPT>(oth, N, ld, s);
+        if (r && !info) info = r;
+        unpermute(T0, ld, oth, ld, N, s, 1.0);  // T0 = G_11
+        __syncthreads();
+        if ((want & WANT_F) && out_first) {
+            // G_k1 = -gR(k-1) G_{k-1,1}, math_kernel.f90:112-129
+            for (int e = threadIdx.x; e < N * N; e += NT) {
+                const int i = e % N, j = e / N;
+                out_first[e] = T0[i + (size_t)ld * j];
+            }
+            __syncthreads();
+            for (int k = 1; k < Nz; ++k) {
+                GemmArgs ga{out_first + NN * k, N, slab + NB2 * (k - 1), ld, nullptr,
+                            out_first + NN * (k - 1), N, nullptr, N, N, N};
+                cta_gemm(ga, s, GEMM_STORE_NEG, g.delta);
+                __syncthreads();
+            }
+        }
+        if (want & WANT_D) {
+            // G_kk = gR(k-1) (I + G_{k-1,k-1} gR(k-1)), math_kernel.f90:94-109.
+            // Block k-1 of the slab is replaced by G_{k-1,k-1} once gR(k-1)
+            // has been used for the last time.
+            double2 *Gc = T0, *Gn = T2;
+            for (int k = 1; k < Nz; ++k) {
+                double2 *gRk = slab + NB2 * (k - 1);
+                GemmArgs g1{T1, ld, Gc, ld, nullptr, gRk, ld, nullptr, N, N, N};
+                cta_gemm(g1, s, GEMM_STORE_ADD_EYE, g.delta);
+                __syncthreads();
+                GemmArgs g2{Gn, ld, gRk, ld, nullptr, T1, ld, nullptr, N, N, N};
+                cta_gemm(g2, s, GEMM_STORE, g.delta);
+                __syncthreads();
+                for (int e = threadIdx.x; e < N * N; e += NT) {
+                    const int i = e % N, j = e / N;
+                    gRk[i + (size_t)ld * j] = Gc[i + (size_t)ld * j];
+                }
+                __syncthreads();
+                double2 *t = Gc; Gc = Gn; Gn = t;
+            }
+            double2 *last = slab + NB2 * (Nz - 1);
+            for (int e = threadIdx.x; e < N * N; e += NT) {
+                const int i = e % N, j = e / N;
+                last[i + (size_t)ld * j] = Gc[i + (size_t)ld * j];
+            }
+            __syncthreads();
+        }
+    }
+    if ((want & WANT_L) && out_last) {
+        // generator_l and the last column, math_kernel.f90:132-162; the
+        // generator_l blocks reuse slab blocks 0..Nz-2 (D/F are done with it).
+        cur = A0; oth = A1;
+        form_block(cur, g, s, 0, E, ik, nullptr, Dexp);
+        __syncthreads();
+        r = gj_invert<NB, RPT>(cur, N, ld, s);
+        if (r && !info) info = r;
+        unpermute(slab, ld, cur, ld, N, s, 1.0);
+        __syncthreads();
+        for (int m = 1; m <= Nz - 2; ++m) {
+            form_block(oth, g, s, m, E, ik, cur, Dexp);
+            __syncthreads();
+            r = gj_invert<NB, RPT>(oth, N, ld, s);
+            if (r && !info) info = r;
+            unpermute(slab + NB2 * m, ld, oth, ld, N, s, 1.0);
+            __syncthreads();
+            double2 *t = cur; cur = oth; oth = t;
+        }
+        form_block(oth, g, s, Nz - 1, E, ik, cur, Dexp);
+        __syncthreads();
+        r = gj_invert<NB, RPT>(oth, N, ld, s);
+        if (r && !info) info = r;
+        unpermute(out_last + NN * (Nz - 1), N, oth, ld, N, s, 1.0);
+        __syncthreads();
+        for (int k = 1; k < Nz; ++k) {
+            GemmArgs ga{out_last + NN * (Nz - 1 - k), N, slab + NB2 * (Nz - 1 - k), ld, nullptr,
+                        out_last + NN * (Nz - k), N, nullptr, N, N, N};
+            cta_gemm(ga, s, GEMM_STORE_NEG, g.delta);
+            __syncthreads();
+        }
+    }
+    if (threadIdx.x == 0 && info_jobs) info_jobs[job] = info;
+}
+
+// out[o](i,j,k) (+)= sum_{q<gsz} coef[o*gsz+q] * ((slab_{o*gsz+q}(i,j,k) * 2) * dz^2)
+// with out blocks of leading dimension N (negf.f90:78-111, 218-234).
+__global__ void k_accumulate(const double2 *__restrict__ slabs, size_t sstride, int ld, int N, int Nz,
+                             const double2 *__restrict__ coef, int gsz, int nout, double dz,
+                             int accumulate, double2 *__restrict__ out) {
+    const size_t per = (size_t)N * N * Nz;
+    const size_t total = per * nout;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total;
+         e += (size_t)gridDim.x * blockDim.x) {
+        const int o = (int)(e / per);
+        const size_t r = e - (size_t)o * per;
+        const int k = (int)(r / ((size_t)N * N));
+        const int rem = (int)(r - (size_t)k * N * N);
+        const int j = rem / N, i = rem - j * N;
+        const size_t off = i + (size_t)ld * j + (size_t)ld * N * k;
+        double2 acc = accumulate ? out[e] : make_double2(0.0, 0.0);
+        for (int q = 0; q < gsz; ++q) {
+            const int b = o * gsz + q;
+            const double2 gv = slabs[(size_t)b * sstride + off];
+            const double2 gs = make_double2(gv.x * 2.0 * (dz * dz), gv.y * 2.0 * (dz * dz));
+            acc = zfma(coef[b], gs, acc);
+        }
+        out[e] = acc;
+    }
+}
+
+}  // namespace
+
+// ======================================================================= host
+struct negf_ctx {
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int N = 0, Nz = 0, ld = 0, ngx = 0, ngy = 0, nk = 0;
+    double Lx = 0, Ly = 0, Lz = 0, V_L = 0, V_R = 0, eta = 0;
+    std::vector<double> kpt;  // nk x 3
+    double2 *d_vhat = nullptr;
+    int *d_nx = nullptr, *d_ny = nullptr;
+    double *d_ax = nullptr, *d_ay = nullptr, *d_kw = nullptr;
+    // scratch grown on demand
+    void *d_ws = nullptr;
+    size_t ws_bytes = 0;
+    double *d_E = nullptr, *d_tau = nullptr, *d_tau_jobs = nullptr;
+    int *d_info = nullptr;
+    int cap_E = 0, cap_jobs = 0;
+};
+
+namespace {
+
+#define CK(x)                                                                              \
+    do {                                                                                   \
+        cudaError_t e_ = (x);                                                              \
+        if (e_ != cudaSuccess) {                                                           \
+            fprintf(stderr, "negf_gpu: %s failed: %s\n", #x, cudaGetErrorString(e_));      \
+            return NEGF_ERR_CUDA;                                                          \
+        }                                                                                  \
+    } while (0)
+
+Geo make_geo(const negf_ctx *c) {
+    Geo g;
+    g.N = c->N; g.Nz = c->Nz; g.ld = c->ld;
+    g.ngx = c->ngx; g.ngy = c->ngy; g.W = 2 * c->ngx + 1; g.H = 2 * c->ngy + 1;
+    g.nk = c->nk;
+    g.vhat = c->d_vhat; g.nx = c->d_nx; g.ny = c->d_ny;
+    g.ax = c->d_ax; g.ay = c->d_ay; g.kw = c->d_kw;
+    g.delta = c->Lz / c->Nz;
+    g.c2 = 2 * (g.delta * g.delta);
+    g.V_L = c->V_L; g.V_R = c->V_R; g.eta = c->eta;
+    return g;
+}
+
+int ensure_ws(negf_ctx *c, size_t bytes) {
+    if (bytes <= c->ws_bytes) return 0;
+    if (c->d_ws) CK(cudaFree(c->d_ws));
+    c->d_ws = nullptr;
+    c->ws_bytes = 0;
+    if (cudaMalloc(&c->d_ws, bytes) != cudaSuccess) { cudaGetLastError(); return NEGF_ERR_NOMEM; }
+    c->ws_bytes = bytes;
+    return 0;
+}
+
+int ensure_jobs(negf_ctx *c, int nE, int njobs) {
+    if (nE > c->cap_E) {
+        if (c->d_E) CK(cudaFree(c->d_E));
+        if (c->d_tau) CK(cudaFree(c->d_tau));
+        CK(cudaMalloc(&c->d_E, sizeof(double) * nE));
+        CK(cudaMalloc(&c->d_tau, sizeof(double) * nE));
+        c->cap_E = nE;
+    }
+    if (njobs > c->cap_jobs) {
+        if (c->d_tau_jobs) CK(cudaFree(c->d_tau_jobs));
+        if (c->d_info) CK(cudaFree(c->d_info));
+        CK(cudaMalloc(&c->d_tau_jobs, sizeof(double) * njobs));
+        CK(cudaMalloc(&c->d_info, sizeof(int) * njobs));
+        c->cap_jobs = njobs;
+    }
+    return 0;
+}
+
+// Kernel variants by basis size: (panel width NB, rows per thread RPT).
+enum Variant { V32x1 = 0, V16x2 = 1, V8x4 = 2, VNONE = 3 };
+Variant pick_variant(int N) {
+    if (N <= NT) return V32x1;
+    if (N <= 2 * NT) return V16x2;
+    if (N <= 4 * NT) return V8x4;
+    return VNONE;
+}
+size_t variant_smem(Variant v, int N) {
+    switch (v) {
+        case V32x1: return smem_bytes<32>(N);
+        case V16x2: return smem_bytes<16>(N);
+        case V8x4: return smem_bytes<8>(N);
+        default: return 0;
+    }
+}
+
+template <typename K>
+int prep_kernel(K kern, size_t smem) {
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    return 0;
+}
+
+int transmission_launch(negf_ctx *c, const double *d_E, int nE, double *d_tau, double *d_tau_jobs,
+                        int *d_info, cudaStream_t st) {
+    const int njobs = nE * c->nk;
+    const Variant v = pick_variant(c->N);
+    if (v == VNONE) return NEGF_ERR_UNSUPPORTED;
+    const size_t smem = variant_smem(v, c->N);
+    const int grid = std::min(njobs, c->num_sms);
+    const size_t wstride = 4 * (size_t)c->ld * c->N;
+    int rc = ensure_ws(c, sizeof(double2) * wstride * grid);
+    if (rc) return rc;
+    Geo g = make_geo(c);
+    double2 *ws = (double2 *)c->d_ws;
+    switch (v) {
+        case V32x1:
+            if ((rc = prep_kernel(k_transmission<32, 1>, smem))) return rc;
+            k_transmission<32, 1><<<grid, NT, smem, st>>>(g, d_E, nE, njobs, ws, wstride, d_tau_jobs, d_info);
+            break;
+        case V16x2:
+            if ((rc = prep_kernel(k_transmission<16, 2>, smem))) return rc;
+            k_transmission<16, 2><<<grid, NT, smem, st>>>(g, d_E, nE, njobs, ws, wstride, d_tau_jobs, d_info);
+            break;
+        default:
+            if ((rc = prep_kernel(k_transmission<8, 4>, smem))) return rc;
+            k_transmission<8, 4><<<grid, NT, smem, st>>>(g, d_E, nE, njobs, ws, wstride, d_tau_jobs, d_info);
+            break;
+    }
+    CK(cudaGetLastError());
+    k_tau_reduce<<<(nE + 127) / 128, 128, 0, st>>>(d_tau_jobs, c->d_kw, nE, c->nk, d_tau);
+    CK(cudaGetLastError());
+    return 0;
+}
+
+int slab_launch(negf_ctx *c, const Geo &g, const RgfJob *d_jobs, int njobs, const double2 *d_D,
+                double2 *d_slabs, size_t sstride, int want, double2 *d_first, double2 *d_last,
+                int *d_info, cudaStream_t st) {
+    const Variant v = pick_variant(g.N);
+    if (v == VNONE) return NEGF_ERR_UNSUPPORTED;
+    const size_t smem = variant_smem(v, g.N);
+    const size_t wstride = 5 * (size_t)g.ld * g.N;
+    int rc = ensure_ws(c, sizeof(double2) * wstride * njobs);
+    if (rc) return rc;
+    double2 *ws = (double2 *)c->d_ws;
+    switch (v) {
+        case V32x1:
+            if ((rc = prep_kernel(k_rgf_slab<32, 1>, smem))) return rc;
+            k_rgf_slab<32, 1><<<njobs, NT, smem, st>>>(g, d_jobs, njobs, d_D, ws, wstride, d_slabs, sstride,
+                                                        want, d_first, d_last, d_info);
+            break;
+        case V16x2:
+            if ((rc = prep_kernel(k_rgf_slab<16, 2>, smem))) return rc;
+            k_rgf_slab<16, 2><<<njobs, NT, smem, st>>>(g, d_jobs, njobs, d_D, ws, wstride, d_slabs, sstride,
+                                                        want, d_first, d_last, d_info);
+            break;
+        default:
+            if ((rc = prep_kernel(k_rgf_slab<8, 4>, smem))) return rc;
+            k_rgf_slab<8, 4><<<njobs, NT, smem, st>>>(g, d_jobs, njobs, d_D, ws, wstride, d_slabs, sstride,
+                                                       want, d_first, d_last, d_info);
+            break;
+    }
+    CK(cudaGetLastError());
+    return 0;
+}
+
+void fill_stats(negf_stats *st, const std::vector<int> &info, double ms) {
+    if (!st) return;
+    st->n_jobs = (int)info.size();
+    st->n_singular = 0;
+    st->first_bad_job = -1;
+    st->info = 0;
+    for (size_t i = 0; i < info.size(); ++i)
+        if (info[i]) {
+            if (st->first_bad_job < 0) { st->first_bad_job = (int)i; st->info = info[i]; }
+            st->n_singular++;
+        }
+    st->device_ms = ms;
+}
+
+int first_info(const std::vector<int> &info) {
+    for (int v : info)
+        if (v) return v;
+    return 0;
+}
+
+// Jobs that fit in device memory at once for the slab kernel.
+int slab_jobs_in_flight(negf_ctx *c, size_t per_job_bytes, int njobs) {
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    free_b += c->ws_bytes;  // the workspace is re-sized for the chunk
+    const size_t budget = (size_t)(0.8 * (double)free_b);
+    size_t fit = per_job_bytes ? budget / per_job_bytes : (size_t)njobs;
+    int b = (int)std::min<size_t>(fit, (size_t)std::min(njobs, c->num_sms));
+    return std::max(b, 0);
+}
+
+// Runs the D-mode sweeps for `jobs` in chunks and forms the weighted sums of
+// their diagonal blocks, 2 dz^2 G_kk scaled by coef[job]:
+//   gsz == 0: every job sums into out[0] (density; chunks accumulate);
+//   gsz  > 0: jobs [o*gsz, (o+1)*gsz) sum into out[o] (LDOS per energy).
+int diag_accumulate(negf_ctx *c, const std::vector<RgfJob> &jobs, const std::vector<double2> &coef,
+                    int gsz, double2 *d_out, std::vector<int> &info_all, double &ms_total) {
+    const int njobs = (int)jobs.size();
+    const int N = c->N, Nz = c->Nz, ld = c->ld;
+    const size_t sstride = (size_t)ld * N * Nz;
+    const size_t per_job = sizeof(double2) * (sstride + 5 * (size_t)ld * N);
+    int b = slab_jobs_in_flight(c, per_job, njobs);
+    if (gsz > 0) b = (b / gsz) * gsz;
+    if (b < std::max(gsz, 1)) return NEGF_ERR_NOMEM;
+    double2 *d_slabs = nullptr, *d_coef = nullptr;
+    RgfJob *d_jobs = nullptr;
+    int *d_info = nullptr;
+    int rc = 0;
+    if (cudaMalloc(&d_slabs, sizeof(double2) * sstride * b) != cudaSuccess) { cudaGetLastError(); return NEGF_ERR_NOMEM; }
+    if (cudaMalloc(&d_coef, sizeof(double2) * b) != cudaSuccess ||
+        cudaMalloc(&d_jobs, sizeof(RgfJob) * b) != cudaSuccess ||
+        cudaMalloc(&d_info, sizeof(int) * b) != cudaSuccess) {
+        cudaFree(d_slabs); cudaFree(d_coef); cudaFree(d_jobs);
+        return NEGF_ERR_CUDA;
+    }
+    Geo g = make_geo(c);
+    info_all.assign(njobs, 0);
+    ms_total = 0.0;
+    for (int j0 = 0; j0 < njobs && !rc; j0 += b) {
+        const int nb = std::min(b, njobs - j0);
+        const int gs = gsz > 0 ? gsz : nb;
+        const int nout = nb / gs;
+        const int o0 = gsz > 0 ? j0 / gsz : 0;
+        const int acc = gsz > 0 ? 0 : (j0 > 0);
+        if (cudaMemcpyAsync(d_jobs, jobs.data() + j0, sizeof(RgfJob) * nb, cudaMemcpyHostToDevice, c->stream) ||
+            cudaMemcpyAsync(d_coef, coef.data() + j0, sizeof(double2) * nb, cudaMemcpyHostToDevice, c->stream) ||
+            cudaEventRecord(c->ev0, c->stream)) { rc = NEGF_ERR_CUDA; break; }
+        rc = slab_launch(c, g, d_jobs, nb, nullptr, d_slabs, sstride, WANT_D, nullptr, nullptr, d_info, c->stream);
+        if (rc) break;
+        const size_t tot = (size_t)N * N * Nz * nout;
+        const int blocks = (int)std::min<size_t>((tot + 255) / 256, (size_t)c->num_sms * 8);
+        k_accumulate<<<blocks, 256, 0, c->stream>>>(d_slabs, sstride, ld, N, Nz, d_coef, gs, nout,
+                                                    c->Lz / Nz, acc, d_out + (size_t)o0 * N * N * Nz);
+        float ms = 0.f;
+        if (cudaGetLastError() || cudaEventRecord(c->ev1, c->stream) ||
+            cudaMemcpyAsync(info_all.data() + j0, d_info, sizeof(int) * nb, cudaMemcpyDeviceToHost, c->stream) ||
+            cudaStreamSynchronize(c->stream) || cudaEventElapsedTime(&ms, c->ev0, c->ev1)) {
+            rc = NEGF_ERR_CUDA;
+            break;
+        }
+        ms_total += ms;
+    }
+    cudaFree(d_slabs);
+    cudaFree(d_coef);
+    cudaFree(d_jobs);
+    cudaFree(d_info);
+    return rc;
+}
+
+int check_problem(const negf_problem *p) {
+    if (!p || p->N < 1 || p->Nz < 2 || p->ngx < 0 || p->ngy < 0 || !p->nx || !p->ny || !p->vhat ||
+        p->nk < 1 || !p->kpt || !(p->Lx > 0) || !(p->Ly > 0) || !(p->Lz > 0))
+        return NEGF_ERR_ARG;
+    for (int i = 0; i < p->N; ++i)
+        for (int j = 0; j < p->N; ++j) {
+            const int dx = p->nx[i] - p->nx[j], dy = p->ny[i] - p->ny[j];
+            if (dx < -p->ngx || dx > p->ngx || dy < -p->ngy || dy > p->ngy) return NEGF_ERR_ARG;
+        }
+    if (pick_variant(p->N) == VNONE) return NEGF_ERR_UNSUPPORTED;
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *negf_version(void) { return "negftrans_b200 0.1 (sm_100a, FP64 RGF)"; }
+
+int negf_ctx_create(const negf_problem *p, int32_t device, negf_ctx **out) {
+    if (!out) return NEGF_ERR_ARG;
+    *out = nullptr;
+    int rc = check_problem(p);
+    if (rc) return rc;
+    negf_ctx *c = new negf_ctx();
+    c->device = device;
+    if (cudaSetDevice(device) != cudaSuccess) { delete c; return NEGF_ERR_CUDA; }
+    cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+    c->N = p->N; c->Nz = p->Nz; c->ld = round_up(p->N, 8);
+    c->ngx = p->ngx; c->ngy = p->ngy; c->nk = p->nk;
+    c->Lx = p->Lx; c->Ly = p->Ly; c->Lz = p->Lz;
+    c->V_L = p->V_L; c->V_R = p->V_R; c->eta = p->eta;
+    c->kpt.assign(p->kpt, p->kpt + 3 * (size_t)p->nk);
+    const size_t nv = (size_t)(2 * p->ngx + 1) * (2 * p->ngy + 1) * p->Nz;
+    std::vector<double> ax((size_t)p->nk * p->N), ay((size_t)p->nk * p->N), kw(p->nk);
+    for (int k = 0; k < p->nk; ++k) {
+        kw[k] = p->kpt[3 * k + 2];
+        for (int i = 0; i < p->N; ++i) {
+            // (2 * nx_grid(i) * pi / Lx + kx), grid.f90:258
+            ax[(size_t)k * p->N + i] = (double)(2 * p->nx[i]) * PI / p->Lx + p->kpt[3 * k];
+            ay[(size_t)k * p->N + i] = (double)(2 * p->ny[i]) * PI / p->Ly + p->kpt[3 * k + 1];
+        }
+    }
+#define CKC(x) do { if ((x) != cudaSuccess) { negf_ctx_destroy(c); return NEGF_ERR_CUDA; } } while (0)
+    CKC(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    CKC(cudaEventCreate(&c->ev0));
+    CKC(cudaEventCreate(&c->ev1));
+    CKC(cudaMalloc(&c->d_vhat, sizeof(double2) * nv));
+    CKC(cudaMalloc(&c->d_nx, sizeof(int) * p->N));
+    CKC(cudaMalloc(&c->d_ny, sizeof(int) * p->N));
+    CKC(cudaMalloc(&c->d_ax, sizeof(double) * ax.size()));
+    CKC(cudaMalloc(&c->d_ay, sizeof(double) * ay.size()));
+    CKC(cudaMalloc(&c->d_kw, sizeof(double) * kw.size()));
+    CKC(cudaMemcpy(c->d_vhat, p->vhat, sizeof(double2) * nv, cudaMemcpyHostToDevice));
+    CKC(cudaMemcpy(c->d_nx, p->nx, sizeof(int) * p->N, cudaMemcpyHostToDevice));
+    CKC(cudaMemcpy(c->d_ny, p->ny, sizeof(int) * p->N, cudaMemcpyHostToDevice));
+    CKC(cudaMemcpy(c->d_ax, ax.data(), sizeof(double) * ax.size(), cudaMemcpyHostToDevice));
+    CKC(cudaMemcpy(c->d_ay, ay.data(), sizeof(double) * ay.size(), cudaMemcpyHostToDevice));
+    CKC(cudaMemcpy(c->d_kw, kw.data(), sizeof(double) * kw.size(), cudaMemcpyHostToDevice));
+#undef CKC
+    *out = c;
+    return NEGF_OK;
+}
+
+int negf_ctx_destroy(negf_ctx *c) {
+    if (!c) return NEGF_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    cudaFree(c->d_vhat); cudaFree(c->d_nx); cudaFree(c->d_ny);
+    cudaFree(c->d_ax); cudaFree(c->d_ay); cudaFree(c->d_kw);
+    cudaFree(c->d_ws); cudaFree(c->d_E); cudaFree(c->d_tau); cudaFree(c->d_tau_jobs); cudaFree(c->d_info);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return NEGF_OK;
+}
+
+int negf_transmission_device(negf_ctx *c, const double *d_energies, int32_t nE, int32_t precision,
+                             double *d_tau, double *d_tau_jobs, int32_t *d_info, void *stream) {
+    if (!c || !d_energies || !d_tau || nE < 1) return NEGF_ERR_ARG;
+    if (precision != NEGF_FP64) return NEGF_ERR_UNSUPPORTED;
+    if (cudaSetDevice(c->device) != cudaSuccess) return NEGF_ERR_CUDA;
+    const int njobs = nE * c->nk;
+    int rc = ensure_jobs(c, 1, njobs);
+    if (rc) return rc;
+    double *tj = d_tau_jobs ? d_tau_jobs : c->d_tau_jobs;
+    return transmission_launch(c, d_energies, nE, d_tau, tj, d_info, (cudaStream_t)stream);
+}
+
+int negf_transmission(negf_ctx *c, const double *energies, int32_t nE, int32_t precision, double *tau,
+                      negf_stats *stats) {
+    if (!c || !energies || !tau || nE < 1) return NEGF_ERR_ARG;
+    if (precision != NEGF_FP64) return NEGF_ERR_UNSUPPORTED;
+    if (cudaSetDevice(c->device) != cudaSuccess) return NEGF_ERR_CUDA;
+    const int njobs = nE * c->nk;
+    int rc = ensure_jobs(c, nE, njobs);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(c->d_E, energies, sizeof(double) * nE, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaEventRecord(c->ev0, c->stream));
+    rc = transmission_launch(c, c->d_E, nE, c->d_tau, c->d_tau_jobs, c->d_info, c->stream);
+    if (rc) return rc;
+    CK(cudaEventRecord(c->ev1, c->stream));
+    std::vector<int> info(njobs);
+    CK(cudaMemcpyAsync(tau, c->d_tau, sizeof(double) * nE, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(info.data(), c->d_info, sizeof(int) * njobs, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    fill_stats(stats, info, ms);
+    return first_info(info);
+}
+
+int negf_density(negf_ctx *c, int32_t n_circle, int32_t n_line, double min_v, double mu, double gap,
+                 double temperature, double *dm, negf_stats *stats) {
+    if (!c || !dm || n_circle < 2 || n_line < 2) return NEGF_ERR_ARG;
+    if (cudaSetDevice(c->device) != cudaSuccess) return NEGF_ERR_CUDA;
+    // contour of negf.f90:37-65 and weights of negf.f90:86-111
+    const double circle_L = min_v - 1.0 / HARTREE, circle_R = mu - gap;
+    const double line_L = mu - gap, line_R = mu + gap;
+    const double E_c = (circle_R + circle_L) / 2, E_R = (circle_R - circle_L) / 2;
+    const int n_int = n_circle + n_line, njobs = n_int * c->nk;
+    auto simpson_c = [](int i, int n, double a, double b) {  // math_kernel.f90:167-204
+        double cf;
+        if (n % 2 == 1) {
+            cf = (i == 1 || i == n) ? 1.0 / 3 : (i % 2 == 0 ? 4.0 / 3 : 2.0 / 3);
+        } else if (i == 1) cf = 1.0 / 3;
+        else if (i == n - 3) cf = 1.0 / 3 + 1.0 * 3 / 8;
+        else if (i == n - 2 || i == n - 1) cf = 3.0 * 3 / 8;
+        else if (i == n) cf = 1.0 * 3 / 8;
+        else cf = (i % 2 == 0) ? 4.0 / 3 : 2.0 / 3;
+        return cf * (b - a) / (n - 1);
+    };
+    auto simpson_x = [](int i, int n, double a, double b) { return (i - 1) * (b - a) / (n - 1) + a; };
+    std::vector<RgfJob> jobs(njobs);
+    std::vector<double2> coef(njobs);
+    for (int job = 0; job < njobs; ++job) {
+        const int i_int = 1 + job % n_int, ik = job / n_int;
+        const double w = c->kpt[3 * ik + 2];
+        RgfJob jb{};
+        jb.ik = ik;
+        double2 cf;
+        if (i_int <= n_circle) {
+            const double th = simpson_x(i_int, n_circle, 0.0, PI);
+            const double ex = E_c + E_R * std::cos(th), ey = E_R * std::sin(th);
+            jb.e_re = ex; jb.e_im = ey + c->eta; jb.e_t = ex;
+            // w * 2/pi * c_i * i * E_R * exp(i theta)
+            const double s = w * 2.0 / PI * simpson_c(i_int, n_circle, 0.0, PI);
+            const double re = 0.0, im = s;  // s * i
+            const double re2 = re * E_R, im2 = im * E_R;
+            cf.x = re2 * std::cos(th) - im2 * std::sin(th);
+            cf.y = re2 * std::sin(th) + im2 * std::cos(th);
+        } else {
+            const double ex = simpson_x(i_int - n_circle, n_line, line_L, line_R);
+            jb.e_re = ex; jb.e_im = c->eta; jb.e_t = ex;
+            const double f = 1.0 / (std::exp((ex - mu) / (K_B * temperature)) + 1);
+            cf.x = -(w * 2.0 / PI * simpson_c(i_int - n_circle, n_line, line_L, line_R) * f);
+            cf.y = 0.0;
+        }
+        jobs[job] = jb;
+        coef[job] = cf;
+    }
+    const size_t per = (size_t)c->N * c->N * c->Nz;
+    double2 *d_out = nullptr;
+    if (cudaMalloc(&d_out, sizeof(double2) * per) != cudaSuccess) { cudaGetLastError(); return NEGF_ERR_NOMEM; }
+    std::vector<int> info;
+    double ms = 0;
+    int rc = diag_accumulate(c, jobs, coef, 0, d_out, info, ms);
+    if (!rc) {
+        cudaError_t e = cudaMemcpy(dm, d_out, sizeof(double2) * per, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) rc = NEGF_ERR_CUDA;
+    }
+    cudaFree(d_out);
+    if (rc) return rc;
+    fill_stats(stats, info, ms);
+    return first_info(info);
+}
+
+int negf_ldos_matrix(negf_ctx *c, double e_lo, double e_hi, int32_t n_e, int32_t i_e0, int32_t n_chunk,
+                     double *ldos, negf_stats *stats) {
+    if (!c || !ldos || n_e < 1 || i_e0 < 0 || n_chunk < 1 || i_e0 + n_chunk > n_e) return NEGF_ERR_ARG;
+    if (cudaSetDevice(c->device) != cudaSuccess) return NEGF_ERR_CUDA;
+    const int nk = c->nk, njobs = n_chunk * nk;
+    std::vector<RgfJob> jobs(njobs);
+    std::vector<double2> coef(njobs);
+    for (int o = 0; o < n_chunk; ++o) {
+        // LDOS energy grid, negf.f90:203-204 (last point excluded)
+        const int i_energy = i_e0 + o + 1;
+        const double e = e_lo + (e_hi - e_lo) * (i_energy - 1) / n_e;
+        for (int ik = 0; ik < nk; ++ik) {
+            RgfJob jb{};
+            jb.e_re = e; jb.e_im = c->eta; jb.e_t = e; jb.ik = ik;
+            jobs[o * nk + ik] = jb;
+            coef[o * nk + ik] = make_double2(-(c->kpt[3 * ik + 2] * 1.0 / PI), 0.0);  // negf.f90:230-231
+        }
+    }
+    const size_t per = (size_t)c->N * c->N * c->Nz;
+    double2 *d_out = nullptr;
+    if (cudaMalloc(&d_out, sizeof(double2) * per * n_chunk) != cudaSuccess) { cudaGetLastError(); return NEGF_ERR_NOMEM; }
+    std::vector<int> info;
+    double ms = 0;
+    int rc = diag_accumulate(c, jobs, coef, nk, d_out, info, ms);
+    if (!rc && cudaMemcpy(ldos, d_out, sizeof(double2) * per * n_chunk, cudaMemcpyDeviceToHost) != cudaSuccess)
+        rc = NEGF_ERR_CUDA;
+    cudaFree(d_out);
+    if (rc) return rc;
+    fill_stats(stats, info, ms);
+    return first_info(info);
+}
+
+int negf_tri_solve(negf_ctx *ctx, const double *D, int32_t N, int32_t Nz, const char *dfl, double *diag,
+                   double *first, double *last) {
+    if (!D || N < 1 || Nz < 2 || !dfl) return NEGF_ERR_ARG;
+    if (pick_variant(N) == VNONE) return NEGF_ERR_UNSUPPORTED;
+    const int dev = ctx ? ctx->device : 0;
+    if (cudaSetDevice(dev) != cudaSuccess) return NEGF_ERR_CUDA;
+    int want = 0;
+    if (strpbrk(dfl, "Dd")) want |= WANT_D;
+    if (strpbrk(dfl, "Ff")) want |= WANT_F;
+    if (strpbrk(dfl, "Ll")) want |= WANT_L;
+    const size_t per = (size_t)N * N * Nz;
+    const size_t bytes = sizeof(double2) * per;
+    // the reference zero-fills every plane (math_kernel.f90:75-77)
+    if (diag) memset(diag, 0, bytes);
+    if (first) memset(first, 0, bytes);
+    if (last) memset(last, 0, bytes);
+    negf_ctx local;
+    negf_ctx *c = &local;
+    c->device = dev;
+    cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, dev);
+    Geo g{};
+    g.N = N; g.Nz = Nz; g.ld = round_up(N, 8);
+    g.delta = 1.0; g.c2 = 1.0;
+    double2 *d_D = nullptr, *d_slab = nullptr, *d_first = nullptr, *d_last = nullptr;
+    int *d_nx = nullptr, *d_ny = nullptr, *d_info = nullptr;
+    int rc = 0, hinfo = 0;
+    const size_t sstride = (size_t)g.ld * N * Nz;
+    cudaStream_t st = nullptr;
+#define CKT(x) do { if ((x) != cudaSuccess) { rc = NEGF_ERR_CUDA; goto done; } } while (0)
+    CKT(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    CKT(cudaMalloc(&d_D, bytes));
+    CKT(cudaMalloc(&d_slab, sizeof(double2) * sstride));
+    CKT(cudaMalloc(&d_nx, sizeof(int) * N));
+    CKT(cudaMalloc(&d_ny, sizeof(int) * N));
+    CKT(cudaMalloc(&d_info, sizeof(int)));
+    CKT(cudaMemset(d_nx, 0, sizeof(int) * N));
+    CKT(cudaMemset(d_ny, 0, sizeof(int) * N));
+    if ((want & WANT_F) && first) CKT(cudaMalloc(&d_first, bytes));
+    if ((want & WANT_L) && last) CKT(cudaMalloc(&d_last, bytes));
+    CKT(cudaMemcpy(d_D, D, bytes, cudaMemcpyHostToDevice));
+    g.nx = d_nx; g.ny = d_ny;
+    {
+        RgfJob jb{};
+        RgfJob *d_job = nullptr;
+        int i2 = 0;
+        CKT(cudaMalloc(&d_job, sizeof(RgfJob)));
+        CKT(cudaMemcpy(d_job, &jb, sizeof(RgfJob), cudaMemcpyHostToDevice));
+        // pass 1: generator_r sweep, diagonal and first-column blocks
+        int w = want & (WANT_D | WANT_F);
+        if (!diag) w &= ~WANT_D;
+        if (!first) w &= ~WANT_F;
+        if (w) {
+            rc = slab_launch(c, g, d_job, 1, d_D, d_slab, sstride, w, d_first, nullptr, d_info, st);
+            if (!rc && (cudaStreamSynchronize(st) != cudaSuccess ||
+                        cudaMemcpy(&hinfo, d_info, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess))
+                rc = NEGF_ERR_CUDA;
+            if (!rc && (w & WANT_D) &&
+                cudaMemcpy2D(diag, sizeof(double2) * N, d_slab, sizeof(double2) * g.ld, sizeof(double2) * N,
+                             (size_t)N * Nz, cudaMemcpyDeviceToHost) != cudaSuccess)
+                rc = NEGF_ERR_CUDA;
+        }
+        // pass 2: generator_l sweep and last-column blocks (reuses the slab)
+        if (!rc && (want & WANT_L) && last) {
+            rc = slab_launch(c, g, d_job, 1, d_D, d_slab, sstride, WANT_L, nullptr, d_last, d_info, st);
+            if (!rc && (cudaStreamSynchronize(st) != cudaSuccess ||
+                        cudaMemcpy(&i2, d_info, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess))
+                rc = NEGF_ERR_CUDA;
+            if (!hinfo) hinfo = i2;
+        }
+        cudaFree(d_job);
+        if (rc) goto done;
+    }
+    if (d_first) CKT(cudaMemcpy(first, d_first, bytes, cudaMemcpyDeviceToHost));
+    if (d_last) CKT(cudaMemcpy(last, d_last, bytes, cudaMemcpyDeviceToHost));
+#undef CKT
+done:
+    cudaFree(d_D); cudaFree(d_slab); cudaFree(d_first); cudaFree(d_last);
+    cudaFree(d_nx); cudaFree(d_ny); cudaFree(d_info);
+    cudaFree(c->d_ws);
+    c->d_ws = nullptr;
+    if (st) cudaStreamDestroy(st);
+    if (rc) return rc;
+    return hinfo;
+}
+
+}  // extern "C"

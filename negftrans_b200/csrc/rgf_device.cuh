@@ -1,0 +1,544 @@
+// rgf_device.cuh -- CTA-level building blocks of the FP64 recursive Green's
+// function (RGF) engine for sm_100a.
+//
+// One CTA owns one (E,k) job at a time and runs its whole z sweep
+// (math_kernel.f90:44-165) without leaving the kernel.  Blocks are never read
+// from HBM: D_k = 2*dz^2*((E+i*eta)I - H_k) - 2I (grid.f90:236-333) is
+// generated from the V(G-G') table while the previous inverse is subtracted.
+// Inverses use a blocked Gauss-Jordan elimination with implicit partial
+// pivoting (the pivot choice of LAPACK zgetf2: largest |re|+|im| among the
+// rows not yet used), whose panel lives in registers; the rank-NB trailing
+// update and the chain products are complex FP64 GEMMs tiled through shared
+// memory.  The raw Gauss-Jordan result R satisfies
+//     inv(M)(r, c) = R(prow[r], iprow[c])
+// so consumers read it through two index gathers instead of permuting it.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace negf {
+
+constexpr int NT = 256;          // threads per CTA
+constexpr int NWARP = NT / 32;
+constexpr int TM = 64;           // GEMM tile rows
+constexpr int TN = 64;           // GEMM tile columns
+constexpr int TK = 16;           // GEMM k chunk
+
+// ------------------------------------------------------------ complex FP64
+__device__ __forceinline__ double2 zmake(double x, double y) { return make_double2(x, y); }
+__device__ __forceinline__ double2 zadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 zsub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 zmul(double2 a, double2 b) {
+    return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+// c + a*b
+__device__ __forceinline__ double2 zfma(double2 a, double2 b, double2 c) {
+    c.x = fma(a.x, b.x, c.x);
+    c.x = fma(-a.y, b.y, c.x);
+    c.y = fma(a.x, b.y, c.y);
+    c.y = fma(a.y, b.x, c.y);
+    return c;
+}
+// c - a*b
+__device__ __forceinline__ double2 zfms(double2 a, double2 b, double2 c) {
+    c.x = fma(-a.x, b.x, c.x);
+    c.x = fma(a.y, b.y, c.x);
+    c.y = fma(-a.x, b.y, c.y);
+    c.y = fma(-a.y, b.x, c.y);
+    return c;
+}
+// 1/a with the ratio scaling of Smith's algorithm (no overflow of |a|^2).
+__device__ __forceinline__ double2 zrcp(double2 a) {
+    if (fabs(a.x) >= fabs(a.y)) {
+        double r = a.y / a.x, den = a.x + a.y * r;
+        return make_double2(1.0 / den, -r / den);
+    }
+    double r = a.x / a.y, den = a.x * r + a.y;
+    return make_double2(r / den, -1.0 / den);
+}
+__device__ __forceinline__ double cabs1(double2 a) { return fabs(a.x) + fabs(a.y); }
+
+// Principal square root, Re >= 0, branch cut on the negative real axis
+// (the Fortran intrinsic sqrt of complex*16 used at grid.f90:285-288).
+__device__ __forceinline__ double2 zsqrt(double2 z) {
+    if (z.x == 0.0 && z.y == 0.0) return make_double2(0.0, z.y);
+    double t = sqrt(0.5 * (fabs(z.x) + hypot(z.x, z.y)));
+    if (z.x >= 0.0) return make_double2(t, z.y / (2.0 * t));
+    return make_double2(fabs(z.y) / (2.0 * t), copysign(t, z.y));
+}
+// exp(i*q*delta), grid.f90:325,330
+__device__ __forceinline__ double2 self_energy(double2 q, double delta) {
+    double s, c;
+    sincos(q.x * delta, &s, &c);
+    double m = exp(-q.y * delta);
+    return make_double2(m * c, m * s);
+}
+
+// ------------------------------------------------------------ cp.async
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool valid) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    int n = valid ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// ------------------------------------------------------------ geometry
+// Everything a CTA needs to generate D_k for any (E, k-point) job.
+struct Geo {
+    int N, Nz, ld;          // basis size, slices, leading dimension of workspace blocks
+    int ngx, ngy, W, H;     // V table bounds, W = 2ngx+1, H = 2ngy+1
+    int nk;
+    const double2 *vhat;    // [Nz][H][W]  V_reciprocal_all, zero outside |i|<=ngx/2,|j|<=ngy/2
+    const int *nx, *ny;     // [N]
+    const double *ax, *ay;  // [nk][N]  2*pi*n/L + k  (grid.f90:258,285)
+    const double *kw;       // [nk]     k-point weights
+    double delta;           // Lz / Nz
+    double c2;              // 2*delta**2 (grid.f90:311)
+    double V_L, V_R, eta;
+};
+
+struct Red {
+    double v;
+    int idx;
+    int pad;
+    double2 val;
+};
+
+// Shared memory carve-up (dynamic).
+struct Smem {
+    int *prow;      // [N] pivot row of column k
+    int *iprow;     // [N] inverse permutation
+    int *nx, *ny;   // [N]
+    int *inP;       // [N] 1 if row is a pivot row of the current panel
+    double2 *sigL;  // [N] exp(i q_L dz)
+    double2 *sigR;  // [N] exp(i q_R dz)
+    double *gL;     // [N] gamma_L  sin(q dz)/dz^2 (grid.f90:365)
+    double *gR;     // [N] gamma_R
+    double2 *srow;  // [NBMAX] pivot row of the panel step
+    Red *red;       // [NWARP]
+    double *fred;   // [NWARP] float reductions
+    double2 *big;   // union: GJ panel sW[NB][ldw] + sB[NB][TN] | GEMM stages
+    int ldw;
+};
+
+__host__ __device__ inline int round_up(int a, int b) { return (a + b - 1) / b * b; }
+
+template <int NB>
+__host__ __device__ inline size_t smem_bytes(int N) {
+    int ldw = round_up(N, TM);
+    size_t big = (size_t)NB * ldw + (size_t)NB * TN;
+    size_t gemm = 2 * (size_t)TK * (TM + TN);
+    if (gemm > big) big = gemm;
+    size_t b = 0;
+    b += 5 * (size_t)round_up(N, 4) * sizeof(int);
+    b += 2 * (size_t)round_up(N, 2) * sizeof(double2);
+    b += 2 * (size_t)round_up(N, 2) * sizeof(double);
+    b += 32 * sizeof(double2);
+    b += NWARP * sizeof(Red) + NWARP * sizeof(double);
+    b = (b + 255) / 256 * 256;
+    return b + big * sizeof(double2);
+}
+
+template <int NB>
+__device__ inline Smem carve(unsigned char *base, int N) {
+    Smem s;
+    const int n4 = round_up(N, 4), n2 = round_up(N, 2);
+    s.prow = (int *)base;
+    s.iprow = s.prow + n4;
+    s.nx = s.iprow + n4;
+    s.ny = s.nx + n4;
+    s.inP = s.ny + n4;
+    s.sigL = (double2 *)(s.inP + n4);
+    s.sigR = s.sigL + n2;
+    s.gL = (double *)(s.sigR + n2);
+    s.gR = s.gL + n2;
+    s.srow = (double2 *)(s.gR + n2);
+    s.red = (Red *)(s.srow + 32);
+    s.fred = (double *)(s.red + NWARP);
+    size_t off = (size_t)((unsigned char *)(s.fred + NWARP) - base);
+    off = (off + 255) / 256 * 256;
+    s.big = (double2 *)(base + off);
+    s.ldw = round_up(N, TM);
+    return s;
+}
+
+// ------------------------------------------------------- block generation
+// Self energies of the two leads for one job (grid.f90:284-289, 323-331) and
+// the transmission weights (grid.f90:354-360) at the real energy e_t.
+__device__ inline void job_vectors(const Geo &g, const Smem &s, double2 E, double e_t, int ik) {
+    for (int i = threadIdx.x; i < g.N; i += NT) {
+        const double ax = g.ax[ik * g.N + i], ay = g.ay[ik * g.N + i];
+        double2 zl = make_double2(2.0 * (E.x - g.V_L) - ax * ax - ay * ay, 2.0 * E.y);
+        double2 zr = make_double2(2.0 * (E.x - g.V_R) - ax * ax - ay * ay, 2.0 * E.y);
+        s.sigL[i] = self_energy(zsqrt(zl), g.delta);
+        s.sigR[i] = self_energy(zsqrt(zr), g.delta);
+        double ql = sqrt(fmax(2.0 * (e_t - g.V_L) - ax * ax - ay * ay, 0.0));
+        double qr = sqrt(fmax(2.0 * (e_t - g.V_R) - ax * ax - ay * ay, 0.0));
+        s.gL[i] = sin(ql * g.delta) / (g.delta * g.delta);
+        s.gR[i] = sin(qr * g.delta) / (g.delta * g.delta);
+    }
+}
+
+// M = D_k - inv(prev), where inv(prev)(i,j) = R(prow[i], iprow[j]).
+// D_k is generated from V_reciprocal_all (generated = true) or read from an
+// explicit (N,N,Nz) array with leading dimension N (generated = false).
+__device__ inline void form_block(double2 *__restrict__ M, const Geo &g, const Smem &s, int k,
+                                  double2 E, int ik, const double2 *__restrict__ R,
+                                  const double2 *__restrict__ Dexp) {
+    const int N = g.N, ld = g.ld;
+    const double2 *vs = g.vhat ? g.vhat + (size_t)g.W * g.H * k : nullptr;
+    const double2 *Dk = Dexp ? Dexp + (size_t)N * N * k : nullptr;
+    for (int j = 0; j < N; ++j) {
+        const int nxj = s.nx[j], nyj = s.ny[j];
+        const int jc = R ? s.iprow[j] : 0;
+        for (int i = threadIdx.x; i < N; i += NT) {
+            double2 d;
+            if (Dk) {
+                d = Dk[i + (size_t)N * j];
+            } else {
+                const int dx = s.nx[i] - nxj + g.ngx, dy = s.ny[i] - nyj + g.ngy;
+                const double2 v = __ldg(vs + dx + g.W * dy);
+                if (i != j) {
+                    d = make_double2(-v.x * g.c2, -v.y * g.c2);
+                } else {
+                    const double ax = g.ax[ik * N + i], ay = g.ay[ik * N + i];
+                    const double hx = v.x + (ax * ax + ay * ay) / 2;
+                    d = make_double2((-hx + E.x) * g.c2 - 2.0, (-v.y + E.y) * g.c2);
+                    if (k == 0) d = zadd(d, s.sigL[i]);
+                    if (k == g.Nz - 1) d = zadd(d, s.sigR[i]);
+                }
+            }
+            if (R) d = zsub(d, R[s.prow[i] + (size_t)ld * jc]);
+            M[i + (size_t)ld * j] = d;
+        }
+    }
+}
+
+// out(i,j) = inv(R)(i,j) = R(prow[i], iprow[j]) (+ identity when add_eye).
+__device__ inline void unpermute(double2 *__restrict__ out, int ldo, const double2 *__restrict__ R,
+                                 int ld, int N, const Smem &s, double scale) {
+    for (int j = 0; j < N; ++j) {
+        const int jc = s.iprow[j];
+        for (int i = threadIdx.x; i < N; i += NT) {
+            double2 v = R[s.prow[i] + (size_t)ld * jc];
+            out[i + (size_t)ldo * j] = make_double2(v.x * scale, v.y * scale);
+        }
+    }
+}
+
+// ------------------------------------------------------------------ GEMM
+// C(i,j) = sum_k A(i, acol[k]) * B(k, bcol[j]) for one CTA, complex FP64.
+// acol/bcol == nullptr means identity.  Modes of the epilogue:
+enum GemmOut { GEMM_STORE = 0, GEMM_STORE_NEG = 1, GEMM_TAU = 2, GEMM_STORE_ADD_EYE = 3 };
+
+struct GemmArgs {
+    double2 *C;
+    int ldc;
+    const double2 *A;
+    int lda;
+    const int *acol;
+    const double2 *B;
+    int ldb;
+    const int *bcol;
+    int M, Ncol, K;
+};
+
+// Returns, for GEMM_TAU, this thread's partial sum of
+// gL[i] * gR[j] * |(C(i,j)*2)*delta^2|^2 (grid.f90:362-383 after negf.f90:159-165).
+__device__ inline double cta_gemm(const GemmArgs &a, const Smem &s, int mode, double delta) {
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    double2 *sA = s.big;                 // [2][TK][TM]
+    double2 *sB = s.big + 2 * TK * TM;   // [2][TN][TK]
+    const int ntm = (a.M + TM - 1) / TM, ntn = (a.Ncol + TN - 1) / TN;
+    const int nkc = (a.K + TK - 1) / TK;
+    double tau = 0.0;
+    for (int t = 0; t < ntm * ntn; ++t) {
+        const int I0 = (t % ntm) * TM, J0 = (t / ntm) * TN;
+        double2 acc[4][4];
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[p][q] = make_double2(0.0, 0.0);
+
+        auto load_stage = [&](int st, int k0) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int e = tid + NT * q;
+                // A tile: e -> (kk = e / TM, ii = e % TM)
+                {
+                    const int kk = e / TM, ii = e % TM;
+                    const int k = k0 + kk, i = I0 + ii;
+                    const bool v = (k < a.K) && (i < a.M);
+                    const int kc = v ? (a.acol ? a.acol[k] : k) : 0;
+                    cp_async16(sA + st * TK * TM + kk * TM + ii, a.A + (v ? (i + (size_t)a.lda * kc) : 0), v);
+                }
+                // B tile: e -> (jj = e / TK, kk = e % TK), stored [jj][kk]
+                {
+                    const int jj = e / TK, kk = e % TK;
+                    const int k = k0 + kk, j = J0 + jj;
+                    const bool v = (k < a.K) && (j < a.Ncol);
+                    const int jc = v ? (a.bcol ? a.bcol[j] : j) : 0;
+                    cp_async16(sB + st * TN * TK + jj * TK + kk, a.B + (v ? (k + (size_t)a.ldb * jc) : 0), v);
+                }
+            }
+            cp_async_commit();
+        };
+
+        load_stage(0, 0);
+        for (int c = 0; c < nkc; ++c) {
+            if (c + 1 < nkc) {
+                load_stage((c + 1) & 1, (c + 1) * TK);
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
+            }
+            __syncthreads();
+            const double2 *cA = sA + (c & 1) * TK * TM;
+            const double2 *cB = sB + (c & 1) * TN * TK;
+#pragma unroll 4
+            for (int kk = 0; kk < TK; ++kk) {
+                double2 av[4], bv[4];
+#pragma unroll
+                for (int p = 0; p < 4; ++p) av[p] = cA[kk * TM + tx + 16 * p];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) bv[q] = cB[(ty + 16 * q) * TK + kk];
+#pragma unroll
+                for (int p = 0; p < 4; ++p)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) acc[p][q] = zfma(av[p], bv[q], acc[p][q]);
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            const int i = I0 + tx + 16 * p;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int j = J0 + ty + 16 * q;
+                if (i < a.M && j < a.Ncol) {
+                    double2 v = acc[p][q];
+                    if (mode == GEMM_TAU) {
+                        const double gx = v.x * 2.0 * (delta * delta), gy = v.y * 2.0 * (delta * delta);
+                        tau += s.gL[i] * s.gR[j] * (gx * gx + gy * gy);
+                    } else {
+                        if (mode == GEMM_STORE_NEG) v = make_double2(-v.x, -v.y);
+                        if (mode == GEMM_STORE_ADD_EYE && i == j) v.x += 1.0;
+                        a.C[i + (size_t)a.ldc * j] = v;
+                    }
+                }
+            }
+        }
+    }
+    return tau;
+}
+
+// Block-wide sum of one double per thread; result valid in every thread.
+__device__ inline double block_sum(double v, const Smem &s) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) s.fred[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double t = 0.0;
+#pragma unroll
+    for (int w = 0; w < NWARP; ++w) t += s.fred[w];
+    __syncthreads();
+    return t;
+}
+
+// ----------------------------------------------------- Gauss-Jordan inverse
+// Rank-nbe update of every column outside the panel [k0, k0+nbe):
+//   A(:, j) = mask(A(:, j)) + W * A_old(prow[k0:k0+nbe], j)
+// where W = the panel after elimination (held in sW) and mask zeroes the
+// panel's pivot rows.  See the derivation in the file header.
+template <int NB>
+__device__ inline void trailing_update(double2 *__restrict__ A, int N, int ld, int k0, int nbe,
+                                       const Smem &s) {
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int nrest = N - nbe;
+    const int ldw = s.ldw;
+    const double2 *sW = s.big;
+    double2 *sB = s.big + NB * ldw;
+    for (int J0 = 0; J0 < nrest; J0 += TN) {
+        for (int e = tid; e < NB * TN; e += NT) {
+            const int kk = e / TN, jt = e % TN, jr = J0 + jt;
+            double2 v = make_double2(0.0, 0.0);
+            if (kk < nbe && jr < nrest) {
+                const int j = jr < k0 ? jr : jr + nbe;
+                v = A[s.prow[k0 + kk] + (size_t)ld * j];
+            }
+            sB[e] = v;
+        }
+        __syncthreads();
+        int col[4];
+        bool cv[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int jr = J0 + ty + 16 * q;
+            cv[q] = jr < nrest;
+            col[q] = jr < k0 ? jr : jr + nbe;
+        }
+        for (int I0 = 0; I0 < N; I0 += TM) {
+            double2 acc[4][4];
+#pragma unroll
+            for (int p = 0; p < 4; ++p) {
+                const int i = I0 + tx + 16 * p;
+                const bool rv = (i < N) && !s.inP[i];
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    acc[p][q] = (rv && cv[q]) ? A[i + (size_t)ld * col[q]] : make_double2(0.0, 0.0);
+            }
+#pragma unroll 4
+            for (int kk = 0; kk < nbe; ++kk) {
+                double2 wv[4], bv[4];
+#pragma unroll
+                for (int p = 0; p < 4; ++p) wv[p] = sW[kk * ldw + I0 + tx + 16 * p];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) bv[q] = sB[kk * TN + ty + 16 * q];
+#pragma unroll
+                for (int p = 0; p < 4; ++p)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) acc[p][q] = zfma(wv[p], bv[q], acc[p][q]);
+            }
+#pragma unroll
+            for (int p = 0; p < 4; ++p) {
+                const int i = I0 + tx + 16 * p;
+                if (i < N) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        if (cv[q]) A[i + (size_t)ld * col[q]] = acc[p][q];
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// In-place blocked Gauss-Jordan inverse of the N x N block A (leading
+// dimension ld) with implicit partial pivoting.  On return s.prow/s.iprow
+// hold the permutations; the caller reads inv(A) through them.  Returns the
+// LAPACK-style info (1-based column of the first zero pivot, 0 if none);
+// identical in every thread.  RPT = rows per thread (N <= NT*RPT).
+template <int NB, int RPT>
+__device__ int gj_invert(double2 *__restrict__ A, int N, int ld, const Smem &s) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int ldw = s.ldw;
+    double2 *sW = s.big;
+    int info = 0;
+    unsigned used = 0;
+#pragma unroll
+    for (int r = 0; r < RPT; ++r)
+        if (tid + NT * r >= N) used |= 1u << r;
+    for (int i = tid; i < N; i += NT) s.inP[i] = 0;
+    __syncthreads();
+
+    for (int k0 = 0; k0 < N; k0 += NB) {
+        const int nbe = min(NB, N - k0);
+        double2 w[RPT][NB];
+#pragma unroll
+        for (int r = 0; r < RPT; ++r) {
+            const int i = tid + NT * r;
+#pragma unroll
+            for (int jj = 0; jj < NB; ++jj)
+                w[r][jj] = (i < N && jj < nbe) ? A[i + (size_t)ld * (k0 + jj)] : make_double2(0.0, 0.0);
+        }
+        // The panel step loop is not unrolled: the pivot column kk is picked out
+        // of the register rows by predication, which keeps the code size O(NB).
+#pragma unroll 1
+        for (int kk = 0; kk < nbe; ++kk) {
+            double2 f[RPT];
+#pragma unroll
+            for (int r = 0; r < RPT; ++r) {
+                f[r] = make_double2(0.0, 0.0);
+#pragma unroll
+                for (int jj = 0; jj < NB; ++jj)
+                    if (jj == kk) f[r] = w[r][jj];
+            }
+            // --- pivot search among unused rows (largest |re|+|im|, lowest index on ties)
+            double bv = -1.0;
+            int bi = 0x7fffffff;
+            double2 bval = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int r = 0; r < RPT; ++r) {
+                if (!((used >> r) & 1u)) {
+                    double v = cabs1(f[r]);
+                    if (!(v == v)) v = 0.0;  // NaN rows rank as zero pivots
+                    if (v > bv) { bv = v; bi = tid + NT * r; bval = f[r]; }
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                const double ox = __shfl_xor_sync(0xffffffffu, bval.x, o);
+                const double oy = __shfl_xor_sync(0xffffffffu, bval.y, o);
+                if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; bval = make_double2(ox, oy); }
+            }
+            if (lane == 0) { s.red[warp].v = bv; s.red[warp].idx = bi; s.red[warp].val = bval; }
+            __syncthreads();
+            bv = s.red[0].v; bi = s.red[0].idx; bval = s.red[0].val;
+#pragma unroll
+            for (int q = 1; q < NWARP; ++q) {
+                const Red o = s.red[q];
+                if (o.v > bv || (o.v == bv && o.idx < bi)) { bv = o.v; bi = o.idx; bval = o.val; }
+            }
+            const int p = bi;
+            if (bv == 0.0 && info == 0) info = k0 + kk + 1;
+            const double2 d = zrcp(bval);
+#pragma unroll
+            for (int r = 0; r < RPT; ++r) {
+                if (tid + NT * r == p) {
+                    used |= 1u << r;
+#pragma unroll
+                    for (int jj = 0; jj < NB; ++jj) s.srow[jj] = w[r][jj];
+                }
+            }
+            if (tid == 0) { s.prow[k0 + kk] = p; s.inP[p] = 1; }
+            __syncthreads();
+            // --- eliminate column kk from every row, scale the pivot row
+#pragma unroll
+            for (int r = 0; r < RPT; ++r) {
+                const int i = tid + NT * r;
+                if (i == p) {
+#pragma unroll
+                    for (int jj = 0; jj < NB; ++jj) {
+                        const double2 v = zmul(s.srow[jj], d);
+                        w[r][jj] = (jj == kk) ? d : v;
+                    }
+                } else {
+                    const double2 gm = zmul(f[r], d);
+#pragma unroll
+                    for (int jj = 0; jj < NB; ++jj) {
+                        const double2 v = zfms(gm, s.srow[jj], w[r][jj]);
+                        w[r][jj] = (jj == kk) ? make_double2(-gm.x, -gm.y) : v;
+                    }
+                }
+            }
+        }
+        // --- write the panel back and stage it for the trailing update
+#pragma unroll
+        for (int r = 0; r < RPT; ++r) {
+            const int i = tid + NT * r;
+            if (i < ldw) {
+#pragma unroll
+                for (int jj = 0; jj < NB; ++jj) {
+                    const double2 v = (i < N) ? w[r][jj] : make_double2(0.0, 0.0);
+                    sW[jj * ldw + i] = v;
+                    if (i < N && jj < nbe) A[i + (size_t)ld * (k0 + jj)] = v;
+                }
+            }
+        }
+        __syncthreads();
+        if (nbe < N) trailing_update<NB>(A, N, ld, k0, nbe, s);
+        __syncthreads();
+        if (tid < nbe) s.inP[s.prow[k0 + tid]] = 0;
+        __syncthreads();
+    }
+    for (int k = tid; k < N; k += NT) s.iprow[s.prow[k]] = k;
+    __syncthreads();
+    return info;
+}
+
+}  // namespace negf

@@ -1,0 +1,142 @@
+"""The job-level drivers of src/negf.f90 and the solver of src/math_kernel.f90,
+run on the GPU through libnegfgpu.so.
+
+``Engine`` holds one negf_ctx (the V table, basis and k-points resident on the
+device).  Its methods take whole batches of jobs, which is how the MPI job
+loops of src/main.f90 call the reference drivers one job at a time:
+
+=====================================  =====================================
+reference                              here
+=====================================  =====================================
+Transmission_Coefficient (negf:115)    Engine.transmission(energies)
+Equilibrium_Density (negf:9)           Engine.equilibrium_density(...)
+Local_Density_Of_State (negf:176)      Engine.ldos_matrix(...)
+GreensFunction_tri_solver (mk:44)      GreensFunction_tri_solver(D, DFL)
+=====================================  =====================================
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import NEGF_FP64, Problem, Stats, _dp, _ip, check, lib
+
+
+class Engine:
+    """A device-resident problem (negf_ctx).
+
+    nx_grid, ny_grid: basis; V_reciprocal_all: (2NGX+1, 2NGY+1, N_z) complex;
+    Lx, Ly, Lz (bohr); V_L, V_R, ETA (Hartree); kpoint: (nk, 3) of (kx, ky, w).
+    """
+
+    def __init__(self, nx_grid, ny_grid, V_reciprocal_all, Lx, Ly, Lz, V_L, V_R, ETA, kpoint,
+                 device=0):
+        self.nx = np.ascontiguousarray(nx_grid, np.int32)
+        self.ny = np.ascontiguousarray(ny_grid, np.int32)
+        self.vhat = np.asfortranarray(V_reciprocal_all, np.complex128)
+        self.kpt = np.ascontiguousarray(kpoint, np.float64).reshape(-1, 3)
+        self.N = len(self.nx)
+        self.Nz = self.vhat.shape[2]
+        self.Lx, self.Ly, self.Lz = float(Lx), float(Ly), float(Lz)
+        self.V_L, self.V_R, self.eta = float(V_L), float(V_R), float(ETA)
+        p = Problem()
+        p.N, p.Nz = self.N, self.Nz
+        p.ngx = (self.vhat.shape[0] - 1) // 2
+        p.ngy = (self.vhat.shape[1] - 1) // 2
+        p.nx = self.nx.ctypes.data_as(_ip)
+        p.ny = self.ny.ctypes.data_as(_ip)
+        p.vhat = self.vhat.ctypes.data_as(_dp)
+        p.Lx, p.Ly, p.Lz = self.Lx, self.Ly, self.Lz
+        p.V_L, p.V_R, p.eta = self.V_L, self.V_R, self.eta
+        p.nk = len(self.kpt)
+        p.kpt = self.kpt.ctypes.data_as(_dp)
+        self._ctx = C.c_void_p()
+        check("negf_ctx_create", lib().negf_ctx_create(C.byref(p), device, C.byref(self._ctx)))
+        self.device = device
+        self.last_stats = Stats()
+
+    def close(self):
+        if self._ctx:
+            lib().negf_ctx_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._ctx
+
+    # negf.f90:115-174 over all (E, k) jobs
+    def transmission(self, energies, precision=NEGF_FP64):
+        """Transmission(:)%tau after the job loop and reduction of main.f90:384-407.
+
+        energies: Transmission(:)%energy in Hartree.  Returns (tau[nE], info) where
+        info > 0 flags a zero pivot in some job (see last_stats)."""
+        e = np.ascontiguousarray(energies, np.float64)
+        tau = np.zeros(len(e))
+        st = Stats()
+        rc = check("negf_transmission", lib().negf_transmission(
+            self._ctx, e.ctypes.data_as(_dp), len(e), precision, tau.ctypes.data_as(_dp), C.byref(st)))
+        self.last_stats = st
+        return tau, rc
+
+    def transmission_device(self, d_energies, nE, d_tau, d_tau_jobs=None, d_info=None, stream=None,
+                            precision=NEGF_FP64):
+        """Enqueue on device pointers (ints); no synchronisation."""
+        check("negf_transmission_device", lib().negf_transmission_device(
+            self._ctx, C.c_void_p(d_energies), nE, precision, C.c_void_p(d_tau),
+            C.c_void_p(d_tau_jobs or 0), C.c_void_p(d_info or 0), C.c_void_p(stream or 0)))
+
+    # negf.f90:9-113 over all contour jobs
+    def equilibrium_density(self, N_circle, N_line, min_V, MU, GAP, TEMPERATURE):
+        """Density_Matrix (N, N, N_z) complex after main.f90:272-297."""
+        dm = np.zeros((self.N, self.N, self.Nz), np.complex128, order="F")
+        st = Stats()
+        rc = check("negf_density", lib().negf_density(
+            self._ctx, N_circle, N_line, min_V, MU, GAP, TEMPERATURE, dm.ctypes.data_as(_dp),
+            C.byref(st)))
+        self.last_stats = st
+        return dm, rc
+
+    # negf.f90:176-236 summed over k-points, for a range of LDOS energies
+    def ldos_matrix(self, e_lo, e_hi, N_E, i_e0=0, n_chunk=None):
+        """LDOS_Matrix per energy: (n_chunk, N, N, N_z) complex (each Fortran-ordered)."""
+        if n_chunk is None:
+            n_chunk = N_E - i_e0
+        out = np.zeros((n_chunk, self.Nz, self.N, self.N), np.complex128)
+        st = Stats()
+        rc = check("negf_ldos_matrix", lib().negf_ldos_matrix(
+            self._ctx, e_lo, e_hi, N_E, i_e0, n_chunk, out.ctypes.data_as(_dp), C.byref(st)))
+        self.last_stats = st
+        # memory is [o][k][j][i] -> expose (o, i, j, k)
+        return np.transpose(out, (0, 3, 2, 1)), rc
+
+
+def GreensFunction_tri_solver(G_inv_D, DFL, engine: Engine | None = None):
+    """math_kernel.f90:44-165 on the GPU.
+
+    G_inv_D: (N, N, N_z) complex.  Returns ({'D': diag, 'F': first, 'L': last}
+    for the letters in DFL, each (N, N, N_z) complex), info)."""
+    D = np.asfortranarray(G_inv_D, np.complex128)
+    N, _, Nz = D.shape
+    outs, ptrs = {}, []
+    for key in "DFL":
+        if key in DFL.upper():
+            outs[key] = np.zeros_like(D, order="F")
+            ptrs.append(outs[key].ctypes.data_as(_dp))
+        else:
+            ptrs.append(None)
+    rc = check("negf_tri_solve", lib().negf_tri_solve(
+        engine.handle if engine else None, D.ctypes.data_as(_dp), N, Nz, DFL.encode(), *ptrs))
+    return outs, rc

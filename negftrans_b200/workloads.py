@@ -1,0 +1,88 @@
+"""Seeded synthetic workloads (no dataset is involved).
+
+A split-gate quantum point contact in a 100 x 100 nm periodic cell,
+    V(x, z) = V_g exp(-z^2 / 2 s_z^2) (1 - exp(-x^2 / 2 w^2)),
+x and z measured from the cell centre (x_i = (i - N_x/2) dx, z_k = (k + 1/2 - N_z/2) dz
+for 0-based i, k), plus optional Gaussian-correlated disorder (white noise
+filtered by exp(-q^2 l^2 / 4), normalised to an RMS of sigma).  GaAs
+(m* = 0.067) is emulated in the reference's free-electron units by scaling the
+INPUT: V' = m* V, E' = m* E, eta' = m* eta, T' = m* T; tau is unchanged.
+ENCUT' values give the circular cutoffs with N = 69 / 221 / 797 plane waves.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from .constants import HARTREE
+from .prepare import InputDeck
+
+MSTAR = 0.067
+
+
+def qpc_potential(Nx, Ny, Nz, L_nm, Lz_nm, Vg, w_nm, sz_nm, disorder=0.0, corr_nm=10.0, seed=1000):
+    """Potential in eV (unscaled), shape (Nx, Ny, Nz), Fortran order."""
+    dx = L_nm / Nx
+    dz = Lz_nm / Nz
+    x = (np.arange(Nx) - Nx / 2) * dx
+    z = (np.arange(Nz) + 0.5 - Nz / 2) * dz
+    gate = 1.0 - np.exp(-x ** 2 / (2 * w_nm ** 2))
+    env = np.exp(-z ** 2 / (2 * sz_nm ** 2))
+    V = Vg * gate[:, None, None] * env[None, None, :] * np.ones((1, Ny, 1))
+    if disorder > 0:
+        rng = np.random.Generator(np.random.PCG64(seed))
+        noise = rng.standard_normal((Nx, Ny, Nz))
+        qx = 2 * np.pi * np.fft.fftfreq(Nx, d=dx)
+        qy = 2 * np.pi * np.fft.fftfreq(Ny, d=L_nm / Ny)
+        qz = 2 * np.pi * np.fft.fftfreq(Nz, d=dz)
+        q2 = qx[:, None, None] ** 2 + qy[None, :, None] ** 2 + qz[None, None, :] ** 2
+        filt = np.exp(-q2 * corr_nm ** 2 / 4)
+        d = np.real(np.fft.ifftn(np.fft.fftn(noise) * filt))
+        d *= disorder / np.sqrt(np.mean(d ** 2))
+        V = V + d
+    return np.asfortranarray(V)
+
+
+@dataclass
+class Workload:
+    name: str
+    deck: InputDeck
+    V_eV: np.ndarray         # POTENTIAL (already m*-scaled), eV
+    n_energy: int
+    notes: str = ""
+
+
+def _deck(Lz_A, encut, e_max_meV, n_e, nk=1, mu_meV=20.0, t_K=1.1605, n_circle=48, n_line=256):
+    # N_line = IDNINT(N_line_per_eV * 2 * GAP[eV]) with GAP = 6 k_B T' (main.f90:193,261)
+    kT_eV = 8.617333262e-5 * MSTAR * t_K
+    per_eV = int(round(n_line / (12 * kT_eV)))
+    return InputDeck(
+        if_transmission=True, if_density=True, LX=1000.0, LY=1000.0, LZ=Lz_A, ENCUT=encut,
+        ETA=MSTAR * 1e-6 / HARTREE, NKX=nk, NKY=nk, TEMPERATURE=MSTAR * t_K, MU=MSTAR * mu_meV * 1e-3,
+        TRANSMISSION_GRID=(0.0, MSTAR * e_max_meV * 1e-3, float(n_e)), N_circle=n_circle,
+        N_line_per_eV=per_eV)
+
+
+def config(name: str) -> Workload:
+    """Named workloads with the shapes of the benchmark configurations."""
+    if name == "qpc_n69":
+        # 69 plane waves, 200 slices of 1 nm, 512 energies on [0, 30) meV, Gamma only
+        V = MSTAR * qpc_potential(64, 64, 200, 100.0, 200.0, 0.050, 15.0, 20.0)
+        return Workload(name, _deck(2000.0, 0.0033091, 30.0, 512), V, 512)
+    if name == "qpc_disorder_n221":
+        # 221 plane waves, 800 slices of 0.5 nm, 2048 energies on [0, 40) meV, disorder 2 meV / 10 nm
+        V = MSTAR * qpc_potential(64, 64, 800, 100.0, 400.0, 0.050, 15.0, 20.0, disorder=0.002)
+        return Workload(name, _deck(4000.0, 0.0105288, 40.0, 2048), V, 2048)
+    if name == "qpc_disorder_n797":
+        # 797 plane waves (128x128 grid), 400 slices of 1 nm, 1024 energies on [0, 50) meV
+        V = MSTAR * qpc_potential(128, 128, 400, 100.0, 400.0, 0.060, 20.0, 20.0, disorder=0.002)
+        return Workload(name, _deck(4000.0, 0.0385807, 50.0, 1024), V, 1024)
+    if name.startswith("small"):
+        # test-sized QPC: small basis and few slices, same physics
+        # small:<encut_meV>:<Nz>  (e.g. small:1.2:16)
+        _, enc, nz = name.split(":")
+        nz = int(nz)
+        V = MSTAR * qpc_potential(32, 32, nz, 100.0, nz * 1.0, 0.050, 15.0, nz / 10.0, disorder=0.002)
+        return Workload(name, _deck(nz * 10.0, float(enc) * 1e-3, 30.0, 16), V, 16)
+    raise KeyError(name)

@@ -1,0 +1,332 @@
+"""ctypes front end of the C oracle, plus two independent checks of it.
+
+TEST INFRASTRUCTURE ONLY: imported by ``tests/``, by ``__graft_entry__.smoke``
+and by the CPU-baseline leg of ``bench.py``; never by the product package.
+
+* ``C*`` functions call ``liboracle.so`` (the restatement of src/negf.f90,
+  src/math_kernel.f90 and src/grid.f90; see negf_oracle.c for line cites).
+* ``dense_blocks`` inverts the whole block-tridiagonal matrix with NumPy, an
+  algorithm unrelated to RGF, to check the recursions of
+  math_kernel.f90:81-162.
+* ``closed_form_*`` solve potentials that depend on z only.  Then H is
+  diagonal in the plane-wave basis and every mode is a scalar tridiagonal
+  system; its Green's function follows from the three-term determinant
+  recursion, evaluated here in 80-bit long double.  These are the analytic
+  known answers that pin the oracle (the reference ships no golden outputs).
+
+Parity status: unpinned against the reference build (see negf_oracle.h).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import build as _build
+
+HARTREE = 27.211386245988          # global.f90:24
+K_B = 8.617333262e-5 / HARTREE     # global.f90:26
+A_0 = 0.529177210903               # global.f90:27
+PI = 3.141592653589793             # global.f90:28
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+
+
+class _Problem(C.Structure):
+    _fields_ = [("N", C.c_int32), ("Nz", C.c_int32), ("ngx", C.c_int32), ("ngy", C.c_int32),
+                ("nx", _ip), ("ny", _ip), ("vhat", _dp), ("Lx", C.c_double), ("Ly", C.c_double),
+                ("Lz", C.c_double), ("V_L", C.c_double), ("V_R", C.c_double), ("eta", C.c_double),
+                ("nk", C.c_int32), ("kpt", _dp)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = _build.build()
+        L = C.CDLL(path)
+        rc = L.oracle_init(_build.lapack_path().encode())
+        if rc != 0:
+            raise RuntimeError(f"oracle_init failed ({rc})")
+        L.oracle_basis_findsize.restype = C.c_int32
+        L.oracle_basis_findsize.argtypes = [C.c_double] * 3
+        for name in ("oracle_coefficient_simpson", "oracle_value_simpson"):
+            getattr(L, name).restype = C.c_double
+            getattr(L, name).argtypes = [C.c_int32, C.c_int32, C.c_double, C.c_double]
+        L.oracle_fermi_func.restype = C.c_double
+        L.oracle_fermi_func.argtypes = [C.c_double] * 3
+        L.oracle_transmission_solver.restype = C.c_double
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _i(a):
+    return a.ctypes.data_as(_ip)
+
+
+class Problem:
+    """The inputs of one hot-path run in the reference's atomic units.
+
+    vhat is V_reciprocal_all(-ngx:ngx, -ngy:ngy, 1:Nz) as a complex
+    Fortran-ordered array (already truncated to |i|<=ngx/2, |j|<=ngy/2).
+    kpt is an (nk, 3) array of (kx, ky, weight).
+    """
+
+    def __init__(self, nx, ny, vhat, Lx, Ly, Lz, V_L, V_R, eta, kpt):
+        self.nx = np.ascontiguousarray(nx, dtype=np.int32)
+        self.ny = np.ascontiguousarray(ny, dtype=np.int32)
+        self.vhat = np.asfortranarray(vhat, dtype=np.complex128)
+        self.Lx, self.Ly, self.Lz = float(Lx), float(Ly), float(Lz)
+        self.V_L, self.V_R, self.eta = float(V_L), float(V_R), float(eta)
+        self.kpt = np.ascontiguousarray(kpt, dtype=np.float64).reshape(-1, 3)
+        self.N = len(self.nx)
+        self.ngx = (self.vhat.shape[0] - 1) // 2
+        self.ngy = (self.vhat.shape[1] - 1) // 2
+        self.Nz = self.vhat.shape[2]
+
+    def c(self):
+        s = _Problem()
+        s.N, s.Nz, s.ngx, s.ngy = self.N, self.Nz, self.ngx, self.ngy
+        s.nx, s.ny = _i(self.nx), _i(self.ny)
+        s.vhat = self.vhat.ctypes.data_as(_dp)
+        s.Lx, s.Ly, s.Lz = self.Lx, self.Ly, self.Lz
+        s.V_L, s.V_R, s.eta = self.V_L, self.V_R, self.eta
+        s.nk = len(self.kpt)
+        s.kpt = _d(self.kpt)
+        self._keep = s
+        return C.byref(s)
+
+
+# ------------------------------------------------------------ grid.f90 mirror
+def basis(encut, lx, ly):
+    L = lib()
+    n = L.oracle_basis_findsize(encut, lx, ly)
+    nx = np.zeros(n, np.int32)
+    ny = np.zeros(n, np.int32)
+    L.oracle_basis(C.c_double(encut), C.c_double(lx), C.c_double(ly), _i(nx), _i(ny))
+    return nx, ny
+
+
+def kmesh(nkx, nky, lx, ly):
+    out = np.zeros((nkx * nky, 3))
+    lib().oracle_kmesh(C.c_int32(nkx), C.c_int32(nky), C.c_double(lx), C.c_double(ly), _d(out))
+    return out
+
+
+def rtop(vreal2d, ngx, ngy):
+    v = np.asfortranarray(vreal2d, dtype=np.float64)
+    out = np.zeros((2 * ngx + 1, 2 * ngy + 1), np.complex128, order="F")
+    rc = lib().oracle_rtop(_d(v), C.c_int32(v.shape[0]), C.c_int32(v.shape[1]), C.c_int32(ngx),
+                           C.c_int32(ngy), out.ctypes.data_as(_dp))
+    if rc:
+        raise ValueError("V_reciprocal larger than the real-space grid (grid.f90:33-37)")
+    return out
+
+
+def vhat_all(vreal3d, ngx, ngy):
+    v = np.asfortranarray(vreal3d, dtype=np.float64)
+    Nx, Ny, Nz = v.shape
+    out = np.zeros((2 * ngx + 1, 2 * ngy + 1, Nz), np.complex128, order="F")
+    rc = lib().oracle_vhat_all(_d(v), C.c_int32(Nx), C.c_int32(Ny), C.c_int32(Nz), C.c_int32(ngx),
+                               C.c_int32(ngy), out.ctypes.data_as(_dp))
+    if rc:
+        raise ValueError("V_reciprocal larger than the real-space grid (grid.f90:33-37)")
+    return out
+
+
+def hamiltonian(p: Problem, kx, ky):
+    H = np.zeros((p.N, p.N, p.Nz), np.complex128, order="F")
+    lib().oracle_hamiltonian(p.c(), C.c_double(kx), C.c_double(ky), H.ctypes.data_as(_dp))
+    return H
+
+
+def e_minus_h(p: Problem, H, energy, kx, ky):
+    H = np.asfortranarray(H, dtype=np.complex128)
+    D = np.zeros_like(H, order="F")
+    e = complex(energy)
+    lib().oracle_e_minus_h(p.c(), H.ctypes.data_as(_dp), C.c_double(e.real), C.c_double(e.imag),
+                           C.c_double(kx), C.c_double(ky), D.ctypes.data_as(_dp))
+    return D
+
+
+def tri_solver(D, dfl):
+    D = np.asfortranarray(D, dtype=np.complex128)
+    N, _, Nz = D.shape
+    outs = {}
+    ptrs = []
+    for key in "DFL":
+        if key in dfl.upper():
+            outs[key] = np.zeros_like(D, order="F")
+            ptrs.append(outs[key].ctypes.data_as(_dp))
+        else:
+            ptrs.append(None)
+    info = lib().oracle_tri_solver(D.ctypes.data_as(_dp), C.c_int32(N), C.c_int32(Nz),
+                                   dfl.encode(), *ptrs)
+    if info < 0:
+        raise ValueError("tri_solver needs N >= 1 and Nz >= 2")
+    return outs, info
+
+
+def transmission_solver(p: Problem, first, energy, kx, ky):
+    first = np.asfortranarray(first, dtype=np.complex128)
+    return lib().oracle_transmission_solver(
+        first.ctypes.data_as(_dp), C.c_int32(p.N), C.c_int32(p.Nz), C.c_double(energy), _i(p.nx),
+        _i(p.ny), C.c_double(p.Lx), C.c_double(p.Ly), C.c_double(p.Lz), C.c_double(kx),
+        C.c_double(ky), C.c_double(p.V_L), C.c_double(p.V_R))
+
+
+def coefficient_simpson(i, N, a, b):
+    return lib().oracle_coefficient_simpson(i, N, a, b)
+
+
+def value_simpson(i, N, a, b):
+    return lib().oracle_value_simpson(i, N, a, b)
+
+
+def fermi_func(e, mu, t):
+    return lib().oracle_fermi_func(e, mu, t)
+
+
+# ------------------------------------------------------------ negf.f90 mirror
+def transmission_coefficient(p: Problem, i_job, energies, tau):
+    """negf.f90:115-174 for one 1-based job; accumulates into tau in place."""
+    energies = np.ascontiguousarray(energies, dtype=np.float64)
+    assert tau.dtype == np.float64 and tau.flags.c_contiguous
+    return lib().oracle_transmission_coefficient(p.c(), C.c_int32(i_job), _d(energies),
+                                                 C.c_int32(len(energies)), _d(tau))
+
+
+def transmission_jobs(p: Problem, energies, job_lo=0, job_hi=None, nthreads=1):
+    """main.f90:384-407 job loop (ranks -> threads) -> tau[nE] = sum_k w_k tau."""
+    energies = np.ascontiguousarray(energies, dtype=np.float64)
+    nE = len(energies)
+    if job_hi is None:
+        job_hi = nE * len(p.kpt)
+    tau = np.zeros(nE)
+    info = lib().oracle_transmission_jobs(p.c(), _d(energies), C.c_int32(nE), C.c_int32(job_lo),
+                                          C.c_int32(job_hi), C.c_int32(nthreads), _d(tau))
+    return tau, info
+
+
+def equilibrium_density(p: Problem, i_job, n_circle, n_line, min_v, mu, gap, temperature, dm):
+    return lib().oracle_equilibrium_density(
+        p.c(), C.c_int32(i_job), C.c_int32(n_circle), C.c_int32(n_line), C.c_double(min_v),
+        C.c_double(mu), C.c_double(gap), C.c_double(temperature), dm.ctypes.data_as(_dp))
+
+
+def density_jobs(p: Problem, n_circle, n_line, min_v, mu, gap, temperature, job_lo=0,
+                 job_hi=None, nthreads=1):
+    if job_hi is None:
+        job_hi = (n_circle + n_line) * len(p.kpt)
+    dm = np.zeros((p.N, p.N, p.Nz), np.complex128, order="F")
+    info = lib().oracle_density_jobs(
+        p.c(), C.c_int32(n_circle), C.c_int32(n_line), C.c_double(min_v), C.c_double(mu),
+        C.c_double(gap), C.c_double(temperature), C.c_int32(job_lo), C.c_int32(job_hi),
+        C.c_int32(nthreads), dm.ctypes.data_as(_dp))
+    return dm, info
+
+
+def local_density_of_state(p: Problem, i_kpoint, i_energy, n_e, e_lo, e_hi, ldos):
+    return lib().oracle_local_density_of_state(
+        p.c(), C.c_int32(i_kpoint), C.c_int32(i_energy), C.c_int32(n_e), C.c_double(e_lo),
+        C.c_double(e_hi), ldos.ctypes.data_as(_dp))
+
+
+def ptor(G, nx, ny, Nx, Ny):
+    G = np.asfortranarray(G, dtype=np.complex128)
+    out = np.zeros((Nx, Ny), np.complex128, order="F")
+    lib().oracle_ptor(G.ctypes.data_as(_dp), _i(np.ascontiguousarray(nx, np.int32)),
+                      _i(np.ascontiguousarray(ny, np.int32)), C.c_int32(G.shape[0]),
+                      C.c_int32(Nx), C.c_int32(Ny), out.ctypes.data_as(_dp))
+    return out
+
+
+# ----------------------------------------------------- independent checkers
+def dense_blocks(D):
+    """All blocks of inv(tridiag(I, D_k, I)) by one dense NumPy inverse."""
+    N, _, Nz = D.shape
+    A = np.zeros((N * Nz, N * Nz), np.complex128)
+    for k in range(Nz):
+        A[k * N:(k + 1) * N, k * N:(k + 1) * N] = D[:, :, k]
+        if k + 1 < Nz:
+            A[k * N:(k + 1) * N, (k + 1) * N:(k + 2) * N] = np.eye(N)
+            A[(k + 1) * N:(k + 2) * N, k * N:(k + 1) * N] = np.eye(N)
+    G = np.linalg.inv(A)
+    diag = np.stack([G[k * N:(k + 1) * N, k * N:(k + 1) * N] for k in range(Nz)], axis=2)
+    first = np.stack([G[k * N:(k + 1) * N, 0:N] for k in range(Nz)], axis=2)
+    last = np.stack([G[k * N:(k + 1) * N, (Nz - 1) * N:] for k in range(Nz)], axis=2)
+    return diag, first, last
+
+
+def _kin(n, L, k):
+    return (2.0 * n) * PI / L + k
+
+
+def closed_form_modes(nx, ny, vz, Lx, Ly, Lz, V_L, V_R, eta, energy, kx, ky):
+    """Scalar three-term recursion per plane-wave mode for a z-only potential.
+
+    vz[k] is V_reciprocal(0,0,k) (the xy-average of slice k, Hartree).  Returns
+    (G_first[N] = G_{Nz,1}, G_diag[N, Nz] = G_{kk}) rescaled by 2*Delta^2 as in
+    negf.f90:159-165, computed in long double, plus sL, sR of grid.f90:355-365.
+    """
+    ld = np.longdouble
+    Nz = len(vz)
+    delta = ld(Lz) / Nz
+    c2 = 2 * delta * delta
+    e = complex(energy)
+    N = len(nx)
+    G_first = np.zeros(N, np.complex128)
+    G_diag = np.zeros((N, Nz), np.complex128)
+    sL = np.zeros(N)
+    sR = np.zeros(N)
+    vz = np.asarray(vz)
+    for i in range(N):
+        ax = ld(_kin(int(nx[i]), Lx, kx))
+        ay = ld(_kin(int(ny[i]), Ly, ky))
+        eps = (ax * ax + ay * ay) / 2
+        qL = np.sqrt(np.clongdouble(2 * (np.clongdouble(e) - ld(V_L) + 1j * ld(eta)) - 2 * eps))
+        qR = np.sqrt(np.clongdouble(2 * (np.clongdouble(e) - ld(V_R) + 1j * ld(eta)) - 2 * eps))
+        d = np.empty(Nz, np.clongdouble)
+        for k in range(Nz):
+            d[k] = c2 * (np.clongdouble(e) + 1j * ld(eta) - ld(vz[k].real) - 1j * ld(vz[k].imag)
+                         - eps) - 2
+        d[0] += np.exp(1j * qL * delta)
+        d[-1] += np.exp(1j * qR * delta)
+        # theta_k = det of leading k x k, phi_k = det of trailing block from k
+        th = np.empty(Nz + 1, np.clongdouble)
+        th[0] = 1
+        th[1] = d[0]
+        for k in range(2, Nz + 1):
+            th[k] = d[k - 1] * th[k - 1] - th[k - 2]
+        ph = np.empty(Nz + 2, np.clongdouble)
+        ph[Nz + 1] = 1
+        ph[Nz] = d[Nz - 1]
+        for k in range(Nz - 1, 0, -1):
+            ph[k] = d[k - 1] * ph[k + 1] - ph[k + 2]
+        det = th[Nz]
+        G_first[i] = complex(((-1) ** (Nz - 1)) / det * c2)
+        for k in range(1, Nz + 1):
+            G_diag[i, k - 1] = complex(th[k - 1] * ph[k + 1] / det * c2)
+        qr = np.sqrt(max(2 * (ld(e.real) - ld(V_L)) - 2 * eps, ld(0)))
+        qt = np.sqrt(max(2 * (ld(e.real) - ld(V_R)) - 2 * eps, ld(0)))
+        sL[i] = float(np.sin(qr * delta) / (delta * delta))
+        sR[i] = float(np.sin(qt * delta) / (delta * delta))
+    return G_first, G_diag, sL, sR
+
+
+def closed_form_tau(nx, ny, vz, Lx, Ly, Lz, V_L, V_R, eta, energy, kx, ky):
+    """tau of grid.f90:335-385 for a z-only potential (G diagonal in modes)."""
+    Gf, _, sL, sR = closed_form_modes(nx, ny, vz, Lx, Ly, Lz, V_L, V_R, eta, energy, kx, ky)
+    return float(np.sum(sL * sR * np.abs(Gf) ** 2))
+
+
+lapack_path = _build.lapack_path
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "liboracle.so")

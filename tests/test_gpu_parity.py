@@ -1,0 +1,177 @@
+"""GPU parity: the CUDA path (through the C ABI) against the CPU oracle.
+
+Tolerance: FP64 mode must match within 1e-9 relative (normwise for matrices,
+elementwise with a 1e-12 absolute floor for tau).
+"""
+import numpy as np
+import pytest
+
+from negftrans_b200 import HARTREE, workloads as W
+from negftrans_b200 import prepare as P
+from negftrans_b200.negf import Engine, GreensFunction_tri_solver
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-9
+
+
+def rel_err(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def oracle_problem(O, pr):
+    a = pr.atomic
+    return O.Problem(pr.nx, pr.ny, pr.vhat, a.LX, a.LY, a.LZ, a.V_L, a.V_R, a.ETA, pr.kpoint)
+
+
+def small_problem(encut_meV=1.2, nz=16, nk=1, grid=32, V_L=0.0, V_R=0.0, seed=1000):
+    V = W.MSTAR * W.qpc_potential(grid, grid, nz, 100.0, nz * 1.0, 0.050, 15.0, nz / 10.0,
+                                  disorder=0.002, seed=seed)
+    d = W._deck(nz * 10.0, encut_meV * 1e-3, 30.0, 16, nk=nk)
+    d.V_L, d.V_R = V_L, V_R
+    return P.prepare(d, V)
+
+
+def random_blocks(N, Nz, seed, shift=4.0):
+    rng = np.random.default_rng(seed)
+    D = rng.standard_normal((N, N, Nz)) + 1j * rng.standard_normal((N, N, Nz))
+    for k in range(Nz):
+        D[:, :, k] += shift * np.sqrt(N) * np.eye(N)
+    return np.asfortranarray(D)
+
+
+@pytest.mark.parametrize("N,Nz", [(1, 2), (5, 2), (5, 7), (33, 3), (64, 4), (70, 5), (129, 3)])
+def test_tri_solve_random(oracle, N, Nz):
+    D = random_blocks(N, Nz, seed=N * 100 + Nz)
+    ref, rinfo = oracle.tri_solver(D, "DFL")
+    got, info = GreensFunction_tri_solver(D, "DFL")
+    assert info == rinfo == 0
+    for k in "DFL":
+        assert rel_err(got[k], ref[k]) < RTOL, k
+
+
+@pytest.mark.parametrize("N,Nz", [(300, 3), (600, 2)])
+def test_tri_solve_wide_variants(oracle, N, Nz):
+    """N > 256 runs the 2- and 4-rows-per-thread kernel variants."""
+    D = random_blocks(N, Nz, seed=N)
+    ref, _ = oracle.tri_solver(D, "DF")
+    got, info = GreensFunction_tri_solver(D, "DF")
+    assert info == 0
+    for k in "DF":
+        assert rel_err(got[k], ref[k]) < RTOL, k
+
+
+def test_tri_solve_partial_dfl_zero_fills(oracle):
+    D = random_blocks(6, 4, seed=3)
+    got, _ = GreensFunction_tri_solver(D, "F")
+    ref, _ = oracle.tri_solver(D, "F")
+    assert set(got) == {"F"}
+    assert rel_err(got["F"], ref["F"]) < RTOL
+
+
+def test_tri_solve_singular_reports_info():
+    D = random_blocks(4, 3, seed=5)
+    D[:, :, 2] = 0.0  # inv(D_Nz) of a zero block
+    _, info = GreensFunction_tri_solver(D, "F")
+    assert info > 0
+
+
+def test_tri_solve_physical_blocks(oracle):
+    pr = small_problem()
+    p = oracle_problem(oracle, pr)
+    H = oracle.hamiltonian(p, 0.0, 0.0)
+    D = oracle.e_minus_h(p, H, 0.067 * 0.012 / HARTREE + 1j * pr.atomic.ETA, 0.0, 0.0)
+    ref, _ = oracle.tri_solver(D, "DFL")
+    got, info = GreensFunction_tri_solver(D, "DFL")
+    assert info == 0
+    for k in "DFL":
+        assert rel_err(got[k], ref[k]) < RTOL, k
+
+
+@pytest.mark.parametrize("nk", [1, 2])
+def test_transmission_small(oracle, nk):
+    pr = small_problem(nk=nk)
+    E = P.transmission_energies(pr.atomic, 16)
+    tau_ref, _ = oracle.transmission_jobs(oracle_problem(oracle, pr), E, nthreads=4)
+    with Engine(*pr.engine_args()) as eng:
+        tau, info = eng.transmission(E)
+    assert info == 0
+    np.testing.assert_allclose(tau, tau_ref, rtol=RTOL, atol=1e-12)
+
+
+def test_transmission_leads_differ(oracle):
+    """V_L != V_R exercises the gamma_L-on-rows quirk of grid.f90:363-374."""
+    pr = small_problem(V_L=0.067 * 0.002, V_R=0.067 * 0.005)
+    E = P.transmission_energies(pr.atomic, 16)
+    tau_ref, _ = oracle.transmission_jobs(oracle_problem(oracle, pr), E, nthreads=4)
+    with Engine(*pr.engine_args()) as eng:
+        tau, _ = eng.transmission(E)
+    np.testing.assert_allclose(tau, tau_ref, rtol=RTOL, atol=1e-12)
+
+
+def test_transmission_n69_subset(oracle):
+    w = W.config("qpc_n69")
+    pr = P.prepare(w.deck, w.V_eV)
+    E = P.transmission_energies(pr.atomic, 512)[::64]
+    tau_ref, _ = oracle.transmission_jobs(oracle_problem(oracle, pr), E, nthreads=8)
+    with Engine(*pr.engine_args()) as eng:
+        tau, info = eng.transmission(E)
+    assert info == 0
+    np.testing.assert_allclose(tau, tau_ref, rtol=RTOL, atol=1e-12)
+
+
+def test_transmission_closed_form(oracle):
+    """z-only potential: every mode decouples (long-double three-term recursion)."""
+    nz, grid = 24, 32
+    z = (np.arange(nz) + 0.5 - nz / 2)
+    vz = 0.067 * 0.02 * np.exp(-z ** 2 / 18.0)
+    V = np.asfortranarray(np.broadcast_to(vz[None, None, :], (grid, grid, nz)))
+    d = W._deck(nz * 10.0, 1.2e-3, 30.0, 16)
+    pr = P.prepare(d, V)
+    a = pr.atomic
+    E = P.transmission_energies(a, 16)
+    with Engine(*pr.engine_args()) as eng:
+        tau, _ = eng.transmission(E)
+    vz00 = pr.vhat[pr.NGX, pr.NGY, :]
+    cf = [oracle.closed_form_tau(pr.nx, pr.ny, vz00, a.LX, a.LY, a.LZ, a.V_L, a.V_R, a.ETA, e, 0, 0)
+          for e in E]
+    np.testing.assert_allclose(tau, cf, rtol=1e-9, atol=1e-12)
+
+
+def test_transmission_many_jobs_and_determinism(oracle):
+    """More jobs than SMs (persistent loop) and bitwise repeatability."""
+    pr = small_problem(encut_meV=0.6, nz=6)
+    E = P.transmission_energies(pr.atomic, 16)
+    E = np.linspace(E[0], 0.067 * 0.03 / HARTREE, 333)
+    tau_ref, _ = oracle.transmission_jobs(oracle_problem(oracle, pr), E, nthreads=8)
+    with Engine(*pr.engine_args()) as eng:
+        t1, _ = eng.transmission(E)
+        t2, _ = eng.transmission(E)
+    np.testing.assert_allclose(t1, tau_ref, rtol=RTOL, atol=1e-12)
+    assert np.array_equal(t1, t2)
+
+
+def test_density_small(oracle):
+    pr = small_problem(nz=8, nk=2)
+    a = pr.atomic
+    n_c, n_l = 6, 5
+    dm_ref, _ = oracle.density_jobs(oracle_problem(oracle, pr), n_c, n_l, pr.min_V, a.MU, a.GAP,
+                                    a.TEMPERATURE, nthreads=4)
+    with Engine(*pr.engine_args()) as eng:
+        dm, info = eng.equilibrium_density(n_c, n_l, pr.min_V, a.MU, a.GAP, a.TEMPERATURE)
+    assert info == 0
+    assert rel_err(dm, dm_ref) < RTOL
+
+
+def test_ldos_small(oracle):
+    pr = small_problem(nz=8, nk=2)
+    p = oracle_problem(oracle, pr)
+    e_lo, e_hi, n_e = 0.0, 0.067 * 0.03 / HARTREE, 5
+    with Engine(*pr.engine_args()) as eng:
+        got, info = eng.ldos_matrix(e_lo, e_hi, n_e, i_e0=1, n_chunk=3)
+    assert info == 0
+    for o in range(3):
+        ref = np.zeros((pr.N, pr.N, pr.Nz), np.complex128, order="F")
+        for ik in range(len(pr.kpoint)):
+            oracle.local_density_of_state(p, ik + 1, o + 2, n_e, e_lo, e_hi, ref)
+        assert rel_err(got[o], ref) < RTOL
