@@ -40,6 +40,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="qpc_disorder_n221")
     ap.add_argument("--batch", type=int, default=296, help="energies per step and GPU")
+    ap.add_argument("--nz", type=int, default=0,
+                    help="profiling only: rebuild the workload with this many slices (same dz)")
     ap.add_argument("--cpu-threads", type=int, default=0, help="0 = all host cores (max 16)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -196,7 +198,7 @@ def run_ours(args):
     from negftrans_b200 import prepare as P, workloads as W
     from negftrans_b200.negf import Engine
 
-    w = W.config(args.workload)
+    w = W.config(args.workload, nz=args.nz or None)
     pr = P.prepare(w.deck, w.V_eV)
     E_all = P.transmission_energies(pr.atomic, w.n_energy)
     B = args.batch
@@ -268,7 +270,7 @@ def run_ours(args):
                          "frac": achieved / peak, "traffic": None,
                          "peak_source": "measured in-run: cuBLAS FP64 GEMM 8192^3 (MEASURED_PEAKS.json "
                                         "has no FP64 figure)",
-                         "flops_per_launch": fl, "kernel": "k_transmission<32,1>"},
+                         "flops_per_launch": fl, "kernel": "k_transmission<16,1,2>"},
             "gpu_launches": 2 * args.steps,
             "clocks": cs,
             "singular_jobs": info_bad,

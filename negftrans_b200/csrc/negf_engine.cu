@@ -36,8 +36,8 @@ struct RgfJob {
 };
 
 // ------------------------------------------------------------------ kernels
-template <int NB, int RPT>
-__global__ void __launch_bounds__(NT, 1)
+template <int NB, int RPT, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
     k_transmission(Geo g, const double *__restrict__ energies, int nE, int njobs, double2 *ws,
                    size_t wstride, double *tau_jobs, int *info_jobs) {
     extern __shared__ __align__(256) unsigned char smem[];
@@ -109,8 +109,8 @@ enum { WANT_D = 1, WANT_F = 2, WANT_L = 4 };
 // One job per CTA.  slab (Nz blocks, leading dimension ld) first receives
 // the generator_r blocks; with WANT_D it ends up holding G_kk in block k.
 // out_first / out_last (leading dimension N) receive G_k1 / G_kNz.
-template <int NB, int RPT>
-__global__ void __launch_bounds__(NT, 1)
+template <int NB, int RPT, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
     k_rgf_slab(Geo g, const RgfJob *__restrict__ jobs, int njobs, const double2 *__restrict__ Dexp,
                double2 *ws, size_t wstride, double2 *slabs, size_t sstride, int want,
                double2 *out_first, double2 *out_last, int *info_jobs) {
@@ -333,17 +333,18 @@ int ensure_jobs(negf_ctx *c, int nE, int njobs) {
     return 0;
 }
 
-// Kernel variants by basis size: (panel width NB, rows per thread RPT).
-enum Variant { V32x1 = 0, V16x2 = 1, V8x4 = 2, VNONE = 3 };
+// Kernel variants by basis size: (panel width NB, rows per thread RPT,
+// CTAs per SM).  Up to 256 plane waves two CTAs share an SM.
+enum Variant { V16x1 = 0, V16x2 = 1, V8x4 = 2, VNONE = 3 };
 Variant pick_variant(int N) {
-    if (N <= NT) return V32x1;
+    if (N <= NT) return V16x1;
     if (N <= 2 * NT) return V16x2;
     if (N <= 4 * NT) return V8x4;
     return VNONE;
 }
 size_t variant_smem(Variant v, int N) {
     switch (v) {
-        case V32x1: return smem_bytes<32>(N);
+        case V16x1: return smem_bytes<16>(N);
         case V16x2: return smem_bytes<16>(N);
         case V8x4: return smem_bytes<8>(N);
         default: return 0;
@@ -351,9 +352,26 @@ size_t variant_smem(Variant v, int N) {
 }
 
 template <typename K>
-int prep_kernel(K kern, size_t smem) {
+int prep_kernel(K kern, size_t smem, int *occ) {
     CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int o = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, NT, smem));
+    *occ = o > 0 ? o : 1;
     return 0;
+}
+
+// CTAs of the transmission kernel resident per SM for this N.
+int resident_ctas(int N) {
+    const Variant v = pick_variant(N);
+    const size_t smem = variant_smem(v, N);
+    int occ = 1;
+    switch (v) {
+        case V16x1: prep_kernel(k_transmission<16, 1, 2>, smem, &occ); break;
+        case V16x2: prep_kernel(k_transmission<16, 2, 1>, smem, &occ); break;
+        case V8x4: prep_kernel(k_transmission<8, 4, 1>, smem, &occ); break;
+        default: break;
+    }
+    return occ;
 }
 
 int transmission_launch(negf_ctx *c, const double *d_E, int nE, double *d_tau, double *d_tau_jobs,
@@ -362,24 +380,28 @@ int transmission_launch(negf_ctx *c, const double *d_E, int nE, double *d_tau, d
     const Variant v = pick_variant(c->N);
     if (v == VNONE) return NEGF_ERR_UNSUPPORTED;
     const size_t smem = variant_smem(v, c->N);
-    const int grid = std::min(njobs, c->num_sms);
+    int occ = 1, rc = 0;
+    switch (v) {
+        case V16x1: rc = prep_kernel(k_transmission<16, 1, 2>, smem, &occ); break;
+        case V16x2: rc = prep_kernel(k_transmission<16, 2, 1>, smem, &occ); break;
+        default: rc = prep_kernel(k_transmission<8, 4, 1>, smem, &occ); break;
+    }
+    if (rc) return rc;
+    const int grid = std::min(njobs, c->num_sms * occ);
     const size_t wstride = 4 * (size_t)c->ld * c->N;
-    int rc = ensure_ws(c, sizeof(double2) * wstride * grid);
+    rc = ensure_ws(c, sizeof(double2) * wstride * grid);
     if (rc) return rc;
     Geo g = make_geo(c);
     double2 *ws = (double2 *)c->d_ws;
     switch (v) {
-        case V32x1:
-            if ((rc = prep_kernel(k_transmission<32, 1>, smem))) return rc;
-            k_transmission<32, 1><<<grid, NT, smem, st>>>(g, d_E, nE, njobs, ws, wstride, d_tau_jobs, d_info);
+        case V16x1:
+            k_transmission<16, 1, 2><<<grid, NT, smem, st>>>(g, d_E, nE, njobs, ws, wstride, d_tau_jobs, d_info);
             break;
         case V16x2:
-            if ((rc = prep_kernel(k_transmission<16, 2>, smem))) return rc;
-            k_transmission<16, 2><<<grid, NT, smem, st>>>(g, d_E, nE, njobs, ws, wstride, d_tau_jobs, d_info);
+            k_transmission<16, 2, 1><<<grid, NT, smem, st>>>(g, d_E, nE, njobs, ws, wstride, d_tau_jobs, d_info);
             break;
         default:
-            if ((rc = prep_kernel(k_transmission<8, 4>, smem))) return rc;
-            k_transmission<8, 4><<<grid, NT, smem, st>>>(g, d_E, nE, njobs, ws, wstride, d_tau_jobs, d_info);
+            k_transmission<8, 4, 1><<<grid, NT, smem, st>>>(g, d_E, nE, njobs, ws, wstride, d_tau_jobs, d_info);
             break;
     }
     CK(cudaGetLastError());
@@ -398,21 +420,22 @@ int slab_launch(negf_ctx *c, const Geo &g, const RgfJob *d_jobs, int njobs, cons
     int rc = ensure_ws(c, sizeof(double2) * wstride * njobs);
     if (rc) return rc;
     double2 *ws = (double2 *)c->d_ws;
+    int occ = 1;
     switch (v) {
-        case V32x1:
-            if ((rc = prep_kernel(k_rgf_slab<32, 1>, smem))) return rc;
-            k_rgf_slab<32, 1><<<njobs, NT, smem, st>>>(g, d_jobs, njobs, d_D, ws, wstride, d_slabs, sstride,
-                                                        want, d_first, d_last, d_info);
+        case V16x1:
+            if ((rc = prep_kernel(k_rgf_slab<16, 1, 2>, smem, &occ))) return rc;
+            k_rgf_slab<16, 1, 2><<<njobs, NT, smem, st>>>(g, d_jobs, njobs, d_D, ws, wstride, d_slabs, sstride,
+                                                           want, d_first, d_last, d_info);
             break;
         case V16x2:
-            if ((rc = prep_kernel(k_rgf_slab<16, 2>, smem))) return rc;
-            k_rgf_slab<16, 2><<<njobs, NT, smem, st>>>(g, d_jobs, njobs, d_D, ws, wstride, d_slabs, sstride,
-                                                        want, d_first, d_last, d_info);
+            if ((rc = prep_kernel(k_rgf_slab<16, 2, 1>, smem, &occ))) return rc;
+            k_rgf_slab<16, 2, 1><<<njobs, NT, smem, st>>>(g, d_jobs, njobs, d_D, ws, wstride, d_slabs, sstride,
+                                                           want, d_first, d_last, d_info);
             break;
         default:
-            if ((rc = prep_kernel(k_rgf_slab<8, 4>, smem))) return rc;
-            k_rgf_slab<8, 4><<<njobs, NT, smem, st>>>(g, d_jobs, njobs, d_D, ws, wstride, d_slabs, sstride,
-                                                       want, d_first, d_last, d_info);
+            if ((rc = prep_kernel(k_rgf_slab<8, 4, 1>, smem, &occ))) return rc;
+            k_rgf_slab<8, 4, 1><<<njobs, NT, smem, st>>>(g, d_jobs, njobs, d_D, ws, wstride, d_slabs, sstride,
+                                                          want, d_first, d_last, d_info);
             break;
     }
     CK(cudaGetLastError());
@@ -446,7 +469,7 @@ int slab_jobs_in_flight(negf_ctx *c, size_t per_job_bytes, int njobs) {
     free_b += c->ws_bytes;  // the workspace is re-sized for the chunk
     const size_t budget = (size_t)(0.8 * (double)free_b);
     size_t fit = per_job_bytes ? budget / per_job_bytes : (size_t)njobs;
-    int b = (int)std::min<size_t>(fit, (size_t)std::min(njobs, c->num_sms));
+    int b = (int)std::min<size_t>(fit, (size_t)std::min(njobs, c->num_sms * resident_ctas(c->N)));
     return std::max(b, 0);
 }
 

@@ -20,9 +20,14 @@ namespace negf {
 
 constexpr int NT = 256;          // threads per CTA
 constexpr int NWARP = NT / 32;
-constexpr int TM = 64;           // GEMM tile rows
-constexpr int TN = 64;           // GEMM tile columns
-constexpr int TK = 16;           // GEMM k chunk
+// Complex FP64 GEMMs run on the FP64 tensor cores (DMMA, mma.m8n8k4.f64):
+// a CTA tile of CM x CN outputs is split into 2 x 4 warp tiles of WM x WN
+// (4 x 2 m8n8 tiles each); warps whose tile lies outside the matrix skip
+// their MMAs, so the padding waste is at 8-row granularity only.
+constexpr int CM = 64, CN = 64;  // CTA tile
+constexpr int WM = 32, WN = 16;  // warp tile
+constexpr int KC = 16;           // k chunk staged per pipeline step
+constexpr int BP = CN + 1;       // padded row of a k-major B tile (bank spread)
 
 // ------------------------------------------------------------ complex FP64
 __device__ __forceinline__ double2 zmake(double x, double y) { return make_double2(x, y); }
@@ -119,7 +124,7 @@ struct Smem {
     double2 *srow;  // [NBMAX] pivot row of the panel step
     Red *red;       // [NWARP]
     double *fred;   // [NWARP] float reductions
-    double2 *big;   // union: GJ panel sW[NB][ldw] + sB[NB][TN] | GEMM stages
+    double2 *big;   // union: GJ panel sW[NB][ldw] + sB[NB][BP] | GEMM stages
     int ldw;
 };
 
@@ -127,9 +132,9 @@ __host__ __device__ inline int round_up(int a, int b) { return (a + b - 1) / b *
 
 template <int NB>
 __host__ __device__ inline size_t smem_bytes(int N) {
-    int ldw = round_up(N, TM);
-    size_t big = (size_t)NB * ldw + (size_t)NB * TN;
-    size_t gemm = 2 * (size_t)TK * (TM + TN);
+    int ldw = round_up(N, CM);
+    size_t big = (size_t)NB * ldw + (size_t)NB * BP;
+    size_t gemm = 2 * (size_t)KC * (CM + BP);
     if (gemm > big) big = gemm;
     size_t b = 0;
     b += 5 * (size_t)round_up(N, 4) * sizeof(int);
@@ -160,7 +165,7 @@ __device__ inline Smem carve(unsigned char *base, int N) {
     size_t off = (size_t)((unsigned char *)(s.fred + NWARP) - base);
     off = (off + 255) / 256 * 256;
     s.big = (double2 *)(base + off);
-    s.ldw = round_up(N, TM);
+    s.ldw = round_up(N, CM);
     return s;
 }
 
@@ -182,36 +187,46 @@ __device__ inline void job_vectors(const Geo &g, const Smem &s, double2 E, doubl
 }
 
 // M = D_k - inv(prev), where inv(prev)(i,j) = R(prow[i], iprow[j]).
-// D_k is generated from V_reciprocal_all (generated = true) or read from an
-// explicit (N,N,Nz) array with leading dimension N (generated = false).
+// D_k is generated from V_reciprocal_all (Dexp == nullptr) or read from an
+// explicit (N,N,Nz) array with leading dimension N.  Four columns per pass
+// keep four independent gathers in flight per thread.
+__device__ inline double2 d_element(const Geo &g, const Smem &s, const double2 *vs, int k, double2 E,
+                                    int ik, int i, int j, int nxj, int nyj) {
+    const int dx = s.nx[i] - nxj + g.ngx, dy = s.ny[i] - nyj + g.ngy;
+    const double2 v = __ldg(vs + dx + g.W * dy);
+    if (i != j) return make_double2(-v.x * g.c2, -v.y * g.c2);
+    const double ax = g.ax[ik * g.N + i], ay = g.ay[ik * g.N + i];
+    const double hx = v.x + (ax * ax + ay * ay) / 2;
+    double2 d = make_double2((-hx + E.x) * g.c2 - 2.0, (-v.y + E.y) * g.c2);
+    if (k == 0) d = zadd(d, s.sigL[i]);
+    if (k == g.Nz - 1) d = zadd(d, s.sigR[i]);
+    return d;
+}
+
 __device__ inline void form_block(double2 *__restrict__ M, const Geo &g, const Smem &s, int k,
                                   double2 E, int ik, const double2 *__restrict__ R,
                                   const double2 *__restrict__ Dexp) {
     const int N = g.N, ld = g.ld;
     const double2 *vs = g.vhat ? g.vhat + (size_t)g.W * g.H * k : nullptr;
     const double2 *Dk = Dexp ? Dexp + (size_t)N * N * k : nullptr;
-    for (int j = 0; j < N; ++j) {
-        const int nxj = s.nx[j], nyj = s.ny[j];
-        const int jc = R ? s.iprow[j] : 0;
+    for (int j0 = 0; j0 < N; j0 += 4) {
         for (int i = threadIdx.x; i < N; i += NT) {
-            double2 d;
-            if (Dk) {
-                d = Dk[i + (size_t)N * j];
-            } else {
-                const int dx = s.nx[i] - nxj + g.ngx, dy = s.ny[i] - nyj + g.ngy;
-                const double2 v = __ldg(vs + dx + g.W * dy);
-                if (i != j) {
-                    d = make_double2(-v.x * g.c2, -v.y * g.c2);
-                } else {
-                    const double ax = g.ax[ik * N + i], ay = g.ay[ik * N + i];
-                    const double hx = v.x + (ax * ax + ay * ay) / 2;
-                    d = make_double2((-hx + E.x) * g.c2 - 2.0, (-v.y + E.y) * g.c2);
-                    if (k == 0) d = zadd(d, s.sigL[i]);
-                    if (k == g.Nz - 1) d = zadd(d, s.sigR[i]);
+            double2 d[4], r[4];
+            const int pi = R ? s.prow[i] : 0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int j = j0 + q;
+                d[q] = make_double2(0.0, 0.0);
+                r[q] = make_double2(0.0, 0.0);
+                if (j < N) {
+                    if (Dk) d[q] = Dk[i + (size_t)N * j];
+                    else d[q] = d_element(g, s, vs, k, E, ik, i, j, s.nx[j], s.ny[j]);
+                    if (R) r[q] = R[pi + (size_t)ld * s.iprow[j]];
                 }
             }
-            if (R) d = zsub(d, R[s.prow[i] + (size_t)ld * jc]);
-            M[i + (size_t)ld * j] = d;
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (j0 + q < N) M[i + (size_t)ld * (j0 + q)] = zsub(d[q], r[q]);
         }
     }
 }
@@ -229,6 +244,49 @@ __device__ inline void unpermute(double2 *__restrict__ out, int ldo, const doubl
 }
 
 // ------------------------------------------------------------------ GEMM
+// D(8x8) += A(8x4) * B(4x8) on the FP64 tensor cores.  Fragments (PTX ISA,
+// mma.m8n8k4 .f64): A row = lane>>2, k = lane&3; B k = lane&3, col = lane>>2;
+// C rows lane>>2, cols 2*(lane&3) + {0,1}.
+__device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+// Complex accumulators of one warp tile: 4 x 2 m8n8 tiles, 2 elements each.
+struct WarpAcc {
+    double re[4][2][2], im[4][2][2];
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int m = 0; m < 4; ++m)
+#pragma unroll
+            for (int n = 0; n < 2; ++n)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) re[m][n][e] = im[m][n][e] = 0.0;
+    }
+    // acc += A(k-major, lda) * B(k-major, ldb) over 4 k values starting at kb.
+    __device__ __forceinline__ void step(const double2 *sA, int lda, int arow, const double2 *sB, int ldb,
+                                         int bcol, int kb, int lane) {
+        const int kk = kb + (lane & 3), g = lane >> 2;
+        double2 a[4], b[2];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) a[m] = sA[kk * lda + arow + 8 * m + g];
+#pragma unroll
+        for (int n = 0; n < 2; ++n) b[n] = sB[kk * ldb + bcol + 8 * n + g];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const double nai = -a[m].y;
+#pragma unroll
+            for (int n = 0; n < 2; ++n) {
+                dmma(re[m][n][0], re[m][n][1], a[m].x, b[n].x);
+                dmma(im[m][n][0], im[m][n][1], a[m].x, b[n].y);
+                dmma(re[m][n][0], re[m][n][1], nai, b[n].y);
+                dmma(im[m][n][0], im[m][n][1], a[m].y, b[n].x);
+            }
+        }
+    }
+};
+
 // C(i,j) = sum_k A(i, acol[k]) * B(k, bcol[j]) for one CTA, complex FP64.
 // acol/bcol == nullptr means identity.  Modes of the epilogue:
 enum GemmOut { GEMM_STORE = 0, GEMM_STORE_NEG = 1, GEMM_TAU = 2, GEMM_STORE_ADD_EYE = 3 };
@@ -248,86 +306,79 @@ struct GemmArgs {
 // Returns, for GEMM_TAU, this thread's partial sum of
 // gL[i] * gR[j] * |(C(i,j)*2)*delta^2|^2 (grid.f90:362-383 after negf.f90:159-165).
 __device__ inline double cta_gemm(const GemmArgs &a, const Smem &s, int mode, double delta) {
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-    double2 *sA = s.big;                 // [2][TK][TM]
-    double2 *sB = s.big + 2 * TK * TM;   // [2][TN][TK]
-    const int ntm = (a.M + TM - 1) / TM, ntn = (a.Ncol + TN - 1) / TN;
-    const int nkc = (a.K + TK - 1) / TK;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm0 = (warp & 1) * WM, wn0 = (warp >> 1) * WN;
+    double2 *sA = s.big;                 // [2][KC][CM]
+    double2 *sB = s.big + 2 * KC * CM;   // [2][KC][BP]
+    const int ntm = (a.M + CM - 1) / CM, ntn = (a.Ncol + CN - 1) / CN;
+    const int nkc = (a.K + KC - 1) / KC;
     double tau = 0.0;
     for (int t = 0; t < ntm * ntn; ++t) {
-        const int I0 = (t % ntm) * TM, J0 = (t / ntm) * TN;
-        double2 acc[4][4];
-#pragma unroll
-        for (int p = 0; p < 4; ++p)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) acc[p][q] = make_double2(0.0, 0.0);
-
+        const int I0 = (t % ntm) * CM, J0 = (t / ntm) * CN;
+        const bool active = (I0 + wm0 < a.M) && (J0 + wn0 < a.Ncol);
+        WarpAcc acc;
+        acc.zero();
         auto load_stage = [&](int st, int k0) {
+            double2 *dA = sA + st * KC * CM;
+            double2 *dB = sB + st * KC * BP;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
+            for (int q = 0; q < (KC * CM) / NT; ++q) {
                 const int e = tid + NT * q;
-                // A tile: e -> (kk = e / TM, ii = e % TM)
-                {
-                    const int kk = e / TM, ii = e % TM;
-                    const int k = k0 + kk, i = I0 + ii;
-                    const bool v = (k < a.K) && (i < a.M);
-                    const int kc = v ? (a.acol ? a.acol[k] : k) : 0;
-                    cp_async16(sA + st * TK * TM + kk * TM + ii, a.A + (v ? (i + (size_t)a.lda * kc) : 0), v);
-                }
-                // B tile: e -> (jj = e / TK, kk = e % TK), stored [jj][kk]
-                {
-                    const int jj = e / TK, kk = e % TK;
-                    const int k = k0 + kk, j = J0 + jj;
-                    const bool v = (k < a.K) && (j < a.Ncol);
-                    const int jc = v ? (a.bcol ? a.bcol[j] : j) : 0;
-                    cp_async16(sB + st * TN * TK + jj * TK + kk, a.B + (v ? (k + (size_t)a.ldb * jc) : 0), v);
-                }
+                const int kk = e / CM, ii = e % CM;
+                const int k = k0 + kk, i = I0 + ii;
+                const bool v = (k < a.K) && (i < a.M);
+                const int kc = v ? (a.acol ? a.acol[k] : k) : 0;
+                cp_async16(dA + kk * CM + ii, a.A + (v ? (i + (size_t)a.lda * kc) : 0), v);
+            }
+#pragma unroll
+            for (int q = 0; q < (KC * CN) / NT; ++q) {
+                const int e = tid + NT * q;
+                const int kk = e % KC, jj = e / KC;
+                const int k = k0 + kk, j = J0 + jj;
+                const bool v = (k < a.K) && (j < a.Ncol);
+                const int jc = v ? (a.bcol ? a.bcol[j] : j) : 0;
+                cp_async16(dB + kk * BP + jj, a.B + (v ? (k + (size_t)a.ldb * jc) : 0), v);
             }
             cp_async_commit();
         };
-
         load_stage(0, 0);
         for (int c = 0; c < nkc; ++c) {
             if (c + 1 < nkc) {
-                load_stage((c + 1) & 1, (c + 1) * TK);
+                load_stage((c + 1) & 1, (c + 1) * KC);
                 cp_async_wait<1>();
             } else {
                 cp_async_wait<0>();
             }
             __syncthreads();
-            const double2 *cA = sA + (c & 1) * TK * TM;
-            const double2 *cB = sB + (c & 1) * TN * TK;
-#pragma unroll 4
-            for (int kk = 0; kk < TK; ++kk) {
-                double2 av[4], bv[4];
+            if (active) {
+                const double2 *cA = sA + (c & 1) * KC * CM;
+                const double2 *cB = sB + (c & 1) * KC * BP;
 #pragma unroll
-                for (int p = 0; p < 4; ++p) av[p] = cA[kk * TM + tx + 16 * p];
-#pragma unroll
-                for (int q = 0; q < 4; ++q) bv[q] = cB[(ty + 16 * q) * TK + kk];
-#pragma unroll
-                for (int p = 0; p < 4; ++p)
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) acc[p][q] = zfma(av[p], bv[q], acc[p][q]);
+                for (int kb = 0; kb < KC; kb += 4) acc.step(cA, CM, wm0, cB, BP, wn0, kb, lane);
             }
             __syncthreads();
         }
+        if (active) {
 #pragma unroll
-        for (int p = 0; p < 4; ++p) {
-            const int i = I0 + tx + 16 * p;
+            for (int m = 0; m < 4; ++m) {
+                const int i = I0 + wm0 + 8 * m + (lane >> 2);
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int j = J0 + ty + 16 * q;
-                if (i < a.M && j < a.Ncol) {
-                    double2 v = acc[p][q];
-                    if (mode == GEMM_TAU) {
-                        const double gx = v.x * 2.0 * (delta * delta), gy = v.y * 2.0 * (delta * delta);
-                        tau += s.gL[i] * s.gR[j] * (gx * gx + gy * gy);
-                    } else {
-                        if (mode == GEMM_STORE_NEG) v = make_double2(-v.x, -v.y);
-                        if (mode == GEMM_STORE_ADD_EYE && i == j) v.x += 1.0;
-                        a.C[i + (size_t)a.ldc * j] = v;
+                for (int n = 0; n < 2; ++n)
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        const int j = J0 + wn0 + 8 * n + 2 * (lane & 3) + e;
+                        if (i < a.M && j < a.Ncol) {
+                            double2 v = make_double2(acc.re[m][n][e], acc.im[m][n][e]);
+                            if (mode == GEMM_TAU) {
+                                const double gx = v.x * 2.0 * (delta * delta), gy = v.y * 2.0 * (delta * delta);
+                                tau += s.gL[i] * s.gR[j] * (gx * gx + gy * gy);
+                            } else {
+                                if (mode == GEMM_STORE_NEG) v = make_double2(-v.x, -v.y);
+                                if (mode == GEMM_STORE_ADD_EYE && i == j) v.x += 1.0;
+                                a.C[i + (size_t)a.ldc * j] = v;
+                            }
+                        }
                     }
-                }
             }
         }
     }
@@ -351,64 +402,68 @@ __device__ inline double block_sum(double v, const Smem &s) {
 // ----------------------------------------------------- Gauss-Jordan inverse
 // Rank-nbe update of every column outside the panel [k0, k0+nbe):
 //   A(:, j) = mask(A(:, j)) + W * A_old(prow[k0:k0+nbe], j)
-// where W = the panel after elimination (held in sW) and mask zeroes the
-// panel's pivot rows.  See the derivation in the file header.
+// where W = the panel after elimination (held in sW, k-major) and mask zeroes
+// the panel's pivot rows.  W and the gathered pivot rows feed DMMA tiles.
 template <int NB>
 __device__ inline void trailing_update(double2 *__restrict__ A, int N, int ld, int k0, int nbe,
                                        const Smem &s) {
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm0 = (warp & 1) * WM, wn0 = (warp >> 1) * WN;
     const int nrest = N - nbe;
     const int ldw = s.ldw;
     const double2 *sW = s.big;
-    double2 *sB = s.big + NB * ldw;
-    for (int J0 = 0; J0 < nrest; J0 += TN) {
-        for (int e = tid; e < NB * TN; e += NT) {
-            const int kk = e / TN, jt = e % TN, jr = J0 + jt;
+    double2 *sB = s.big + NB * ldw;  // [NB][BP]
+    for (int J0 = 0; J0 < nrest; J0 += CN) {
+        for (int e = tid; e < NB * CN; e += NT) {
+            const int kk = e / CN, jt = e % CN, jr = J0 + jt;
             double2 v = make_double2(0.0, 0.0);
             if (kk < nbe && jr < nrest) {
                 const int j = jr < k0 ? jr : jr + nbe;
                 v = A[s.prow[k0 + kk] + (size_t)ld * j];
             }
-            sB[e] = v;
+            sB[kk * BP + jt] = v;
         }
         __syncthreads();
-        int col[4];
-        bool cv[4];
+        if (J0 + wn0 < nrest) {
+            int col[2][2];
+            bool cv[2][2];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int jr = J0 + ty + 16 * q;
-            cv[q] = jr < nrest;
-            col[q] = jr < k0 ? jr : jr + nbe;
-        }
-        for (int I0 = 0; I0 < N; I0 += TM) {
-            double2 acc[4][4];
+            for (int n = 0; n < 2; ++n)
 #pragma unroll
-            for (int p = 0; p < 4; ++p) {
-                const int i = I0 + tx + 16 * p;
-                const bool rv = (i < N) && !s.inP[i];
+                for (int e = 0; e < 2; ++e) {
+                    const int jr = J0 + wn0 + 8 * n + 2 * (lane & 3) + e;
+                    cv[n][e] = jr < nrest;
+                    col[n][e] = jr < k0 ? jr : jr + nbe;
+                }
+            for (int I0 = 0; I0 < N; I0 += CM) {
+                if (I0 + wm0 >= N) break;
+                WarpAcc acc;
 #pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    acc[p][q] = (rv && cv[q]) ? A[i + (size_t)ld * col[q]] : make_double2(0.0, 0.0);
-            }
-#pragma unroll 4
-            for (int kk = 0; kk < nbe; ++kk) {
-                double2 wv[4], bv[4];
+                for (int m = 0; m < 4; ++m) {
+                    const int i = I0 + wm0 + 8 * m + (lane >> 2);
+                    const bool rv = (i < N) && !s.inP[i];
 #pragma unroll
-                for (int p = 0; p < 4; ++p) wv[p] = sW[kk * ldw + I0 + tx + 16 * p];
+                    for (int n = 0; n < 2; ++n)
 #pragma unroll
-                for (int q = 0; q < 4; ++q) bv[q] = sB[kk * TN + ty + 16 * q];
+                        for (int e = 0; e < 2; ++e) {
+                            double2 c = make_double2(0.0, 0.0);
+                            if (rv && cv[n][e]) c = A[i + (size_t)ld * col[n][e]];
+                            acc.re[m][n][e] = c.x;
+                            acc.im[m][n][e] = c.y;
+                        }
+                }
 #pragma unroll
-                for (int p = 0; p < 4; ++p)
+                for (int kb = 0; kb < NB; kb += 4) acc.step(sW, ldw, I0 + wm0, sB, BP, wn0, kb, lane);
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) acc[p][q] = zfma(wv[p], bv[q], acc[p][q]);
-            }
+                for (int m = 0; m < 4; ++m) {
+                    const int i = I0 + wm0 + 8 * m + (lane >> 2);
+                    if (i < N) {
 #pragma unroll
-            for (int p = 0; p < 4; ++p) {
-                const int i = I0 + tx + 16 * p;
-                if (i < N) {
+                        for (int n = 0; n < 2; ++n)
 #pragma unroll
-                    for (int q = 0; q < 4; ++q)
-                        if (cv[q]) A[i + (size_t)ld * col[q]] = acc[p][q];
+                            for (int e = 0; e < 2; ++e)
+                                if (cv[n][e]) A[i + (size_t)ld * col[n][e]] = make_double2(acc.re[m][n][e], acc.im[m][n][e]);
+                    }
                 }
             }
         }

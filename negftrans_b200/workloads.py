@@ -64,20 +64,26 @@ def _deck(Lz_A, encut, e_max_meV, n_e, nk=1, mu_meV=20.0, t_K=1.1605, n_circle=4
         N_line_per_eV=per_eV)
 
 
-def config(name: str) -> Workload:
-    """Named workloads with the shapes of the benchmark configurations."""
+def config(name: str, nz: int | None = None) -> Workload:
+    """Named workloads with the shapes of the benchmark configurations.
+
+    nz (profiling only) rebuilds the device with that many slices of the same
+    thickness, which scales the sweep length and nothing else."""
     if name == "qpc_n69":
         # 69 plane waves, 200 slices of 1 nm, 512 energies on [0, 30) meV, Gamma only
-        V = MSTAR * qpc_potential(64, 64, 200, 100.0, 200.0, 0.050, 15.0, 20.0)
-        return Workload(name, _deck(2000.0, 0.0033091, 30.0, 512), V, 512)
+        nz = nz or 200
+        V = MSTAR * qpc_potential(64, 64, nz, 100.0, nz * 1.0, 0.050, 15.0, 20.0)
+        return Workload(name, _deck(nz * 10.0, 0.0033091, 30.0, 512), V, 512)
     if name == "qpc_disorder_n221":
         # 221 plane waves, 800 slices of 0.5 nm, 2048 energies on [0, 40) meV, disorder 2 meV / 10 nm
-        V = MSTAR * qpc_potential(64, 64, 800, 100.0, 400.0, 0.050, 15.0, 20.0, disorder=0.002)
-        return Workload(name, _deck(4000.0, 0.0105288, 40.0, 2048), V, 2048)
+        nz = nz or 800
+        V = MSTAR * qpc_potential(64, 64, nz, 100.0, nz * 0.5, 0.050, 15.0, 20.0, disorder=0.002)
+        return Workload(name, _deck(nz * 5.0, 0.0105288, 40.0, 2048), V, 2048)
     if name == "qpc_disorder_n797":
         # 797 plane waves (128x128 grid), 400 slices of 1 nm, 1024 energies on [0, 50) meV
-        V = MSTAR * qpc_potential(128, 128, 400, 100.0, 400.0, 0.060, 20.0, 20.0, disorder=0.002)
-        return Workload(name, _deck(4000.0, 0.0385807, 50.0, 1024), V, 1024)
+        nz = nz or 400
+        V = MSTAR * qpc_potential(128, 128, nz, 100.0, nz * 1.0, 0.060, 20.0, 20.0, disorder=0.002)
+        return Workload(name, _deck(nz * 10.0, 0.0385807, 50.0, 1024), V, 1024)
     if name.startswith("small"):
         # test-sized QPC: small basis and few slices, same physics
         # small:<encut_meV>:<Nz>  (e.g. small:1.2:16)

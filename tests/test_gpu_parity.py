@@ -175,3 +175,19 @@ def test_ldos_small(oracle):
         for ik in range(len(pr.kpoint)):
             oracle.local_density_of_state(p, ik + 1, o + 2, n_e, e_lo, e_hi, ref)
         assert rel_err(got[o], ref) < RTOL
+
+
+@pytest.mark.parametrize("encut_meV,grid", [(14.5, 64), (29.0, 96)])
+def test_transmission_wide_basis(oracle, encut_meV, grid):
+    """N > 256 and N > 512: the 2- and 4-rows-per-thread kernel variants."""
+    nz = 5
+    V = W.MSTAR * W.qpc_potential(grid, grid, nz, 100.0, nz * 1.0, 0.050, 15.0, 1.0, disorder=0.002)
+    d = W._deck(nz * 10.0, encut_meV * 1e-3, 30.0, 16)
+    pr = P.prepare(d, V)
+    assert pr.N > 256
+    E = P.transmission_energies(pr.atomic, 16)[::3]
+    tau_ref, _ = oracle.transmission_jobs(oracle_problem(oracle, pr), E, nthreads=8)
+    with Engine(*pr.engine_args()) as eng:
+        tau, info = eng.transmission(E)
+    assert info == 0
+    np.testing.assert_allclose(tau, tau_ref, rtol=RTOL, atol=1e-12)
