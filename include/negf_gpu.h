@@ -35,6 +35,7 @@ extern "C" {
 #define NEGF_ERR_CUDA (-2)
 #define NEGF_ERR_NOMEM (-3)
 #define NEGF_ERR_UNSUPPORTED (-4)
+#define NEGF_ERR_TOO_LARGE (-5) /* problem needs more than the fixed scratch */
 
 #define NEGF_FP64 0 /* complex128 throughout */
 
@@ -115,6 +116,31 @@ int negf_transmission(negf_ctx *ctx, const double *energies, int32_t nE, int32_t
 int negf_transmission_device(negf_ctx *ctx, const double *d_energies, int32_t nE,
                              int32_t precision, double *d_tau, double *d_tau_jobs,
                              int32_t *d_info, void *stream);
+
+/* No counterpart in the reference.  The negf_transmission computation for
+ * callers that cannot allocate device memory: code that runs inside another
+ * framework's memory pool or allocator, or under a device memory budget that
+ * is fixed when the process starts, where a cudaMalloc in the middle of a run
+ * is not allowed.  This entry calls no cudaMalloc or cudaFree (and no
+ * allocating library routine); everything is passed in as device pointers:
+ * d_nx, d_ny [N], d_vhat (2ngx+1)*(2ngy+1)*Nz complex, d_kpt [nk][3],
+ * d_energies [nE] in, d_tau [nE] out (sum_k w_k tau), d_info [nk*nE]
+ * optional per-job LAPACK-style info.  Scalars as in negf_problem.
+ * Its working memory is one fixed 64 MiB array in the library, reserved on
+ * every GPU that loads the library until the process exits; problems whose
+ * per-job workspace (64 * roundup(N,8) * N bytes) does not fit return
+ * NEGF_ERR_TOO_LARGE, and fewer jobs run at once when only a few fit.
+ * The first call on a device looks up that array's device address; make
+ * that first call before any stream capture.  The call blocks until a check
+ * that every basis difference indexes inside the V table has run on
+ * `stream`, then enqueues the sweep on `stream` and returns.  All calls share
+ * the one array: calls whose work overlaps on the GPU (other streams, other
+ * host threads) race and must be serialised by the caller. */
+int negf_transmission_noalloc(int32_t N, int32_t Nz, int32_t ngx, int32_t ngy, const int32_t *d_nx,
+                              const int32_t *d_ny, const double *d_vhat, double Lx, double Ly,
+                              double Lz, double V_L, double V_R, double eta, int32_t nk,
+                              const double *d_kpt, const double *d_energies, int32_t nE,
+                              double *d_tau, int32_t *d_info, void *stream);
 
 /* Equilibrium_Density, negf.f90:9-113, for all (N_circle+N_line)*nk jobs
  * (main.f90:258-297).  gap = atomic%GAP (Hartree), min_v = minval(V_real)

@@ -16,13 +16,14 @@ NEGF_ERR_ARG = -1
 NEGF_ERR_CUDA = -2
 NEGF_ERR_NOMEM = -3
 NEGF_ERR_UNSUPPORTED = -4
+NEGF_ERR_TOO_LARGE = -5
 NEGF_FP64 = 0
 
 # every symbol include/negf_gpu.h declares
 EXPORTS = (
     "negf_basis_size", "negf_basis", "negf_kmesh", "negf_vhat", "negf_ctx_create",
     "negf_ctx_destroy", "negf_tri_solve", "negf_transmission", "negf_transmission_device",
-    "negf_density", "negf_ldos_matrix", "negf_ptor", "negf_version",
+    "negf_density", "negf_ldos_matrix", "negf_ptor", "negf_version", "negf_transmission_noalloc",
 )
 
 _dp = C.POINTER(C.c_double)
@@ -44,7 +45,8 @@ class Stats(C.Structure):
 class NegfError(RuntimeError):
     def __init__(self, where, code):
         names = {NEGF_ERR_ARG: "invalid argument", NEGF_ERR_CUDA: "CUDA error",
-                 NEGF_ERR_NOMEM: "out of device memory", NEGF_ERR_UNSUPPORTED: "unsupported"}
+                 NEGF_ERR_NOMEM: "out of device memory", NEGF_ERR_UNSUPPORTED: "unsupported",
+                 NEGF_ERR_TOO_LARGE: "problem larger than the fixed scratch"}
         super().__init__(f"{where}: {names.get(code, code)} ({code})")
         self.code = code
 
@@ -71,6 +73,9 @@ def lib():
     L.negf_transmission.argtypes = [C.c_void_p, _dp, C.c_int32, C.c_int32, _dp, C.POINTER(Stats)]
     L.negf_transmission_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p,
                                            C.c_void_p, C.c_void_p, C.c_void_p]
+    L.negf_transmission_noalloc.argtypes = (
+        [C.c_int32] * 4 + [C.c_void_p] * 3 + [C.c_double] * 6 + [C.c_int32] + [C.c_void_p] * 2
+        + [C.c_int32] + [C.c_void_p] * 3)
     L.negf_density.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
                                C.c_double, _dp, C.POINTER(Stats)]
     L.negf_ldos_matrix.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int32, C.c_int32,

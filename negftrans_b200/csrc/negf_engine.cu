@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "negf_gpu.h"
@@ -827,3 +828,142 @@ done:
 }
 
 }  // extern "C"
+
+// ============================================================ no-alloc entry
+// negf_transmission_noalloc: the transmission sweep for callers that cannot
+// allocate device memory (code running inside another framework's memory
+// pool or allocator, or with a fixed memory budget checked at start-up).
+// Its scratch is this file-scope array, reserved on every GPU that loads
+// the library for as long as the process lives.
+static constexpr size_t NOALLOC_SCRATCH_BYTES = (size_t)64 << 20;  // 64 MiB
+static __device__ __align__(256) double2 g_noalloc_scratch[NOALLOC_SCRATCH_BYTES / sizeof(double2)];
+
+namespace {
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex g_noalloc_mu;
+double2 *g_noalloc_base[NOALLOC_MAX_DEVICES] = {};
+
+// Device address of the scratch on the current device.  In host code the
+// array's name is only a host-side stand-in, so the address comes from
+// cudaGetSymbolAddress, once per device, with that device current.
+int noalloc_scratch(int dev, double2 **out) {
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return NEGF_ERR_ARG;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_base[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
+            cudaGetLastError();
+            return NEGF_ERR_CUDA;
+        }
+        g_noalloc_base[dev] = (double2 *)p;
+    }
+    *out = g_noalloc_base[dev];
+    return 0;
+}
+
+// ax, ay and the weights of grid.f90:258 / global k-points, into the scratch.
+__global__ void k_noalloc_kvectors(const int *__restrict__ nx, const int *__restrict__ ny,
+                                   const double *__restrict__ kpt, int N, int nk, double Lx, double Ly,
+                                   double *ax, double *ay, double *kw) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < nk) kw[t] = kpt[3 * t + 2];
+    if (t >= N * nk) return;
+    const int k = t / N, i = t - k * N;
+    ax[t] = (double)(2 * nx[i]) * PI / Lx + kpt[3 * k];
+    ay[t] = (double)(2 * ny[i]) * PI / Ly + kpt[3 * k + 1];
+}
+
+// flag = 1 if some pair difference n_i - n_j falls outside the V table.
+__global__ void k_noalloc_check(const int *__restrict__ nx, const int *__restrict__ ny, int N, int ngx,
+                                int ngy, int *flag) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < N * N; t += gridDim.x * blockDim.x) {
+        const int i = t % N, j = t / N;
+        const int dx = nx[i] - nx[j], dy = ny[i] - ny[j];
+        if (dx < -ngx || dx > ngx || dy < -ngy || dy > ngy) *flag = 1;
+    }
+}
+}  // namespace
+
+extern "C" int negf_transmission_noalloc(int32_t N, int32_t Nz, int32_t ngx, int32_t ngy,
+                                         const int32_t *d_nx, const int32_t *d_ny, const double *d_vhat,
+                                         double Lx, double Ly, double Lz, double V_L, double V_R,
+                                         double eta, int32_t nk, const double *d_kpt,
+                                         const double *d_energies, int32_t nE, double *d_tau,
+                                         int32_t *d_info, void *stream) {
+    if (N < 1 || Nz < 2 || ngx < 0 || ngy < 0 || nk < 1 || nE < 1 || !d_nx || !d_ny || !d_vhat ||
+        !d_kpt || !d_energies || !d_tau || !(Lx > 0) || !(Ly > 0) || !(Lz > 0))
+        return NEGF_ERR_ARG;
+    const Variant v = pick_variant(N);
+    if (v == VNONE) return NEGF_ERR_UNSUPPORTED;
+    cudaStream_t st = (cudaStream_t)stream;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return NEGF_ERR_CUDA;
+
+    // scratch layout: [flag | ax | ay | kw | tau_jobs] then one workspace per CTA
+    const int ld = round_up(N, 8);
+    const size_t njobs = (size_t)nE * nk;
+    const size_t head_doubles = 2 + 2 * (size_t)nk * N + nk + njobs;
+    const size_t head_bytes = (head_doubles * sizeof(double) + 255) / 256 * 256;
+    const size_t wstride = 4 * (size_t)ld * N;  // double2 per CTA
+    if (head_bytes + wstride * sizeof(double2) > NOALLOC_SCRATCH_BYTES) return NEGF_ERR_TOO_LARGE;
+    const size_t cap = (NOALLOC_SCRATCH_BYTES - head_bytes) / (wstride * sizeof(double2));
+
+    double2 *base = nullptr;
+    int rc = noalloc_scratch(dev, &base);
+    if (rc) return rc;
+    double *head = (double *)base;
+    int *flag = (int *)head;
+    double *ax = head + 2, *ay = ax + (size_t)nk * N, *kw = ay + (size_t)nk * N;
+    double *tau_jobs = kw + nk;
+    double2 *ws = (double2 *)((unsigned char *)base + head_bytes);
+
+    // the pair differences must index inside the V table (the scratch keeps
+    // the last call's contents, so the flag is cleared first)
+    int hflag = 0;
+    CK(cudaMemsetAsync(flag, 0, sizeof(int), st));
+    k_noalloc_check<<<64, 256, 0, st>>>(d_nx, d_ny, N, ngx, ngy, flag);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (hflag) return NEGF_ERR_ARG;
+
+    int sms = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const size_t smem = variant_smem(v, N);
+    int occ = 1;
+    switch (v) {
+        case V16x1: rc = prep_kernel(k_transmission<16, 1, 2>, smem, &occ); break;
+        case V16x2: rc = prep_kernel(k_transmission<16, 2, 1>, smem, &occ); break;
+        default: rc = prep_kernel(k_transmission<8, 4, 1>, smem, &occ); break;
+    }
+    if (rc) return rc;
+    const int grid = (int)std::min<size_t>(std::min<size_t>(njobs, (size_t)sms * occ), cap);
+
+    const int nkv = std::max(N * nk, nk);
+    k_noalloc_kvectors<<<(nkv + 255) / 256, 256, 0, st>>>(d_nx, d_ny, d_kpt, N, nk, Lx, Ly, ax, ay, kw);
+    CK(cudaGetLastError());
+    Geo g;
+    g.N = N; g.Nz = Nz; g.ld = ld;
+    g.ngx = ngx; g.ngy = ngy; g.W = 2 * ngx + 1; g.H = 2 * ngy + 1;
+    g.nk = nk;
+    g.vhat = (const double2 *)d_vhat; g.nx = d_nx; g.ny = d_ny;
+    g.ax = ax; g.ay = ay; g.kw = kw;
+    g.delta = Lz / Nz;
+    g.c2 = 2 * (g.delta * g.delta);
+    g.V_L = V_L; g.V_R = V_R; g.eta = eta;
+    switch (v) {
+        case V16x1:
+            k_transmission<16, 1, 2><<<grid, NT, smem, st>>>(g, d_energies, nE, (int)njobs, ws, wstride, tau_jobs, d_info);
+            break;
+        case V16x2:
+            k_transmission<16, 2, 1><<<grid, NT, smem, st>>>(g, d_energies, nE, (int)njobs, ws, wstride, tau_jobs, d_info);
+            break;
+        default:
+            k_transmission<8, 4, 1><<<grid, NT, smem, st>>>(g, d_energies, nE, (int)njobs, ws, wstride, tau_jobs, d_info);
+            break;
+    }
+    CK(cudaGetLastError());
+    k_tau_reduce<<<(nE + 127) / 128, 128, 0, st>>>(tau_jobs, kw, nE, nk, d_tau);
+    CK(cudaGetLastError());
+    return NEGF_OK;
+}
