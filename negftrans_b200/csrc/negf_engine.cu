@@ -57,22 +57,26 @@ __global__ void __launch_bounds__(NT, MINB)
         const double2 E = make_double2(e, g.eta);
         job_vectors(g, s, E, e, ik);
         __syncthreads();
+        open_rows(N, s);
+        __syncthreads();
+        const int nr = *s.nrows;
         double2 *cur = A0, *oth = A1, *P = P0, *Pn = P1;
         // generator_r(N_z-1) = inv(D_Nz)          math_kernel.f90:82
         form_block(cur, g, s, Nz - 1, E, ik, nullptr, nullptr);
         __syncthreads();
         int info = gj_invert<NB, RPT>(cur, N, ld, s);
-        unpermute(P, ld, cur, ld, N, s, 1.0);
+        unpermute_rows(P, ld, cur, ld, N, nr, s);
         __syncthreads();
-        // generator_r(m) = inv(D_{m+1} - generator_r(m+1)), with the running
-        // product P = gR(Nz-1) ... gR(m) of the first-column chain
+        // generator_r(m) = inv(D_{m+1} - generator_r(m+1)), with the rows of the
+        // running product P = gR(Nz-1) ... gR(m) of the first-column chain
         // G_{Nz,1} = (-1)^(Nz-1) gR(Nz-1) ... gR(1) G_11 (math_kernel.f90:83-90,120-128)
+        // that the trace reads
         for (int m = Nz - 3; m >= 0; --m) {
             form_block(oth, g, s, m + 1, E, ik, cur, nullptr);
             __syncthreads();
             const int r = gj_invert<NB, RPT>(oth, N, ld, s);
             if (r && !info) info = r;
-            GemmArgs ga{Pn, ld, P, ld, s.iprow, oth, ld, s.iprow, N, N, N};
+            GemmArgs ga{Pn, ld, P, ld, s.iprow, oth, ld, s.iprow, nr, N, N, nullptr};
             cta_gemm(ga, s, GEMM_STORE, g.delta);
             __syncthreads();
             double2 *t = cur; cur = oth; oth = t;
@@ -84,7 +88,7 @@ __global__ void __launch_bounds__(NT, MINB)
         const int r = gj_invert<NB, RPT>(oth, N, ld, s);
         if (r && !info) info = r;
         // tau = sum_ij gamma_L,i gamma_R,j |2 dz^2 G_{Nz,1}(i,j)|^2   grid.f90:362-383
-        GemmArgs ga{nullptr, 0, P, ld, s.iprow, oth, ld, s.iprow, N, N, N};
+        GemmArgs ga{nullptr, 0, P, ld, s.iprow, oth, ld, s.iprow, nr, N, N, s.rows};
         double t = cta_gemm(ga, s, GEMM_TAU, g.delta);
         t = block_sum(t, s);
         if (threadIdx.x == 0) {
@@ -166,7 +170,7 @@ __global__ void __launch_bounds__(NT, MINB)
             __syncthreads();
             for (int k = 1; k < Nz; ++k) {
                 GemmArgs ga{out_first + NN * k, N, slab + NB2 * (k - 1), ld, nullptr,
-                            out_first + NN * (k - 1), N, nullptr, N, N, N};
+                            out_first + NN * (k - 1), N, nullptr, N, N, N, nullptr};
                 cta_gemm(ga, s, GEMM_STORE_NEG, g.delta);
                 __syncthreads();
             }
@@ -178,10 +182,10 @@ __global__ void __launch_bounds__(NT, MINB)
             double2 *Gc = T0, *Gn = T2;
             for (int k = 1; k < Nz; ++k) {
                 double2 *gRk = slab + NB2 * (k - 1);
-                GemmArgs g1{T1, ld, Gc, ld, nullptr, gRk, ld, nullptr, N, N, N};
+                GemmArgs g1{T1, ld, Gc, ld, nullptr, gRk, ld, nullptr, N, N, N, nullptr};
                 cta_gemm(g1, s, GEMM_STORE_ADD_EYE, g.delta);
                 __syncthreads();
-                GemmArgs g2{Gn, ld, gRk, ld, nullptr, T1, ld, nullptr, N, N, N};
+                GemmArgs g2{Gn, ld, gRk, ld, nullptr, T1, ld, nullptr, N, N, N, nullptr};
                 cta_gemm(g2, s, GEMM_STORE, g.delta);
                 __syncthreads();
                 for (int e = threadIdx.x; e < N * N; e += NT) {
@@ -226,7 +230,7 @@ __global__ void __launch_bounds__(NT, MINB)
         __syncthreads();
         for (int k = 1; k < Nz; ++k) {
             GemmArgs ga{out_last + NN * (Nz - 1 - k), N, slab + NB2 * (Nz - 1 - k), ld, nullptr,
-                        out_last + NN * (Nz - k), N, nullptr, N, N, N};
+                        out_last + NN * (Nz - k), N, nullptr, N, N, N, nullptr};
             cta_gemm(ga, s, GEMM_STORE_NEG, g.delta);
             __syncthreads();
         }

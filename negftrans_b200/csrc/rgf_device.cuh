@@ -117,6 +117,8 @@ struct Smem {
     int *iprow;     // [N] inverse permutation
     int *nx, *ny;   // [N]
     int *inP;       // [N] 1 if row is a pivot row of the current panel
+    int *rows;      // [N] open-channel rows of the left lead (gamma_L != 0), ascending
+    int *nrows;     // [1] their count
     double2 *sigL;  // [N] exp(i q_L dz)
     double2 *sigR;  // [N] exp(i q_R dz)
     double *gL;     // [N] gamma_L  sin(q dz)/dz^2 (grid.f90:365)
@@ -137,7 +139,7 @@ __host__ __device__ inline size_t smem_bytes(int N) {
     size_t gemm = 2 * (size_t)KC * (CM + BP);
     if (gemm > big) big = gemm;
     size_t b = 0;
-    b += 5 * (size_t)round_up(N, 4) * sizeof(int);
+    b += 6 * (size_t)round_up(N, 4) * sizeof(int) + 4 * sizeof(int);
     b += 2 * (size_t)round_up(N, 2) * sizeof(double2);
     b += 2 * (size_t)round_up(N, 2) * sizeof(double);
     b += 32 * sizeof(double2);
@@ -155,7 +157,9 @@ __device__ inline Smem carve(unsigned char *base, int N) {
     s.nx = s.iprow + n4;
     s.ny = s.nx + n4;
     s.inP = s.ny + n4;
-    s.sigL = (double2 *)(s.inP + n4);
+    s.rows = s.inP + n4;
+    s.nrows = s.rows + n4;
+    s.sigL = (double2 *)(s.nrows + 4);
     s.sigR = s.sigL + n2;
     s.gL = (double *)(s.sigR + n2);
     s.gR = s.gL + n2;
@@ -243,6 +247,28 @@ __device__ inline void unpermute(double2 *__restrict__ out, int ldo, const doubl
     }
 }
 
+// Rows of G_{Nz,1} that the transmission trace reads: gamma_L,i != 0, the
+// channels open in the left lead (grid.f90:355-365).  Row i of the chain
+// product P * gR depends on row i of P only, so the chain can carry just
+// these rows and produce the same values for them.
+__device__ inline void open_rows(int N, const Smem &s) {
+    if (threadIdx.x == 0) {
+        int n = 0;
+        for (int i = 0; i < N; ++i)
+            if (s.gL[i] != 0.0) s.rows[n++] = i;
+        *s.nrows = n;
+    }
+}
+
+// out(r, j) = inv(R)(rows[r], j) = R(prow[rows[r]], iprow[j]), r < n.
+__device__ inline void unpermute_rows(double2 *__restrict__ out, int ldo, const double2 *__restrict__ R,
+                                      int ld, int N, int n, const Smem &s) {
+    for (int j = 0; j < N; ++j) {
+        const int jc = s.iprow[j];
+        for (int r = threadIdx.x; r < n; r += NT) out[r + (size_t)ldo * j] = R[s.prow[s.rows[r]] + (size_t)ld * jc];
+    }
+}
+
 // ------------------------------------------------------------------ GEMM
 // D(8x8) += A(8x4) * B(4x8) on the FP64 tensor cores.  Fragments (PTX ISA,
 // mma.m8n8k4 .f64): A row = lane>>2, k = lane&3; B k = lane&3, col = lane>>2;
@@ -301,6 +327,7 @@ struct GemmArgs {
     int ldb;
     const int *bcol;
     int M, Ncol, K;
+    const int *rowmap;  // GEMM_TAU: row i of C is basis row rowmap[i] (nullptr = identity)
 };
 
 // Returns, for GEMM_TAU, this thread's partial sum of
@@ -371,7 +398,8 @@ __device__ inline double cta_gemm(const GemmArgs &a, const Smem &s, int mode, do
                             double2 v = make_double2(acc.re[m][n][e], acc.im[m][n][e]);
                             if (mode == GEMM_TAU) {
                                 const double gx = v.x * 2.0 * (delta * delta), gy = v.y * 2.0 * (delta * delta);
-                                tau += s.gL[i] * s.gR[j] * (gx * gx + gy * gy);
+                                const int ib = a.rowmap ? a.rowmap[i] : i;
+                                tau += s.gL[ib] * s.gR[j] * (gx * gx + gy * gy);
                             } else {
                                 if (mode == GEMM_STORE_NEG) v = make_double2(-v.x, -v.y);
                                 if (mode == GEMM_STORE_ADD_EYE && i == j) v.x += 1.0;
