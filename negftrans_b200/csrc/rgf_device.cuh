@@ -27,7 +27,10 @@ constexpr int NWARP = NT / 32;
 constexpr int CM = 64, CN = 64;  // CTA tile
 constexpr int WM = 32, WN = 16;  // warp tile
 constexpr int KC = 16;           // k chunk staged per pipeline step
-constexpr int BP = CN + 1;       // padded row of a k-major B tile (bank spread)
+// k-major tiles use a 66-element row pitch: successive k rows shift by 8
+// banks, so the four k rows of an m8n8k4 fragment load hit distinct banks.
+constexpr int AP = CM + 2;       // padded row of a k-major A tile
+constexpr int BP = CN + 2;       // padded row of a k-major B tile
 
 // ------------------------------------------------------------ complex FP64
 __device__ __forceinline__ double2 zmake(double x, double y) { return make_double2(x, y); }
@@ -52,14 +55,11 @@ __device__ __forceinline__ double2 zfms(double2 a, double2 b, double2 c) {
     c.y = fma(-a.y, b.x, c.y);
     return c;
 }
-// 1/a with the ratio scaling of Smith's algorithm (no overflow of |a|^2).
+// 1/a = conj(a) / |a|^2 with one division (block entries here are O(1..1e3),
+// far from the overflow range of |a|^2).
 __device__ __forceinline__ double2 zrcp(double2 a) {
-    if (fabs(a.x) >= fabs(a.y)) {
-        double r = a.y / a.x, den = a.x + a.y * r;
-        return make_double2(1.0 / den, -r / den);
-    }
-    double r = a.x / a.y, den = a.x * r + a.y;
-    return make_double2(r / den, -1.0 / den);
+    const double s = 1.0 / (a.x * a.x + a.y * a.y);
+    return make_double2(a.x * s, -a.y * s);
 }
 __device__ __forceinline__ double cabs1(double2 a) { return fabs(a.x) + fabs(a.y); }
 
@@ -104,12 +104,21 @@ struct Geo {
     double V_L, V_R, eta;
 };
 
+// One warp's pivot candidate: a sortable key and the reciprocal of its value.
 struct Red {
-    double v;
-    int idx;
-    int pad;
-    double2 val;
+    unsigned long long key;
+    unsigned long long pad;
+    double2 d;
 };
+
+// Key that orders candidates by |re|+|im| (v >= 0, so its bit pattern sorts
+// as an unsigned integer), then by lower row index.  The low 11 bits of v
+// carry the index; two magnitudes that agree in all but those bits (a
+// relative difference below 2^-41) count as a tie.  Key 0 = no candidate.
+__device__ __forceinline__ unsigned long long pivot_key(double v, int row) {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    return (b & ~0x7FFull) | (unsigned long long)(0x7FF - row);
+}
 
 // Shared memory carve-up (dynamic).
 struct Smem {
@@ -126,7 +135,7 @@ struct Smem {
     double2 *srow;  // [NBMAX] pivot row of the panel step
     Red *red;       // [NWARP]
     double *fred;   // [NWARP] float reductions
-    double2 *big;   // union: GJ panel sW[NB][ldw] + sB[NB][BP] | GEMM stages
+    double2 *big;   // union: sub-panel + block | trailing rows + W tile | GEMM stages
     int ldw;
 };
 
@@ -135,8 +144,10 @@ __host__ __device__ inline int round_up(int a, int b) { return (a + b - 1) / b *
 template <int NB>
 __host__ __device__ inline size_t smem_bytes(int N) {
     int ldw = round_up(N, CM);
-    size_t big = (size_t)NB * ldw + (size_t)NB * BP;
-    size_t gemm = 2 * (size_t)KC * (CM + BP);
+    size_t big = (size_t)NB * ldw + (size_t)NB * NB;         // sub-panel a + 16x16 block
+    size_t trail = 2 * (size_t)NB * (BP + AP);               // gathered rows + W tile
+    size_t gemm = 2 * (size_t)KC * (AP + BP);
+    if (trail > big) big = trail;
     if (gemm > big) big = gemm;
     size_t b = 0;
     b += 6 * (size_t)round_up(N, 4) * sizeof(int) + 4 * sizeof(int);
@@ -300,12 +311,20 @@ struct WarpAcc {
 #pragma unroll
         for (int n = 0; n < 2; ++n) b[n] = sB[kk * ldb + bcol + 8 * n + g];
 #pragma unroll
-        for (int m = 0; m < 4; ++m) {
-            const double nai = -a[m].y;
+        // first the a.re products of all tiles, then the a.im ones, so that
+        // the two MMAs into one accumulator are 16 instructions apart
+#pragma unroll
+        for (int m = 0; m < 4; ++m)
 #pragma unroll
             for (int n = 0; n < 2; ++n) {
                 dmma(re[m][n][0], re[m][n][1], a[m].x, b[n].x);
                 dmma(im[m][n][0], im[m][n][1], a[m].x, b[n].y);
+            }
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const double nai = -a[m].y;
+#pragma unroll
+            for (int n = 0; n < 2; ++n) {
                 dmma(re[m][n][0], re[m][n][1], nai, b[n].y);
                 dmma(im[m][n][0], im[m][n][1], a[m].y, b[n].x);
             }
@@ -335,8 +354,8 @@ struct GemmArgs {
 __device__ inline double cta_gemm(const GemmArgs &a, const Smem &s, int mode, double delta) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wm0 = (warp & 1) * WM, wn0 = (warp >> 1) * WN;
-    double2 *sA = s.big;                 // [2][KC][CM]
-    double2 *sB = s.big + 2 * KC * CM;   // [2][KC][BP]
+    double2 *sA = s.big;                 // [2][KC][AP]
+    double2 *sB = s.big + 2 * KC * AP;   // [2][KC][BP]
     const int ntm = (a.M + CM - 1) / CM, ntn = (a.Ncol + CN - 1) / CN;
     const int nkc = (a.K + KC - 1) / KC;
     double tau = 0.0;
@@ -346,7 +365,7 @@ __device__ inline double cta_gemm(const GemmArgs &a, const Smem &s, int mode, do
         WarpAcc acc;
         acc.zero();
         auto load_stage = [&](int st, int k0) {
-            double2 *dA = sA + st * KC * CM;
+            double2 *dA = sA + st * KC * AP;
             double2 *dB = sB + st * KC * BP;
 #pragma unroll
             for (int q = 0; q < (KC * CM) / NT; ++q) {
@@ -355,7 +374,7 @@ __device__ inline double cta_gemm(const GemmArgs &a, const Smem &s, int mode, do
                 const int k = k0 + kk, i = I0 + ii;
                 const bool v = (k < a.K) && (i < a.M);
                 const int kc = v ? (a.acol ? a.acol[k] : k) : 0;
-                cp_async16(dA + kk * CM + ii, a.A + (v ? (i + (size_t)a.lda * kc) : 0), v);
+                cp_async16(dA + kk * AP + ii, a.A + (v ? (i + (size_t)a.lda * kc) : 0), v);
             }
 #pragma unroll
             for (int q = 0; q < (KC * CN) / NT; ++q) {
@@ -378,10 +397,10 @@ __device__ inline double cta_gemm(const GemmArgs &a, const Smem &s, int mode, do
             }
             __syncthreads();
             if (active) {
-                const double2 *cA = sA + (c & 1) * KC * CM;
+                const double2 *cA = sA + (c & 1) * KC * AP;
                 const double2 *cB = sB + (c & 1) * KC * BP;
 #pragma unroll
-                for (int kb = 0; kb < KC; kb += 4) acc.step(cA, CM, wm0, cB, BP, wn0, kb, lane);
+                for (int kb = 0; kb < KC; kb += 4) acc.step(cA, AP, wm0, cB, BP, wn0, kb, lane);
             }
             __syncthreads();
         }
@@ -428,43 +447,53 @@ __device__ inline double block_sum(double v, const Smem &s) {
 }
 
 // ----------------------------------------------------- Gauss-Jordan inverse
-// Rank-nbe update of every column outside the panel [k0, k0+nbe):
-//   A(:, j) = mask(A(:, j)) + W * A_old(prow[k0:k0+nbe], j)
-// where W = the panel after elimination (held in sW, k-major) and mask zeroes
-// the panel's pivot rows.  W and the gathered pivot rows feed DMMA tiles.
-template <int NB>
-__device__ inline void trailing_update(double2 *__restrict__ A, int N, int ld, int k0, int nbe,
+// Rank-nbt update of every column outside the panel [k0, k0+nbt):
+//   A(:, j) = mask(A(:, j)) + W * A_old(prow[k0:k0+nbt], j)
+// where W = A(:, k0:k0+nbt), the panel after elimination, and mask zeroes the
+// panel's pivot rows.  This is the whole effect of the panel's Gauss-Jordan
+// steps on the other columns, so one pass over the matrix applies KMAX
+// elimination steps.  W tiles are staged from global memory with cp.async;
+// W and the gathered pivot rows feed DMMA warp tiles.
+template <int KMAX>
+__device__ inline void trailing_update(double2 *__restrict__ A, int N, int ld, int k0, int nbt,
                                        const Smem &s) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wm0 = (warp & 1) * WM, wn0 = (warp >> 1) * WN;
-    const int nrest = N - nbe;
-    const int ldw = s.ldw;
-    const double2 *sW = s.big;
-    double2 *sB = s.big + NB * ldw;  // [NB][BP]
+    const int nrest = N - nbt;
+    double2 *sB = s.big;               // [KMAX][BP] pivot rows of the column tile
+    double2 *sW = s.big + KMAX * BP;   // [KMAX][AP] rows I0.. of the panel
     for (int J0 = 0; J0 < nrest; J0 += CN) {
-        for (int e = tid; e < NB * CN; e += NT) {
+        for (int e = tid; e < KMAX * CN; e += NT) {
             const int kk = e / CN, jt = e % CN, jr = J0 + jt;
             double2 v = make_double2(0.0, 0.0);
-            if (kk < nbe && jr < nrest) {
-                const int j = jr < k0 ? jr : jr + nbe;
+            if (kk < nbt && jr < nrest) {
+                const int j = jr < k0 ? jr : jr + nbt;
                 v = A[s.prow[k0 + kk] + (size_t)ld * j];
             }
             sB[kk * BP + jt] = v;
         }
-        __syncthreads();
-        if (J0 + wn0 < nrest) {
-            int col[2][2];
-            bool cv[2][2];
+        int col[2][2];
+        bool cv[2][2];
 #pragma unroll
-            for (int n = 0; n < 2; ++n)
+        for (int n = 0; n < 2; ++n)
 #pragma unroll
-                for (int e = 0; e < 2; ++e) {
-                    const int jr = J0 + wn0 + 8 * n + 2 * (lane & 3) + e;
-                    cv[n][e] = jr < nrest;
-                    col[n][e] = jr < k0 ? jr : jr + nbe;
-                }
-            for (int I0 = 0; I0 < N; I0 += CM) {
-                if (I0 + wm0 >= N) break;
+            for (int e = 0; e < 2; ++e) {
+                const int jr = J0 + wn0 + 8 * n + 2 * (lane & 3) + e;
+                cv[n][e] = jr < nrest;
+                col[n][e] = jr < k0 ? jr : jr + nbt;
+            }
+        for (int I0 = 0; I0 < N; I0 += CM) {
+#pragma unroll
+            for (int q = 0; q < (KMAX * CM) / NT; ++q) {
+                const int e = tid + NT * q;
+                const int kk = e / CM, r = e % CM, i = I0 + r;
+                const bool v = (kk < nbt) && (i < N);
+                cp_async16(sW + kk * AP + r, A + (v ? (i + (size_t)ld * (k0 + kk)) : 0), v);
+            }
+            cp_async_commit();
+            cp_async_wait<0>();
+            __syncthreads();
+            if ((I0 + wm0 < N) && (J0 + wn0 < nrest)) {
                 WarpAcc acc;
 #pragma unroll
                 for (int m = 0; m < 4; ++m) {
@@ -480,8 +509,8 @@ __device__ inline void trailing_update(double2 *__restrict__ A, int N, int ld, i
                             acc.im[m][n][e] = c.y;
                         }
                 }
-#pragma unroll
-                for (int kb = 0; kb < NB; kb += 4) acc.step(sW, ldw, I0 + wm0, sB, BP, wn0, kb, lane);
+#pragma unroll 2
+                for (int kb = 0; kb < nbt; kb += 4) acc.step(sW, AP, wm0, sB, BP, wn0, kb, lane);
 #pragma unroll
                 for (int m = 0; m < 4; ++m) {
                     const int i = I0 + wm0 + 8 * m + (lane >> 2);
@@ -494,21 +523,129 @@ __device__ inline void trailing_update(double2 *__restrict__ A, int N, int ld, i
                     }
                 }
             }
+            __syncthreads();
         }
-        __syncthreads();
     }
 }
 
+// Gauss-Jordan elimination of the columns [kb, kb+nbe) of a register panel
+// w (row tid + NT*r of the block in w[r][.]), with implicit partial pivoting:
+// the pivot of each column is the unused row with the largest |re|+|im|
+// (lowest index on ties), as zgetf2 chooses.  Pivot rows get inP = tag.
+// The step loop is not unrolled: columns are picked out of the register rows
+// by predication, which keeps the code size O(NB).  Each step updates the
+// next pivot column first and runs its warp-level argmax while the rest of
+// the row is updated; the winning lane of each warp computes the reciprocal
+// of its candidate before the barrier.
+template <int NB, int RPT>
+__device__ inline void warp_pivot(const double2 (&f)[RPT], unsigned used, const Smem &s) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    unsigned long long key = 0;
+    int rbest = -1;
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+        if (!((used >> r) & 1u)) {
+            double v = cabs1(f[r]);
+            if (!(v == v)) v = 0.0;  // NaN rows rank as zero pivots
+            const unsigned long long k = pivot_key(v, tid + NT * r);
+            if (k > key) { key = k; rbest = r; }
+        }
+    }
+    unsigned long long wk = key;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long ok = __shfl_xor_sync(0xffffffffu, wk, o);
+        wk = ok > wk ? ok : wk;
+    }
+    if (lane == 0) s.red[warp].key = wk;
+    if (wk != 0 && key == wk) {
+#pragma unroll
+        for (int r = 0; r < RPT; ++r)
+            if (r == rbest) s.red[warp].d = zrcp(f[r]);
+    }
+}
+
+template <int NB, int RPT>
+__device__ inline void factor_subpanel(double2 (&w)[RPT][NB], int kb, int nbe, unsigned &used, int &info,
+                                       int tag, const Smem &s) {
+    const int tid = threadIdx.x;
+    double2 f[RPT];
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) f[r] = w[r][0];
+    warp_pivot<NB, RPT>(f, used, s);
+#pragma unroll 1
+    for (int kk = 0; kk < nbe; ++kk) {
+        __syncthreads();
+        unsigned long long key = s.red[0].key;
+        int q = 0;
+#pragma unroll
+        for (int j = 1; j < NWARP; ++j) {
+            const unsigned long long k = s.red[j].key;
+            if (k > key) { key = k; q = j; }
+        }
+        const double2 d = s.red[q].d;
+        const int p = 0x7FF - (int)(key & 0x7FFull);
+        if ((key >> 11) == 0 && info == 0) info = kb + kk + 1;
+#pragma unroll
+        for (int r = 0; r < RPT; ++r) {
+            if (tid + NT * r == p) {
+                used |= 1u << r;
+#pragma unroll
+                for (int jj = 0; jj < NB; ++jj) s.srow[jj] = w[r][jj];
+            }
+        }
+        if (tid == 0) { s.prow[kb + kk] = p; s.inP[p] = tag; }
+        __syncthreads();
+        // column kk+1 first, then its pivot search overlaps the rest of the row
+        double2 gm[RPT], fn[RPT];
+        const bool more = kk + 1 < nbe;
+        double2 rn = make_double2(0.0, 0.0);
+        if (more) rn = s.srow[kk + 1];
+#pragma unroll
+        for (int r = 0; r < RPT; ++r) {
+            const bool piv = (tid + NT * r == p);
+            gm[r] = piv ? make_double2(0.0, 0.0) : zmul(f[r], d);
+            double2 wn = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int jj = 1; jj < NB; ++jj)
+                if (jj == kk + 1) wn = w[r][jj];
+            fn[r] = piv ? zmul(rn, d) : zfms(gm[r], rn, wn);
+        }
+        if (more) warp_pivot<NB, RPT>(fn, used, s);
+#pragma unroll
+        for (int r = 0; r < RPT; ++r) {
+            const int i = tid + NT * r;
+            if (i == p) {
+#pragma unroll
+                for (int jj = 0; jj < NB; ++jj) {
+                    const double2 v = zmul(s.srow[jj], d);
+                    w[r][jj] = (jj == kk) ? d : v;
+                }
+            } else {
+#pragma unroll
+                for (int jj = 0; jj < NB; ++jj) {
+                    const double2 v = zfms(gm[r], s.srow[jj], w[r][jj]);
+                    w[r][jj] = (jj == kk) ? make_double2(-gm[r].x, -gm[r].y) : v;
+                }
+            }
+            f[r] = fn[r];
+        }
+    }
+    __syncthreads();
+}
+
 // In-place blocked Gauss-Jordan inverse of the N x N block A (leading
-// dimension ld) with implicit partial pivoting.  On return s.prow/s.iprow
-// hold the permutations; the caller reads inv(A) through them.  Returns the
-// LAPACK-style info (1-based column of the first zero pivot, 0 if none);
-// identical in every thread.  RPT = rows per thread (N <= NT*RPT).
+// dimension ld) with implicit partial pivoting.  Panels of 2*NB columns are
+// eliminated as two register sub-panels a and b:
+//   1. eliminate a;  2. bring b up to date with a's steps;  3. eliminate b;
+//   4. apply b's steps to a;  5. one rank-2NB trailing update of the rest.
+// On return s.prow/s.iprow hold the permutations (inv(A)(r,c) =
+// A(prow[r], iprow[c])).  Returns the LAPACK-style info (1-based column of
+// the first zero pivot, 0 if none); identical in every thread.
 template <int NB, int RPT>
 __device__ int gj_invert(double2 *__restrict__ A, int N, int ld, const Smem &s) {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x;
     const int ldw = s.ldw;
-    double2 *sW = s.big;
     int info = 0;
     unsigned used = 0;
 #pragma unroll
@@ -517,106 +654,94 @@ __device__ int gj_invert(double2 *__restrict__ A, int N, int ld, const Smem &s) 
     for (int i = tid; i < N; i += NT) s.inP[i] = 0;
     __syncthreads();
 
-    for (int k0 = 0; k0 < N; k0 += NB) {
-        const int nbe = min(NB, N - k0);
+    for (int k0 = 0; k0 < N; k0 += 2 * NB) {
+        const int nba = min(NB, N - k0);
+        const int nbb = max(0, min(NB, N - k0 - nba));
+        const int nbt = nba + nbb;
         double2 w[RPT][NB];
 #pragma unroll
         for (int r = 0; r < RPT; ++r) {
             const int i = tid + NT * r;
 #pragma unroll
             for (int jj = 0; jj < NB; ++jj)
-                w[r][jj] = (i < N && jj < nbe) ? A[i + (size_t)ld * (k0 + jj)] : make_double2(0.0, 0.0);
+                w[r][jj] = (i < N && jj < nba) ? A[i + (size_t)ld * (k0 + jj)] : make_double2(0.0, 0.0);
         }
-        // The panel step loop is not unrolled: the pivot column kk is picked out
-        // of the register rows by predication, which keeps the code size O(NB).
-#pragma unroll 1
-        for (int kk = 0; kk < nbe; ++kk) {
-            double2 f[RPT];
-#pragma unroll
-            for (int r = 0; r < RPT; ++r) {
-                f[r] = make_double2(0.0, 0.0);
-#pragma unroll
-                for (int jj = 0; jj < NB; ++jj)
-                    if (jj == kk) f[r] = w[r][jj];
-            }
-            // --- pivot search among unused rows (largest |re|+|im|, lowest index on ties)
-            double bv = -1.0;
-            int bi = 0x7fffffff;
-            double2 bval = make_double2(0.0, 0.0);
-#pragma unroll
-            for (int r = 0; r < RPT; ++r) {
-                if (!((used >> r) & 1u)) {
-                    double v = cabs1(f[r]);
-                    if (!(v == v)) v = 0.0;  // NaN rows rank as zero pivots
-                    if (v > bv) { bv = v; bi = tid + NT * r; bval = f[r]; }
-                }
-            }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
-                const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-                const double ox = __shfl_xor_sync(0xffffffffu, bval.x, o);
-                const double oy = __shfl_xor_sync(0xffffffffu, bval.y, o);
-                if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; bval = make_double2(ox, oy); }
-            }
-            if (lane == 0) { s.red[warp].v = bv; s.red[warp].idx = bi; s.red[warp].val = bval; }
-            __syncthreads();
-            bv = s.red[0].v; bi = s.red[0].idx; bval = s.red[0].val;
-#pragma unroll
-            for (int q = 1; q < NWARP; ++q) {
-                const Red o = s.red[q];
-                if (o.v > bv || (o.v == bv && o.idx < bi)) { bv = o.v; bi = o.idx; bval = o.val; }
-            }
-            const int p = bi;
-            if (bv == 0.0 && info == 0) info = k0 + kk + 1;
-            const double2 d = zrcp(bval);
-#pragma unroll
-            for (int r = 0; r < RPT; ++r) {
-                if (tid + NT * r == p) {
-                    used |= 1u << r;
-#pragma unroll
-                    for (int jj = 0; jj < NB; ++jj) s.srow[jj] = w[r][jj];
-                }
-            }
-            if (tid == 0) { s.prow[k0 + kk] = p; s.inP[p] = 1; }
-            __syncthreads();
-            // --- eliminate column kk from every row, scale the pivot row
+        factor_subpanel<NB, RPT>(w, k0, nba, used, info, 1, s);
+        if (nbb > 0) {
+            double2 *sWa = s.big;              // [NB][ldw] sub-panel a after step 1
+            double2 *sX = s.big + NB * ldw;    // [NB][NB]
+            const int kbb = k0 + nba;
 #pragma unroll
             for (int r = 0; r < RPT; ++r) {
                 const int i = tid + NT * r;
-                if (i == p) {
+                if (i < ldw) {
 #pragma unroll
-                    for (int jj = 0; jj < NB; ++jj) {
-                        const double2 v = zmul(s.srow[jj], d);
-                        w[r][jj] = (jj == kk) ? d : v;
-                    }
-                } else {
-                    const double2 gm = zmul(f[r], d);
+                    for (int jj = 0; jj < NB; ++jj) sWa[jj * ldw + i] = (i < N) ? w[r][jj] : make_double2(0.0, 0.0);
+                }
+            }
+            // rows P_a of sub-panel b before a's steps
+            for (int e = tid; e < NB * NB; e += NT) {
+                const int kk = e / NB, c = e % NB;
+                sX[e] = (kk < nba && c < nbb) ? A[s.prow[k0 + kk] + (size_t)ld * (kbb + c)] : make_double2(0.0, 0.0);
+            }
+            __syncthreads();
+            // 2. b = mask_a(b) + W_a * b(P_a, :)
 #pragma unroll
-                    for (int jj = 0; jj < NB; ++jj) {
-                        const double2 v = zfms(gm, s.srow[jj], w[r][jj]);
-                        w[r][jj] = (jj == kk) ? make_double2(-gm.x, -gm.y) : v;
+            for (int r = 0; r < RPT; ++r) {
+                const int i = tid + NT * r;
+                const bool keep = (i < N) && s.inP[i] != 1;
+#pragma unroll
+                for (int c = 0; c < NB; ++c)
+                    w[r][c] = (keep && c < nbb) ? A[i + (size_t)ld * (kbb + c)] : make_double2(0.0, 0.0);
+                if (i < N) {
+#pragma unroll 1
+                    for (int kk = 0; kk < nba; ++kk) {
+                        const double2 wa = sWa[kk * ldw + i];
+#pragma unroll
+                        for (int c = 0; c < NB; ++c) w[r][c] = zfma(wa, sX[kk * NB + c], w[r][c]);
                     }
                 }
             }
-        }
-        // --- write the panel back and stage it for the trailing update
+            // 3. eliminate b
+            factor_subpanel<NB, RPT>(w, kbb, nbb, used, info, 2, s);
+            // rows P_b of sub-panel a after step 1
+            for (int e = tid; e < NB * NB; e += NT) {
+                const int kk = e / NB, c = e % NB;
+                sX[e] = (kk < nbb && c < nba) ? sWa[c * ldw + s.prow[kbb + kk]] : make_double2(0.0, 0.0);
+            }
+            __syncthreads();
+            // 4. a = mask_b(a) + W_b * a(P_b, :); write W = [a | b] back
 #pragma unroll
-        for (int r = 0; r < RPT; ++r) {
-            const int i = tid + NT * r;
-            if (i < ldw) {
+            for (int r = 0; r < RPT; ++r) {
+                const int i = tid + NT * r;
+                if (i < N) {
+                    const bool keep = s.inP[i] != 2;
+                    for (int c = 0; c < nba; ++c) {
+                        double2 v = keep ? sWa[c * ldw + i] : make_double2(0.0, 0.0);
 #pragma unroll
-                for (int jj = 0; jj < NB; ++jj) {
-                    const double2 v = (i < N) ? w[r][jj] : make_double2(0.0, 0.0);
-                    sW[jj * ldw + i] = v;
-                    if (i < N && jj < nbe) A[i + (size_t)ld * (k0 + jj)] = v;
+                        for (int kk = 0; kk < NB; ++kk) v = zfma(w[r][kk], sX[kk * NB + c], v);
+                        A[i + (size_t)ld * (k0 + c)] = v;
+                    }
+#pragma unroll
+                    for (int kk = 0; kk < NB; ++kk)
+                        if (kk < nbb) A[i + (size_t)ld * (kbb + kk)] = w[r][kk];
+                }
+            }
+        } else {
+#pragma unroll
+            for (int r = 0; r < RPT; ++r) {
+                const int i = tid + NT * r;
+                if (i < N) {
+#pragma unroll
+                    for (int jj = 0; jj < NB; ++jj)
+                        if (jj < nba) A[i + (size_t)ld * (k0 + jj)] = w[r][jj];
                 }
             }
         }
         __syncthreads();
-        if (nbe < N) trailing_update<NB>(A, N, ld, k0, nbe, s);
+        if (nbt < N) trailing_update<2 * NB>(A, N, ld, k0, nbt, s);
         __syncthreads();
-        if (tid < nbe) s.inP[s.prow[k0 + tid]] = 0;
+        if (tid < nbt) s.inP[s.prow[k0 + tid]] = 0;
         __syncthreads();
     }
     for (int k = tid; k < N; k += NT) s.iprow[s.prow[k]] = k;
