@@ -156,6 +156,27 @@ int negf_density(negf_ctx *ctx, int32_t n_circle, int32_t n_line, double min_v, 
 int negf_ldos_matrix(negf_ctx *ctx, double e_lo, double e_hi, int32_t n_e, int32_t i_e0,
                      int32_t n_chunk, double *ldos, negf_stats *stats);
 
+/* The density of main.f90:258-351 on the GPU: negf_density, then per slice
+ * Greensfunction_PlanewaveToReal (grid.f90:71-135) and Density = Im(diag) * scale
+ * with scale = N_z/(LX*LY*LZ) in the reference's Angstrom units
+ * (main.f90:342-347).  density (Nx,Ny,Nz) receives Angstrom^-3; dm
+ * (optional, (N,N,Nz) complex) receives Density_Matrix.  Errors if the basis
+ * does not fit the real-space grid (2*max|n| >= N_x). */
+int negf_density_real(negf_ctx *ctx, int32_t n_circle, int32_t n_line, double min_v, double mu,
+                      double gap, double temperature, int32_t Nx, int32_t Ny, double scale,
+                      double *density, double *dm, negf_stats *stats);
+
+/* The LDOS of main.f90:417-554 on the GPU for the grid
+ * E_i = e_lo + (e_hi-e_lo)*i/n_e: per energy the k-summed LDOS_Matrix
+ * (negf.f90:176-236), Greensfunction_PlanewaveToReal per slice, and the
+ * LDOS_grid_converter mapping of tools.f90:6-40 (ldos_grid = LDOS_GRID:
+ * 0 keeps the axis, -1 integrates with dxyz[axis] = L/N, m > 0 takes grid
+ * point m).  scale = N_z/(LX*LY*LZ)/hartree (main.f90:514).  ldos receives
+ * (Mx,My,Mz,n_e) with M = N_axis if LDOS_GRID = 0 else 1. */
+int negf_ldos(negf_ctx *ctx, double e_lo, double e_hi, int32_t n_e, const int32_t *ldos_grid,
+              int32_t Nx, int32_t Ny, const double *dxyz, double scale, double *ldos,
+              negf_stats *stats);
+
 /* Greensfunction_PlanewaveToReal, grid.f90:71-135, for Nz_s slices:
  * g (N,N,Nz_s) complex -> out (Nx,Ny,Nz_s) complex, the unnormalised
  * real-space diagonal.  Computed by binning G(a,b) on n_a-n_b and one 2-D

@@ -24,6 +24,7 @@ EXPORTS = (
     "negf_basis_size", "negf_basis", "negf_kmesh", "negf_vhat", "negf_ctx_create",
     "negf_ctx_destroy", "negf_tri_solve", "negf_transmission", "negf_transmission_device",
     "negf_density", "negf_ldos_matrix", "negf_ptor", "negf_version", "negf_transmission_noalloc",
+    "negf_density_real", "negf_ldos",
 )
 
 _dp = C.POINTER(C.c_double)
@@ -80,6 +81,11 @@ def lib():
                                C.c_double, _dp, C.POINTER(Stats)]
     L.negf_ldos_matrix.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int32, C.c_int32,
                                    C.c_int32, _dp, C.POINTER(Stats)]
+    L.negf_density_real.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
+                                    C.c_double, C.c_int32, C.c_int32, C.c_double, _dp, _dp,
+                                    C.POINTER(Stats)]
+    L.negf_ldos.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int32, _ip, C.c_int32, C.c_int32, _dp,
+                            C.c_double, _dp, C.POINTER(Stats)]
     L.negf_ptor.argtypes = [_dp, _ip, _ip, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _dp]
     _lib = L
     return L

@@ -12,6 +12,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libnegfgpu.so")
+DRIVER = os.path.join(PKG, "negftrans")   # the main.f90-style executable
 SOURCES = ["negf_engine.cu", "negf_host.cpp"]
 HEADERS = ["rgf_device.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -27,8 +28,20 @@ def _stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+def build_driver(force: bool = False) -> str:
+    src = os.path.join(CSRC, "negftrans_main.cpp")
+    if (not force and os.path.exists(DRIVER)
+            and os.path.getmtime(DRIVER) >= max(os.path.getmtime(src), os.path.getmtime(LIB))):
+        return DRIVER
+    cmd = ["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), src, "-L", PKG, "-lnegfgpu",
+           "-Wl,-rpath,$ORIGIN", "-o", DRIVER]
+    subprocess.run(cmd, check=True)
+    return DRIVER
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not _stale():
+        build_driver()
         return LIB
     cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
            "-I", os.path.join(ROOT, "include"), "-I", CSRC, "-cudart", "static", "-o", LIB]
@@ -36,6 +49,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         cmd += ["-Xptxas", "-v"]
     cmd += [os.path.join(CSRC, f) for f in SOURCES]
     subprocess.run(cmd, check=True)
+    build_driver(force=True)
     return LIB
 
 

@@ -264,6 +264,102 @@ __global__ void k_accumulate(const double2 *__restrict__ slabs, size_t sstride, 
     }
 }
 
+// ------------------------------------------------- plane wave -> real space
+// diag(u,v) = sum_ab G(a,b) e^{+2 pi i ((nx_a-nx_b) u/Nx + (ny_a-ny_b) v/Ny)}, the
+// diagonal that the FFT pair of grid.f90:88-133 extracts.  One CTA per slice:
+// G is binned on the difference n_a - n_b in shared memory, then transformed
+// along x (UC rows of u at a time) and along y.  Writes Im(diag) * scale
+// (main.f90:341-351) to dens, or the complex diagonal to cdiag.
+constexpr int PT_THREADS = 256;
+constexpr int PT_UC = 16;
+
+__global__ void __launch_bounds__(PT_THREADS)
+    k_ptor(const double2 *__restrict__ G, int N, int ldg, size_t gstride, const int *__restrict__ nx,
+           const int *__restrict__ ny, int mx, int my, int Nx, int Ny, double scale,
+           double *__restrict__ dens, double2 *__restrict__ cdiag) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int BX = 4 * mx + 1, BY = 4 * my + 1;
+    double2 *bin = (double2 *)smem_raw;                  // [BY][BX]
+    double2 *T = bin + (size_t)BX * BY;                  // [PT_UC][BY]
+    double2 *twx = T + (size_t)PT_UC * BY;               // [Nx] e^{+2 pi i m/Nx}
+    double2 *twy = twx + Nx;                             // [Ny]
+    const int k = blockIdx.x;
+    const double2 *Gk = G + gstride * k;
+    for (int e = threadIdx.x; e < BX * BY; e += PT_THREADS) bin[e] = make_double2(0.0, 0.0);
+    for (int m = threadIdx.x; m < Nx; m += PT_THREADS) {
+        double sn, cs;
+        sincospi(2.0 * m / Nx, &sn, &cs);
+        twx[m] = make_double2(cs, sn);
+    }
+    for (int m = threadIdx.x; m < Ny; m += PT_THREADS) {
+        double sn, cs;
+        sincospi(2.0 * m / Ny, &sn, &cs);
+        twy[m] = make_double2(cs, sn);
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < N * N; e += PT_THREADS) {
+        const int a = e % N, b = e / N;
+        const double2 v = Gk[a + (size_t)ldg * b];
+        double2 *t = bin + (nx[a] - nx[b] + 2 * mx) + BX * (ny[a] - ny[b] + 2 * my);
+        atomicAdd(&t->x, v.x);
+        atomicAdd(&t->y, v.y);
+    }
+    __syncthreads();
+    for (int u0 = 0; u0 < Nx; u0 += PT_UC) {
+        // T(u, dy) = sum_dx bin(dx, dy) e^{+2 pi i (dx - 2mx) u / Nx}
+        for (int e = threadIdx.x; e < PT_UC * BY; e += PT_THREADS) {
+            const int uu = e % PT_UC, dy = e / PT_UC, u = u0 + uu;
+            double2 acc = make_double2(0.0, 0.0);
+            if (u < Nx)
+                for (int dx = 0; dx < BX; ++dx) {
+                    int m = ((dx - 2 * mx) * u) % Nx;
+                    if (m < 0) m += Nx;
+                    acc = zfma(bin[dx + BX * dy], twx[m], acc);
+                }
+            T[uu + PT_UC * dy] = acc;
+        }
+        __syncthreads();
+        // diag(u, v) = sum_dy T(u, dy) e^{+2 pi i (dy - 2my) v / Ny}
+        for (int e = threadIdx.x; e < PT_UC * Ny; e += PT_THREADS) {
+            const int uu = e % PT_UC, v = e / PT_UC, u = u0 + uu;
+            if (u >= Nx) continue;
+            double2 acc = make_double2(0.0, 0.0);
+            for (int dy = 0; dy < BY; ++dy) {
+                int m = ((dy - 2 * my) * v) % Ny;
+                if (m < 0) m += Ny;
+                acc = zfma(T[uu + PT_UC * dy], twy[m], acc);
+            }
+            const size_t o = u + (size_t)Nx * v + (size_t)Nx * Ny * k;
+            if (dens) dens[o] = acc.y * scale;
+            if (cdiag) cdiag[o] = acc;
+        }
+        __syncthreads();
+    }
+}
+
+size_t ptor_smem(int mx, int my, int Nx, int Ny) {
+    const size_t BX = 4 * (size_t)mx + 1, BY = 4 * (size_t)my + 1;
+    return sizeof(double2) * (BX * BY + PT_UC * BY + Nx + Ny);
+}
+
+// LDOS_grid_converter (tools.f90:18-40) applied to one energy's real-space
+// diagonal: LDOS(ii,jj,kk) += Im(diag(i,j,k)) * scale * factors (main.f90:510-526).
+__global__ void k_ldos_convert(const double2 *__restrict__ diag, int Nx, int Ny, int Nz, int gx, int gy,
+                               int gz, double dx, double dy, double dz, double scale, int Mx, int My,
+                               double *__restrict__ out) {
+    const size_t tot = (size_t)Nx * Ny * Nz;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < tot; e += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(e % Nx), j = (int)((e / Nx) % Ny), k = (int)(e / ((size_t)Nx * Ny));
+        double f = scale;
+        int ii = 0, jj = 0, kk = 0;
+        // 1-based grid index m selects one point, -1 integrates (x delta), 0 keeps the axis
+        if (gx == 0) ii = i; else if (gx == -1) f *= dx; else if (gx != i + 1) f = 0.0;
+        if (gy == 0) jj = j; else if (gy == -1) f *= dy; else if (gy != j + 1) f = 0.0;
+        if (gz == 0) kk = k; else if (gz == -1) f *= dz; else if (gz != k + 1) f = 0.0;
+        if (f != 0.0) atomicAdd(out + ii + (size_t)Mx * (jj + (size_t)My * kk), diag[e].y * f);
+    }
+}
+
 }  // namespace
 
 // ======================================================================= host
@@ -832,6 +928,129 @@ done:
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------ real-space outputs
+namespace {
+int basis_extent(const negf_ctx *c, int *mx, int *my) {
+    std::vector<int> nx(c->N), ny(c->N);
+    if (cudaMemcpy(nx.data(), c->d_nx, sizeof(int) * c->N, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(ny.data(), c->d_ny, sizeof(int) * c->N, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return NEGF_ERR_CUDA;
+    *mx = *my = 0;
+    for (int a = 0; a < c->N; ++a) {
+        *mx = std::max(*mx, std::abs(nx[a]));
+        *my = std::max(*my, std::abs(ny[a]));
+    }
+    return 0;
+}
+
+int launch_ptor(negf_ctx *c, const double2 *d_G, int nslices, int Nx, int Ny, double scale, double *d_dens,
+                double2 *d_cdiag, cudaStream_t st) {
+    int mx, my;
+    int rc = basis_extent(c, &mx, &my);
+    if (rc) return rc;
+    if (2 * mx >= Nx || 2 * my >= Ny) return NEGF_ERR_ARG;  // index nx+Nx/2 must fit (grid.f90:92-94)
+    const size_t smem = ptor_smem(mx, my, Nx, Ny);
+    if (smem > 200 * 1024) return NEGF_ERR_UNSUPPORTED;
+    CK(cudaFuncSetAttribute(k_ptor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_ptor<<<nslices, PT_THREADS, smem, st>>>(d_G, c->N, c->N, (size_t)c->N * c->N, c->d_nx, c->d_ny, mx, my,
+                                              Nx, Ny, scale, d_dens, d_cdiag);
+    CK(cudaGetLastError());
+    return 0;
+}
+}  // namespace
+
+extern "C" int negf_density_real(negf_ctx *c, int32_t n_circle, int32_t n_line, double min_v, double mu,
+                                 double gap, double temperature, int32_t Nx, int32_t Ny, double scale,
+                                 double *density, double *dm, negf_stats *stats) {
+    if (!c || !density || Nx < 1 || Ny < 1) return NEGF_ERR_ARG;
+    const size_t per = (size_t)c->N * c->N * c->Nz;
+    std::vector<double> host_dm;
+    double *dmh = dm;
+    if (!dmh) { host_dm.resize(2 * per); dmh = host_dm.data(); }
+    int rc = negf_density(c, n_circle, n_line, min_v, mu, gap, temperature, dmh, stats);
+    if (rc < 0) return rc;
+    const int info = rc;
+    double2 *d_G = nullptr;
+    double *d_dens = nullptr;
+    const size_t nd = (size_t)Nx * Ny * c->Nz;
+    if (cudaMalloc(&d_G, sizeof(double2) * per) != cudaSuccess) { cudaGetLastError(); return NEGF_ERR_NOMEM; }
+    if (cudaMalloc(&d_dens, sizeof(double) * nd) != cudaSuccess) { cudaGetLastError(); cudaFree(d_G); return NEGF_ERR_NOMEM; }
+    rc = 0;
+    if (cudaMemcpyAsync(d_G, dmh, sizeof(double2) * per, cudaMemcpyHostToDevice, c->stream) != cudaSuccess) rc = NEGF_ERR_CUDA;
+    if (!rc) rc = launch_ptor(c, d_G, c->Nz, Nx, Ny, scale, d_dens, nullptr, c->stream);
+    if (!rc && (cudaMemcpyAsync(density, d_dens, sizeof(double) * nd, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+                cudaStreamSynchronize(c->stream) != cudaSuccess))
+        rc = NEGF_ERR_CUDA;
+    cudaFree(d_G);
+    cudaFree(d_dens);
+    return rc ? rc : info;
+}
+
+extern "C" int negf_ldos(negf_ctx *c, double e_lo, double e_hi, int32_t n_e, const int32_t *ldos_grid,
+                         int32_t Nx, int32_t Ny, const double *dxyz, double scale, double *ldos,
+                         negf_stats *stats) {
+    if (!c || !ldos || !ldos_grid || !dxyz || n_e < 1 || Nx < 1 || Ny < 1) return NEGF_ERR_ARG;
+    for (int a = 0; a < 3; ++a)
+        if (ldos_grid[a] < -1) return NEGF_ERR_ARG;  // main.f90:125-128
+    if (cudaSetDevice(c->device) != cudaSuccess) return NEGF_ERR_CUDA;
+    const int Nz = c->Nz, nk = c->nk;
+    const int Mx = ldos_grid[0] == 0 ? Nx : 1, My = ldos_grid[1] == 0 ? Ny : 1, Mz = ldos_grid[2] == 0 ? Nz : 1;
+    const size_t per = (size_t)c->N * c->N * Nz, nreal = (size_t)Nx * Ny * Nz, nout = (size_t)Mx * My * Mz;
+    // energies per chunk: LDOS matrices and their real-space diagonals resident at once
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    const size_t per_e = sizeof(double2) * (per + nreal);
+    int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)n_e, (free_b / 4) / std::max<size_t>(per_e, 1)));
+    double2 *d_mat = nullptr, *d_diag = nullptr;
+    double *d_out = nullptr;
+    if (cudaMalloc(&d_mat, sizeof(double2) * per * chunk) != cudaSuccess ||
+        cudaMalloc(&d_diag, sizeof(double2) * nreal * chunk) != cudaSuccess ||
+        cudaMalloc(&d_out, sizeof(double) * nout * n_e) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(d_mat); cudaFree(d_diag);
+        return NEGF_ERR_NOMEM;
+    }
+    int rc = cudaMemsetAsync(d_out, 0, sizeof(double) * nout * n_e, c->stream) == cudaSuccess ? 0 : NEGF_ERR_CUDA;
+    std::vector<int> info_all;
+    double ms_all = 0;
+    for (int e0 = 0; e0 < n_e && !rc; e0 += chunk) {
+        const int nc = std::min(chunk, n_e - e0);
+        std::vector<RgfJob> jobs(nc * nk);
+        std::vector<double2> coef(nc * nk);
+        for (int o = 0; o < nc; ++o) {
+            const int i_energy = e0 + o + 1;  // negf.f90:203-204
+            const double e = e_lo + (e_hi - e_lo) * (i_energy - 1) / n_e;
+            for (int ik = 0; ik < nk; ++ik) {
+                RgfJob jb{};
+                jb.e_re = e; jb.e_im = c->eta; jb.e_t = e; jb.ik = ik;
+                jobs[o * nk + ik] = jb;
+                coef[o * nk + ik] = make_double2(-(c->kpt[3 * ik + 2] * 1.0 / PI), 0.0);
+            }
+        }
+        std::vector<int> info;
+        double ms = 0;
+        rc = diag_accumulate(c, jobs, coef, nk, d_mat, info, ms);
+        if (rc) break;
+        info_all.insert(info_all.end(), info.begin(), info.end());
+        ms_all += ms;
+        rc = launch_ptor(c, d_mat, nc * Nz, Nx, Ny, 1.0, nullptr, d_diag, c->stream);
+        for (int o = 0; o < nc && !rc; ++o) {
+            const int blocks = (int)std::min<size_t>((nreal + 255) / 256, (size_t)c->num_sms * 8);
+            k_ldos_convert<<<blocks, 256, 0, c->stream>>>(d_diag + nreal * o, Nx, Ny, Nz, ldos_grid[0], ldos_grid[1],
+                                                         ldos_grid[2], dxyz[0], dxyz[1], dxyz[2], scale, Mx, My,
+                                                         d_out + nout * (e0 + o));
+            if (cudaGetLastError() != cudaSuccess) rc = NEGF_ERR_CUDA;
+        }
+    }
+    if (!rc && (cudaMemcpyAsync(ldos, d_out, sizeof(double) * nout * n_e, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+                cudaStreamSynchronize(c->stream) != cudaSuccess))
+        rc = NEGF_ERR_CUDA;
+    cudaFree(d_mat); cudaFree(d_diag); cudaFree(d_out);
+    if (rc) return rc;
+    fill_stats(stats, info_all, ms_all);
+    return first_info(info_all);
+}
 
 // ============================================================ no-alloc entry
 // negf_transmission_noalloc: the transmission sweep for callers that cannot

@@ -109,6 +109,34 @@ class Engine:
         self.last_stats = st
         return dm, rc
 
+    def density_real(self, N_circle, N_line, min_V, MU, GAP, TEMPERATURE, N_x, N_y, LX_A, LY_A, LZ_A):
+        """Density (N_x, N_y, N_z) in Angstrom^-3 after main.f90:258-351 (all on the GPU);
+        returns (density, Density_Matrix, info)."""
+        dens = np.zeros((N_x, N_y, self.Nz), np.float64, order="F")
+        dm = np.zeros((self.N, self.N, self.Nz), np.complex128, order="F")
+        scale = self.Nz / (LX_A * LY_A * LZ_A)
+        st = Stats()
+        rc = check("negf_density_real", lib().negf_density_real(
+            self._ctx, N_circle, N_line, min_V, MU, GAP, TEMPERATURE, N_x, N_y, scale,
+            dens.ctypes.data_as(_dp), dm.ctypes.data_as(_dp), C.byref(st)))
+        self.last_stats = st
+        return dens, dm, rc
+
+    def ldos(self, e_lo, e_hi, N_E, LDOS_GRID, N_x, N_y, LX_A, LY_A, LZ_A):
+        """LDOS (M_x, M_y, M_z, N_E) after main.f90:417-554 (Angstrom^-n eV^-1)."""
+        from .constants import HARTREE
+        g = np.ascontiguousarray(LDOS_GRID, np.int32)
+        M = [N_x if g[0] == 0 else 1, N_y if g[1] == 0 else 1, self.Nz if g[2] == 0 else 1]
+        out = np.zeros((M[0], M[1], M[2], N_E), np.float64, order="F")
+        dxyz = np.array([LX_A / N_x, LY_A / N_y, LZ_A / self.Nz])
+        scale = self.Nz / (LX_A * LY_A * LZ_A) / HARTREE
+        st = Stats()
+        rc = check("negf_ldos", lib().negf_ldos(
+            self._ctx, e_lo, e_hi, N_E, g.ctypes.data_as(_ip), N_x, N_y, dxyz.ctypes.data_as(_dp), scale,
+            out.ctypes.data_as(_dp), C.byref(st)))
+        self.last_stats = st
+        return out, rc
+
     # negf.f90:176-236 summed over k-points, for a range of LDOS energies
     def ldos_matrix(self, e_lo, e_hi, N_E, i_e0=0, n_chunk=None):
         """LDOS_Matrix per energy: (n_chunk, N, N, N_z) complex (each Fortran-ordered)."""

@@ -249,6 +249,46 @@ def ptor(G, nx, ny, Nx, Ny):
     return out
 
 
+def density_from_matrix(dm, nx, ny, N_x, N_y, LX_A, LY_A, LZ_A):
+    """main.f90:306-351: PtoR per slice (oracle_ptor), Density = Im(.) * N_z/(LX*LY*LZ)."""
+    Nz = dm.shape[2]
+    out = np.zeros((N_x, N_y, Nz))
+    for k in range(Nz):
+        out[:, :, k] = ptor(dm[:, :, k], nx, ny, N_x, N_y).imag * (Nz / (LX_A * LY_A * LZ_A))
+    return out
+
+
+def _grid_converter(i, m, delta, rescale):
+    """tools.f90:18-40 (i 1-based); returns (ii 1-based, rescale)."""
+    ii = i if m == 0 else 1
+    if m == 0:
+        pass
+    elif m == -1:
+        rescale = rescale * delta
+    elif m == i:
+        pass
+    else:
+        rescale = 0.0
+    return ii, rescale
+
+
+def ldos_from_matrix(ldos_mat, nx, ny, N_x, N_y, LX_A, LY_A, LZ_A, LDOS_GRID):
+    """main.f90:479-526 for one energy: PtoR per slice and the grid conversion."""
+    Nz = ldos_mat.shape[2]
+    size = lambda m, n: n if m == 0 else 1      # tools.f90:6-16
+    out = np.zeros((size(LDOS_GRID[0], N_x), size(LDOS_GRID[1], N_y), size(LDOS_GRID[2], Nz)))
+    real = np.stack([ptor(ldos_mat[:, :, k], nx, ny, N_x, N_y) for k in range(Nz)], axis=2)
+    for k in range(1, Nz + 1):
+        for j in range(1, N_y + 1):
+            for i in range(1, N_x + 1):
+                r = Nz / (LX_A * LY_A * LZ_A) / HARTREE
+                ii, r = _grid_converter(i, LDOS_GRID[0], LX_A / N_x, r)
+                jj, r = _grid_converter(j, LDOS_GRID[1], LY_A / N_y, r)
+                kk, r = _grid_converter(k, LDOS_GRID[2], LZ_A / Nz, r)
+                out[ii - 1, jj - 1, kk - 1] += real[i - 1, j - 1, k - 1].imag * r
+    return out
+
+
 # ----------------------------------------------------- independent checkers
 def dense_blocks(D):
     """All blocks of inv(tridiag(I, D_k, I)) by one dense NumPy inverse."""

@@ -191,3 +191,40 @@ def test_transmission_wide_basis(oracle, encut_meV, grid):
         tau, info = eng.transmission(E)
     assert info == 0
     np.testing.assert_allclose(tau, tau_ref, rtol=RTOL, atol=1e-12)
+
+
+def test_density_real_space(oracle):
+    """Density (main.f90:258-351): contour, G_kk sum, PtoR and scale on the GPU."""
+    pr = small_problem(nz=6, nk=1)
+    a, d = pr.atomic, None
+    Nx, Ny = 32, 32
+    LX, LY, LZ = 1000.0, 1000.0, pr.Nz * 10.0
+    n_c, n_l = 5, 4
+    with Engine(*pr.engine_args()) as eng:
+        dens, dm, info = eng.density_real(n_c, n_l, pr.min_V, a.MU, a.GAP, a.TEMPERATURE, Nx, Ny, LX, LY, LZ)
+    assert info == 0
+    dm_ref, _ = oracle.density_jobs(oracle_problem(oracle, pr), n_c, n_l, pr.min_V, a.MU, a.GAP,
+                                    a.TEMPERATURE)
+    assert rel_err(dm, dm_ref) < RTOL
+    ref = oracle.density_from_matrix(dm_ref, pr.nx, pr.ny, Nx, Ny, LX, LY, LZ)
+    assert rel_err(dens, ref) < RTOL
+
+
+@pytest.mark.parametrize("grid", [(0, 0, 0), (-1, -1, 0), (-1, 5, -1), (3, 0, 2)])
+def test_ldos_real_space(oracle, grid):
+    """LDOS (main.f90:417-554) incl. every LDOS_GRID mode of tools.f90:6-40."""
+    pr = small_problem(nz=4, nk=2)
+    p = oracle_problem(oracle, pr)
+    Nx, Ny = 32, 32
+    LX, LY, LZ = 1000.0, 1000.0, pr.Nz * 10.0
+    e_lo, e_hi, n_e = 0.0, 0.067 * 0.03 / HARTREE, 3
+    with Engine(*pr.engine_args()) as eng:
+        got, info = eng.ldos(e_lo, e_hi, n_e, grid, Nx, Ny, LX, LY, LZ)
+    assert info == 0
+    for ie in range(n_e):
+        mat = np.zeros((pr.N, pr.N, pr.Nz), np.complex128, order="F")
+        for ik in range(len(pr.kpoint)):
+            oracle.local_density_of_state(p, ik + 1, ie + 1, n_e, e_lo, e_hi, mat)
+        ref = oracle.ldos_from_matrix(mat, pr.nx, pr.ny, Nx, Ny, LX, LY, LZ, grid)
+        assert got.shape[:3] == ref.shape
+        assert rel_err(got[..., ie], ref) < RTOL
