@@ -143,7 +143,7 @@ def test_end_to_end_against_oracle(driver, tmp_path, oracle):
     assert r.returncode == 0, (tmp_path / "OUTPUT").read_text()
     assert "DONE" in (tmp_path / "OUTPUT").read_text()
     # the driver reads POTENTIAL as written (8 significant digits)
-    Vf = np.loadtxt(tmp_path / "POTENTIAL", skiprows=1).ravel()[: V.size].reshape(V.shape, order="F")
+    Vf = np.array((tmp_path / "POTENTIAL").read_text().split()[3:], float).reshape(V.shape, order="F")
     pr = P.prepare(deck, Vf)
     a = pr.atomic
     p = oracle.Problem(pr.nx, pr.ny, pr.vhat, a.LX, a.LY, a.LZ, a.V_L, a.V_R, a.ETA, pr.kpoint)
