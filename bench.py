@@ -45,6 +45,7 @@ def parse():
     ap.add_argument("--cpu-threads", type=int, default=0, help="0 = all host cores (max 16)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--density", action="store_true", help="also time the density contour once")
     return ap.parse_args()
 
 
@@ -211,7 +212,9 @@ def run_ours(args):
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if world > 1:
+    # under torchrun (any world size) the ranks meet in an NCCL process group
+    distributed = "RANK" in os.environ and "MASTER_ADDR" in os.environ
+    if distributed:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
 
@@ -245,7 +248,7 @@ def run_ours(args):
     for s in range(args.warmup):
         step(s)
     torch.cuda.synchronize(dev)
-    if world > 1:
+    if distributed:
         dist.barrier()
     torch.cuda.synchronize(dev)
     evs = []
@@ -258,12 +261,12 @@ def run_ours(args):
             b.record(stream)
             evs.append((a, b))
         torch.cuda.synchronize(dev)
-    if world > 1:
+    if distributed:
         dist.barrier()
     torch.cuda.synchronize(dev)
     step_ms = [a.elapsed_time(b) for a, b in evs]
     ms = statistics.mean(step_ms)
-    if world > 1:
+    if distributed:
         t = torch.tensor([ms], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
@@ -306,7 +309,7 @@ def run_ours(args):
             "clocks": cs,
             "singular_jobs": info_bad,
         }
-    if world > 1:
+    if distributed:
         dist.barrier()
 
     # end to end through the C ABI with host buffers (copies in the timed region)
@@ -315,13 +318,13 @@ def run_ours(args):
         for s in range(min(args.warmup, 2)):
             eng.transmission(E_host[s])
         torch.cuda.synchronize(dev)
-        if world > 1:
+        if distributed:
             dist.barrier()
         t0 = time.perf_counter()
         for s in range(args.steps):
             tau_h, _ = eng.transmission(E_host[args.warmup + s])
         el = time.perf_counter() - t0
-        if world > 1:
+        if distributed:
             t = torch.tensor([el], dtype=torch.float64, device=dev)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             el = float(t.item())
@@ -336,10 +339,25 @@ def run_ours(args):
         r, t = cpu_rate(pr, E_all[::7], nth)
         line["cpu_baseline"] = {"value": r, "unit": UNIT, "cores": nth, "kind": "port",
                                 "sample": f"{nth} sweeps of this workload, one per thread, {t[0]:.1f} s"}
+    if args.density:
+        # the density path (D mode + contour, negf.f90:9-113) on the same device, as
+        # information beside the headline: contour jobs per second
+        a = pr.atomic
+        nl = P.n_line(a, w.deck.N_line_per_eV)
+        nc = w.deck.N_circle
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        _, info_d = eng.equilibrium_density(nc, nl, pr.min_V, a.MU, a.GAP, a.TEMPERATURE)
+        el = time.perf_counter() - t0
+        if rank == 0:
+            njd = (nc + nl) * nk
+            line["density"] = {"jobs": njd, "seconds": el, "jobs_per_s": njd / el,
+                               "device_ms": eng.last_stats.device_ms,
+                               "flops_per_job": 24.0 * pr.N ** 3 * pr.Nz, "info": info_d}
     if rank == 0:
         print(json.dumps(line), flush=True)
     eng.close()
-    if world > 1:
+    if distributed:
         dist.destroy_process_group()
 
 
