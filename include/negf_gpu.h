@@ -72,6 +72,11 @@ typedef struct negf_stats {
 int negf_basis_size(double encut, double lx, double ly, int32_t *n);
 /* PlaneWaveBasis_construction, grid.f90:410-431; nx, ny have room for n */
 int negf_basis(double encut, double lx, double ly, int32_t n, int32_t *nx, int32_t *ny);
+/* Basis of one k-point, |k+G|^2/2 <= encut, in the enumeration order of
+ * grid.f90:420-429 (a per-k basis; the reference uses the k = 0 set for every
+ * k).  *count receives the size; nx, ny (room for n) may be NULL to query it. */
+int negf_basis_k(double encut, double lx, double ly, double kx, double ky, int32_t n, int32_t *count,
+                 int32_t *nx, int32_t *ny);
 /* Kpoint_mesh_construction, grid.f90:433-448; out[3*i] = kx, ky, weight */
 int negf_kmesh(int32_t nkx, int32_t nky, double lx, double ly, double *out);
 /* LocalPotential_RealToPlanewave per slice + the truncated copy of
@@ -108,6 +113,16 @@ int negf_tri_solve(negf_ctx *ctx, const double *D, int32_t N, int32_t Nz, const 
  * tau[e] = sum_k weight_k * tau(E_e, k), the reduced Transmission(:)%tau. */
 int negf_transmission(negf_ctx *ctx, const double *energies, int32_t nE, int32_t precision,
                       double *tau, negf_stats *stats);
+
+/* negf_transmission for nctx problems at once -- e.g. one per k-point with a
+ * per-k basis, or several devices of different length -- on the device of
+ * ctxs[0] (all contexts must share it).  One persistent launch per kernel
+ * variant takes the (problem, E, k) jobs largest-first from a counter.  The
+ * energies are shared; tau[p*nE + e] = sum over the k-points of ctxs[p] of
+ * weight * tau.  A multi-problem generalisation of the job loop of
+ * main.f90:384-407 (the reference runs one problem per process). */
+int negf_transmission_batch(negf_ctx *const *ctxs, int32_t nctx, const double *energies, int32_t nE,
+                            double *tau, negf_stats *stats);
 
 /* Same computation on device-resident buffers, enqueued on `stream`
  * (a cudaStream_t; NULL = legacy default stream), no synchronisation.

@@ -24,7 +24,7 @@ EXPORTS = (
     "negf_basis_size", "negf_basis", "negf_kmesh", "negf_vhat", "negf_ctx_create",
     "negf_ctx_destroy", "negf_tri_solve", "negf_transmission", "negf_transmission_device",
     "negf_density", "negf_ldos_matrix", "negf_ptor", "negf_version", "negf_transmission_noalloc",
-    "negf_density_real", "negf_ldos",
+    "negf_density_real", "negf_ldos", "negf_basis_k", "negf_transmission_batch",
 )
 
 _dp = C.POINTER(C.c_double)
@@ -86,6 +86,9 @@ def lib():
                                     C.POINTER(Stats)]
     L.negf_ldos.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int32, _ip, C.c_int32, C.c_int32, _dp,
                             C.c_double, _dp, C.POINTER(Stats)]
+    L.negf_basis_k.argtypes = [C.c_double] * 5 + [C.c_int32, _ip, _ip, _ip]
+    L.negf_transmission_batch.argtypes = [C.POINTER(C.c_void_p), C.c_int32, _dp, C.c_int32, _dp,
+                                          C.POINTER(Stats)]
     L.negf_ptor.argtypes = [_dp, _ip, _ip, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _dp]
     _lib = L
     return L

@@ -37,63 +37,111 @@ struct RgfJob {
 };
 
 // ------------------------------------------------------------------ kernels
+// One F-mode sweep and the transmission trace for the job (E = e + i*eta,
+// k-point ik) of problem g, in the workspace A0 (four ld x N blocks).  The
+// basis must already be in s.nx / s.ny.  Returns tau in *tau (thread 0) and
+// the LAPACK-style info.
+template <int NB, int RPT>
+__device__ int transmission_job(const Geo &g, const Smem &s, double e, int ik, double2 *A0, double *tau) {
+    const int N = g.N, ld = g.ld, Nz = g.Nz;
+    double2 *A1 = A0 + (size_t)ld * N;
+    double2 *P0 = A1 + (size_t)ld * N;
+    double2 *P1 = P0 + (size_t)ld * N;
+    const double2 E = make_double2(e, g.eta);
+    job_vectors(g, s, E, e, ik);
+    __syncthreads();
+    open_rows(N, s);
+    __syncthreads();
+    const int nr = *s.nrows;
+    double2 *cur = A0, *oth = A1, *P = P0, *Pn = P1;
+    // generator_r(N_z-1) = inv(D_Nz)          math_kernel.f90:82
+    form_block(cur, g, s, Nz - 1, E, ik, nullptr, nullptr);
+    __syncthreads();
+    int info = gj_invert<NB, RPT>(cur, N, ld, s);
+    unpermute_rows(P, ld, cur, ld, N, nr, s);
+    __syncthreads();
+    // generator_r(m) = inv(D_{m+1} - generator_r(m+1)), with the rows of the
+    // running product P = gR(Nz-1) ... gR(m) of the first-column chain
+    // G_{Nz,1} = (-1)^(Nz-1) gR(Nz-1) ... gR(1) G_11 (math_kernel.f90:83-90,120-128)
+    // that the trace reads
+    for (int m = Nz - 3; m >= 0; --m) {
+        form_block(oth, g, s, m + 1, E, ik, cur, nullptr);
+        __syncthreads();
+        const int r = gj_invert<NB, RPT>(oth, N, ld, s);
+        if (r && !info) info = r;
+        GemmArgs ga{Pn, ld, P, ld, s.iprow, oth, ld, s.iprow, nr, N, N, nullptr};
+        cta_gemm(ga, s, GEMM_STORE, g.delta);
+        __syncthreads();
+        double2 *t = cur; cur = oth; oth = t;
+        t = P; P = Pn; Pn = t;
+    }
+    // G_11 = inv(D_1 - generator_r(1))          math_kernel.f90:113-118
+    form_block(oth, g, s, 0, E, ik, cur, nullptr);
+    __syncthreads();
+    const int r = gj_invert<NB, RPT>(oth, N, ld, s);
+    if (r && !info) info = r;
+    // tau = sum_ij gamma_L,i gamma_R,j |2 dz^2 G_{Nz,1}(i,j)|^2   grid.f90:362-383
+    GemmArgs ga{nullptr, 0, P, ld, s.iprow, oth, ld, s.iprow, nr, N, N, s.rows};
+    double t = cta_gemm(ga, s, GEMM_TAU, g.delta);
+    t = block_sum(t, s);
+    *tau = t;
+    return info;
+}
+
 template <int NB, int RPT, int MINB>
 __global__ void __launch_bounds__(NT, MINB)
     k_transmission(Geo g, const double *__restrict__ energies, int nE, int njobs, double2 *ws,
                    size_t wstride, double *tau_jobs, int *info_jobs) {
     extern __shared__ __align__(256) unsigned char smem[];
     Smem s = carve<NB>(smem, g.N);
-    const int N = g.N, ld = g.ld, Nz = g.Nz;
-    for (int i = threadIdx.x; i < N; i += NT) { s.nx[i] = g.nx[i]; s.ny[i] = g.ny[i]; }
+    for (int i = threadIdx.x; i < g.N; i += NT) { s.nx[i] = g.nx[i]; s.ny[i] = g.ny[i]; }
     __syncthreads();
     double2 *A0 = ws + (size_t)blockIdx.x * wstride;
-    double2 *A1 = A0 + (size_t)ld * N;
-    double2 *P0 = A1 + (size_t)ld * N;
-    double2 *P1 = P0 + (size_t)ld * N;
     for (int job = blockIdx.x; job < njobs; job += gridDim.x) {
         // job -> (energy, k-point), energy fastest: negf.f90:131-133
         const int ie = job % nE, ik = job / nE;
-        const double e = energies[ie];
-        const double2 E = make_double2(e, g.eta);
-        job_vectors(g, s, E, e, ik);
-        __syncthreads();
-        open_rows(N, s);
-        __syncthreads();
-        const int nr = *s.nrows;
-        double2 *cur = A0, *oth = A1, *P = P0, *Pn = P1;
-        // generator_r(N_z-1) = inv(D_Nz)          math_kernel.f90:82
-        form_block(cur, g, s, Nz - 1, E, ik, nullptr, nullptr);
-        __syncthreads();
-        int info = gj_invert<NB, RPT>(cur, N, ld, s);
-        unpermute_rows(P, ld, cur, ld, N, nr, s);
-        __syncthreads();
-        // generator_r(m) = inv(D_{m+1} - generator_r(m+1)), with the rows of the
-        // running product P = gR(Nz-1) ... gR(m) of the first-column chain
-        // G_{Nz,1} = (-1)^(Nz-1) gR(Nz-1) ... gR(1) G_11 (math_kernel.f90:83-90,120-128)
-        // that the trace reads
-        for (int m = Nz - 3; m >= 0; --m) {
-            form_block(oth, g, s, m + 1, E, ik, cur, nullptr);
-            __syncthreads();
-            const int r = gj_invert<NB, RPT>(oth, N, ld, s);
-            if (r && !info) info = r;
-            GemmArgs ga{Pn, ld, P, ld, s.iprow, oth, ld, s.iprow, nr, N, N, nullptr};
-            cta_gemm(ga, s, GEMM_STORE, g.delta);
-            __syncthreads();
-            double2 *t = cur; cur = oth; oth = t;
-            t = P; P = Pn; Pn = t;
-        }
-        // G_11 = inv(D_1 - generator_r(1))          math_kernel.f90:113-118
-        form_block(oth, g, s, 0, E, ik, cur, nullptr);
-        __syncthreads();
-        const int r = gj_invert<NB, RPT>(oth, N, ld, s);
-        if (r && !info) info = r;
-        // tau = sum_ij gamma_L,i gamma_R,j |2 dz^2 G_{Nz,1}(i,j)|^2   grid.f90:362-383
-        GemmArgs ga{nullptr, 0, P, ld, s.iprow, oth, ld, s.iprow, nr, N, N, s.rows};
-        double t = cta_gemm(ga, s, GEMM_TAU, g.delta);
-        t = block_sum(t, s);
+        double t = 0.0;
+        const int info = transmission_job<NB, RPT>(g, s, energies[ie], ik, A0, &t);
         if (threadIdx.x == 0) {
             tau_jobs[job] = t;
             if (info_jobs) info_jobs[job] = info;
+        }
+        __syncthreads();
+    }
+}
+
+// One (problem, energy, k-point) job of a batch over several problems.
+struct BatchJob {
+    int prob, ie, ik, pad;
+};
+
+// Several problems (each its own basis, V table, slices and k-points) in one
+// persistent launch: CTAs take jobs from a counter in the given order
+// (largest first), so long and short sweeps balance across the SMs.
+template <int NB, int RPT, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
+    k_transmission_batch(const Geo *__restrict__ geos, const BatchJob *__restrict__ jobs, int njobs,
+                         const double *__restrict__ energies, double2 *ws, size_t wstride, double *tau_jobs,
+                         int *info_jobs, int *counter) {
+    extern __shared__ __align__(256) unsigned char smem[];
+    __shared__ int next;
+    double2 *A0 = ws + (size_t)blockIdx.x * wstride;
+    for (;;) {
+        if (threadIdx.x == 0) next = atomicAdd(counter, 1);
+        __syncthreads();
+        const int q = next;
+        __syncthreads();
+        if (q >= njobs) break;
+        const BatchJob jb = jobs[q];
+        const Geo g = geos[jb.prob];
+        Smem s = carve<NB>(smem, g.N);
+        for (int i = threadIdx.x; i < g.N; i += NT) { s.nx[i] = g.nx[i]; s.ny[i] = g.ny[i]; }
+        __syncthreads();
+        double t = 0.0;
+        const int info = transmission_job<NB, RPT>(g, s, energies[jb.ie], jb.ik, A0, &t);
+        if (threadIdx.x == 0) {
+            tau_jobs[q] = t;
+            info_jobs[q] = info;
         }
         __syncthreads();
     }
@@ -928,6 +976,121 @@ done:
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------ batches of problems
+extern "C" int negf_transmission_batch(negf_ctx *const *ctxs, int32_t nctx, const double *energies, int32_t nE,
+                                       double *tau, negf_stats *stats) {
+    if (!ctxs || nctx < 1 || !energies || !tau || nE < 1) return NEGF_ERR_ARG;
+    for (int p = 0; p < nctx; ++p)
+        if (!ctxs[p] || ctxs[p]->device != ctxs[0]->device) return NEGF_ERR_ARG;
+    negf_ctx *c0 = ctxs[0];
+    if (cudaSetDevice(c0->device) != cudaSuccess) return NEGF_ERR_CUDA;
+    cudaStream_t st = c0->stream;
+    std::fill(tau, tau + (size_t)nctx * nE, 0.0);
+    double *d_E = nullptr;
+    CK(cudaMalloc(&d_E, sizeof(double) * nE));
+    CK(cudaMemcpyAsync(d_E, energies, sizeof(double) * nE, cudaMemcpyHostToDevice, st));
+    std::vector<int> info_all;
+    double ms_all = 0;
+    int rc = 0;
+    for (int v = V16x1; v <= V8x4 && !rc; ++v) {
+        std::vector<int> members;
+        for (int p = 0; p < nctx; ++p)
+            if (pick_variant(ctxs[p]->N) == v) members.push_back(p);
+        if (members.empty()) continue;
+        std::vector<Geo> geos;
+        std::vector<BatchJob> jobs;
+        std::vector<double> cost;
+        int nmax = 0;
+        for (int m = 0; m < (int)members.size(); ++m) {
+            negf_ctx *c = ctxs[members[m]];
+            geos.push_back(make_geo(c));
+            nmax = std::max(nmax, c->N);
+            for (int ik = 0; ik < c->nk; ++ik)
+                for (int ie = 0; ie < nE; ++ie) {
+                    jobs.push_back(BatchJob{m, ie, ik, 0});
+                    cost.push_back((double)c->N * c->N * c->N * c->Nz);
+                }
+        }
+        // largest sweeps first, so the last wave holds the short ones
+        std::vector<int> order(jobs.size());
+        for (size_t q = 0; q < order.size(); ++q) order[q] = (int)q;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+        std::vector<BatchJob> sorted(jobs.size());
+        for (size_t q = 0; q < order.size(); ++q) sorted[q] = jobs[order[q]];
+        const int njobs = (int)sorted.size();
+        const Variant var = (Variant)v;
+        const size_t smem = variant_smem(var, nmax);
+        int occ = 1;
+        switch (var) {
+            case V16x1: rc = prep_kernel(k_transmission_batch<16, 1, 2>, smem, &occ); break;
+            case V16x2: rc = prep_kernel(k_transmission_batch<16, 2, 1>, smem, &occ); break;
+            default: rc = prep_kernel(k_transmission_batch<8, 4, 1>, smem, &occ); break;
+        }
+        if (rc) break;
+        const int grid = std::min(njobs, c0->num_sms * occ);
+        const size_t wstride = 4 * (size_t)round_up(nmax, 8) * nmax;
+        if ((rc = ensure_ws(c0, sizeof(double2) * wstride * grid))) break;
+        Geo *d_geo = nullptr;
+        BatchJob *d_jobs = nullptr;
+        double *d_tj = nullptr;
+        int *d_info = nullptr, *d_counter = nullptr;
+        if (cudaMalloc(&d_geo, sizeof(Geo) * geos.size()) != cudaSuccess ||
+            cudaMalloc(&d_jobs, sizeof(BatchJob) * njobs) != cudaSuccess ||
+            cudaMalloc(&d_tj, sizeof(double) * njobs) != cudaSuccess ||
+            cudaMalloc(&d_info, sizeof(int) * njobs) != cudaSuccess ||
+            cudaMalloc(&d_counter, sizeof(int)) != cudaSuccess) {
+            cudaGetLastError();
+            rc = NEGF_ERR_NOMEM;
+        }
+        std::vector<double> tj(njobs);
+        std::vector<int> info(njobs);
+        float ms = 0.f;
+        if (!rc) {
+            if (cudaMemcpyAsync(d_geo, geos.data(), sizeof(Geo) * geos.size(), cudaMemcpyHostToDevice, st) ||
+                cudaMemcpyAsync(d_jobs, sorted.data(), sizeof(BatchJob) * njobs, cudaMemcpyHostToDevice, st) ||
+                cudaMemsetAsync(d_counter, 0, sizeof(int), st) || cudaEventRecord(c0->ev0, st))
+                rc = NEGF_ERR_CUDA;
+        }
+        if (!rc) {
+            double2 *ws = (double2 *)c0->d_ws;
+            switch (var) {
+                case V16x1:
+                    k_transmission_batch<16, 1, 2><<<grid, NT, smem, st>>>(d_geo, d_jobs, njobs, d_E, ws, wstride, d_tj, d_info, d_counter);
+                    break;
+                case V16x2:
+                    k_transmission_batch<16, 2, 1><<<grid, NT, smem, st>>>(d_geo, d_jobs, njobs, d_E, ws, wstride, d_tj, d_info, d_counter);
+                    break;
+                default:
+                    k_transmission_batch<8, 4, 1><<<grid, NT, smem, st>>>(d_geo, d_jobs, njobs, d_E, ws, wstride, d_tj, d_info, d_counter);
+                    break;
+            }
+            if (cudaGetLastError() || cudaEventRecord(c0->ev1, st) ||
+                cudaMemcpyAsync(tj.data(), d_tj, sizeof(double) * njobs, cudaMemcpyDeviceToHost, st) ||
+                cudaMemcpyAsync(info.data(), d_info, sizeof(int) * njobs, cudaMemcpyDeviceToHost, st) ||
+                cudaStreamSynchronize(st) || cudaEventElapsedTime(&ms, c0->ev0, c0->ev1))
+                rc = NEGF_ERR_CUDA;
+        }
+        cudaFree(d_geo); cudaFree(d_jobs); cudaFree(d_tj); cudaFree(d_info); cudaFree(d_counter);
+        if (rc) break;
+        ms_all += ms;
+        // tau[p][e] = sum_k w_k tau(p, e, k), summed in k order (negf.f90:172)
+        std::vector<double> per(jobs.size());
+        for (size_t q = 0; q < order.size(); ++q) per[order[q]] = tj[q];
+        size_t q = 0;
+        for (int m = 0; m < (int)members.size(); ++m) {
+            negf_ctx *c = ctxs[members[m]];
+            const int pg = members[m];
+            for (int ik = 0; ik < c->nk; ++ik)
+                for (int ie = 0; ie < nE; ++ie, ++q) tau[(size_t)pg * nE + ie] += per[q] * c->kpt[3 * ik + 2];
+        }
+        for (size_t qq = 0; qq < order.size(); ++qq) info_all.push_back(info[qq]);
+    }
+    cudaFree(d_E);
+    if (rc) return rc;
+    fill_stats(stats, info_all, ms_all);
+    return first_info(info_all);
+}
 
 // ------------------------------------------------------ real-space outputs
 namespace {

@@ -61,6 +61,28 @@ int negf_basis(double encut, double lx, double ly, int32_t n, int32_t *nx, int32
     return NEGF_OK;
 }
 
+// |k+G|^2/2 <= encut around one k-point, enumerated j outer / i inner like
+// grid.f90:420-429 (the reference's basis is the k = 0 case).
+int negf_basis_k(double encut, double lx, double ly, double kx, double ky, int32_t n, int32_t *count,
+                 int32_t *nx, int32_t *ny) {
+    if (!count || !(lx > 0) || !(ly > 0) || !(encut >= 0)) return NEGF_ERR_ARG;
+    const double gc = std::sqrt(2 * encut);
+    const int i0 = (int)std::floor((-gc - kx) * lx / (2 * PI)) - 1, i1 = (int)std::ceil((gc - kx) * lx / (2 * PI)) + 1;
+    const int j0 = (int)std::floor((-gc - ky) * ly / (2 * PI)) - 1, j1 = (int)std::ceil((gc - ky) * ly / (2 * PI)) + 1;
+    int c = 0;
+    for (int j = j0; j <= j1; ++j)
+        for (int i = i0; i <= i1; ++i) {
+            const double gx = (double)(2 * i) * PI / lx + kx, gy = (double)(2 * j) * PI / ly + ky;
+            if ((gx * gx + gy * gy) / 2 <= encut) {
+                if (nx && ny && c < n) { nx[c] = i; ny[c] = j; }
+                ++c;
+            }
+        }
+    *count = c;
+    if ((nx || ny) && c > n) return NEGF_ERR_ARG;
+    return NEGF_OK;
+}
+
 int negf_kmesh(int32_t nkx, int32_t nky, double lx, double ly, double *out) {
     if (!out || nkx < 1 || nky < 1) return NEGF_ERR_ARG;
     for (int j = 1; j <= nky; ++j)

@@ -64,3 +64,15 @@ def Greensfunction_PlanewaveToReal(subGreenFunc, nx_grid, ny_grid, N_x, N_y):
         np.ascontiguousarray(ny_grid, np.int32).ctypes.data_as(_ip), N, nzs, N_x, N_y,
         out.ctypes.data_as(_dp)))
     return out[:, :, 0] if squeeze else out
+
+
+def PlaneWaveBasis_k(ENCUT, Lx, Ly, kx, ky):
+    """Per-k basis |k+G|^2/2 <= ENCUT in the reference's enumeration order."""
+    n = C.c_int32(0)
+    check("negf_basis_k", lib().negf_basis_k(ENCUT, Lx, Ly, kx, ky, 0, C.byref(n), None, None))
+    nx = np.zeros(n.value, np.int32)
+    ny = np.zeros(n.value, np.int32)
+    cnt = C.c_int32(0)
+    check("negf_basis_k", lib().negf_basis_k(ENCUT, Lx, Ly, kx, ky, n.value, C.byref(cnt),
+                                              nx.ctypes.data_as(_ip), ny.ctypes.data_as(_ip)))
+    return nx, ny

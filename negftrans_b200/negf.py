@@ -151,6 +151,18 @@ class Engine:
         return np.transpose(out, (0, 3, 2, 1)), rc
 
 
+def transmission_batch(engines, energies):
+    """tau (n_problems, nE) for several Engines on one device in one persistent
+    launch per kernel variant (largest sweeps first)."""
+    e = np.ascontiguousarray(energies, np.float64)
+    arr = (C.c_void_p * len(engines))(*[eng.handle.value for eng in engines])
+    tau = np.zeros((len(engines), len(e)))
+    st = Stats()
+    rc = check("negf_transmission_batch", lib().negf_transmission_batch(
+        arr, len(engines), e.ctypes.data_as(_dp), len(e), tau.ctypes.data_as(_dp), C.byref(st)))
+    return tau, rc, st
+
+
 def GreensFunction_tri_solver(G_inv_D, DFL, engine: Engine | None = None):
     """math_kernel.f90:44-165 on the GPU.
 

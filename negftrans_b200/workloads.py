@@ -92,3 +92,36 @@ def config(name: str, nz: int | None = None) -> Workload:
         V = MSTAR * qpc_potential(32, 32, nz, 100.0, nz * 1.0, 0.050, 15.0, nz / 10.0, disorder=0.002)
         return Workload(name, _deck(nz * 10.0, float(enc) * 1e-3, 30.0, 16), V, 16)
     raise KeyError(name)
+
+
+def batched_uneven(nkx=4, nzs=(300, 600, 1200), encut_eV=0.0105288, grid=64, seed=4000):
+    """Problems of the uneven batch: one per (device, k-point) of an nkx x nkx
+    Monkhorst-Pack mesh, each with its own basis |k+G| <= G_c (sizes vary with
+    k), devices of N_z slices of 1 nm with seeded V_g ~ U[20, 80] meV and
+    w ~ U[8, 25] nm (+ GaAs scaling).  Returns a list of dicts holding the
+    Engine arguments ('args'), 'N', 'Nz' and the device index."""
+    from .grid import Kpoint_mesh_construction, PlaneWaveBasis_k, V_reciprocal_all
+    from .constants import A_0
+    rng = np.random.Generator(np.random.PCG64(seed))
+    L = 1000.0 / A_0
+    enc = encut_eV / HARTREE
+    kp = Kpoint_mesh_construction(nkx, nkx, L, L)
+    bases = [PlaneWaveBasis_k(enc, L, L, kx, ky) for kx, ky, _ in kp]
+    nmax = max(int(np.max(np.abs(np.concatenate([b[0], b[1]])))) for b in bases)
+    # the reference's NGX (main.f90:94-100), raised so that every pair
+    # difference of a shifted basis indexes inside the table; the table keeps
+    # the reference's window |dn| <= NGX/2 (main.f90:242-244)
+    from .prepare import InputDeck, ngrid
+    ng = max(max(ngrid(InputDeck(LX=1000.0, LY=1000.0, ENCUT=encut_eV))), 2 * nmax)
+    out = []
+    for d, nz in enumerate(nzs):
+        vg = rng.uniform(0.020, 0.080)
+        w = rng.uniform(8.0, 25.0)
+        V = MSTAR * qpc_potential(grid, grid, nz, 100.0, nz * 1.0, vg, w, 20.0)
+        vhat = V_reciprocal_all(V / HARTREE, ng, ng)
+        lz = nz * 10.0 / A_0
+        for (kx, ky, wk), (nx, ny) in zip(kp, bases):
+            out.append({"device": d, "Nz": nz, "N": len(nx),
+                        "args": (nx, ny, vhat, L, L, lz, 0.0, 0.0, MSTAR * 1e-6 / HARTREE,
+                                 np.array([[kx, ky, wk]]))})
+    return out

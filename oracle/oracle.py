@@ -115,6 +115,25 @@ def basis(encut, lx, ly):
     return nx, ny
 
 
+def basis_k(encut, lx, ly, kx, ky):
+    """Per-k basis |k+G|^2/2 <= encut in the j-outer / i-inner order of
+    grid.f90:420-429 (restated in Python; the engine's is C++)."""
+    gc = np.sqrt(2 * encut)
+    i0 = int(np.floor((-gc - kx) * lx / (2 * PI))) - 2
+    i1 = int(np.ceil((gc - kx) * lx / (2 * PI))) + 2
+    j0 = int(np.floor((-gc - ky) * ly / (2 * PI))) - 2
+    j1 = int(np.ceil((gc - ky) * ly / (2 * PI))) + 2
+    nx, ny = [], []
+    for j in range(j0, j1 + 1):
+        for i in range(i0, i1 + 1):
+            gx = (2.0 * i) * PI / lx + kx
+            gy = (2.0 * j) * PI / ly + ky
+            if (gx * gx + gy * gy) / 2 <= encut:
+                nx.append(i)
+                ny.append(j)
+    return np.array(nx, np.int32), np.array(ny, np.int32)
+
+
 def kmesh(nkx, nky, lx, ly):
     out = np.zeros((nkx * nky, 3))
     lib().oracle_kmesh(C.c_int32(nkx), C.c_int32(nky), C.c_double(lx), C.c_double(ly), _d(out))

@@ -228,3 +228,28 @@ def test_ldos_real_space(oracle, grid):
         ref = oracle.ldos_from_matrix(mat, pr.nx, pr.ny, Nx, Ny, LX, LY, LZ, grid)
         assert got.shape[:3] == ref.shape
         assert rel_err(got[..., ie], ref) < RTOL
+
+
+def test_transmission_batch_uneven(oracle):
+    """Per-k bases and devices of different length in one persistent launch per
+    kernel variant, each problem against the oracle; one problem has N > 256
+    (second variant)."""
+    from negftrans_b200.negf import transmission_batch
+    probs = W.batched_uneven(nkx=2, nzs=(4, 7), encut_eV=1.2e-3, grid=32)
+    V = W.MSTAR * W.qpc_potential(64, 64, 3, 100.0, 3.0, 0.05, 15.0, 1.0, disorder=0.002)
+    big = P.prepare(W._deck(30.0, 14.5e-3, 30.0, 16), V)
+    probs.append({"device": 2, "Nz": 3, "N": big.N, "args": big.engine_args()})
+    assert len({p["N"] for p in probs}) > 1 and max(p["N"] for p in probs) > 256
+    E = np.linspace(0.0, 0.067 * 0.03 / HARTREE, 6, endpoint=False)
+    engines = [Engine(*p["args"]) for p in probs]
+    try:
+        tau, info, _ = transmission_batch(engines, E)
+    finally:
+        for e in engines:
+            e.close()
+    assert info == 0
+    for p, t in zip(probs, tau):
+        nx, ny, vhat, lx, ly, lz, vl, vr, eta, kp = p["args"]
+        ref, _ = oracle.transmission_jobs(oracle.Problem(nx, ny, vhat, lx, ly, lz, vl, vr, eta, kp), E,
+                                          nthreads=8)
+        np.testing.assert_allclose(t, ref, rtol=RTOL, atol=1e-12)
