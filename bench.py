@@ -299,7 +299,9 @@ def run_ours(args):
                          "frac": achieved / peak, "traffic": None,
                          "peak_source": "measured in-run: cuBLAS FP64 GEMM 8192^3 (MEASURED_PEAKS.json "
                                         "has no FP64 figure)",
-                         "flops_per_launch": fl, "kernel": "k_transmission<16,1,2>",
+                         "flops_per_launch": fl,
+                         "kernel": ("k_transmission<16,1,2>" if N <= 256 else
+                                    "k_transmission<16,2,1>" if N <= 512 else "k_transmission<8,4,1>"),
                          "flops_note": "executed: 8N^3 per inverse + 8 n_open N^2 per chain product "
                                        "(rows of G_{Nz,1} with gamma_L != 0); the reference's "
                                        "16 N^3 N_z per sweep is reported as reference_equiv_tflops",
@@ -361,10 +363,50 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_batched(args):
+    """Uneven batch: one problem per (device, k-point) of a 4x4 mesh with per-k
+    bases, devices of 300/600/1200 slices; a step = --batch energies for every
+    problem through negf_transmission_batch (one persistent launch)."""
+    import torch
+
+    from negftrans_b200 import workloads as W
+    from negftrans_b200.negf import Engine, transmission_batch
+    probs = W.batched_uneven()
+    engines = [Engine(*p["args"]) for p in probs]
+    E_all = np.linspace(0.0, W.MSTAR * 0.030 / 27.211386245988, 1024, endpoint=False)
+    perm = np.random.default_rng(2024).permutation(len(E_all))
+    B = args.batch
+    batches = [E_all[perm[(s * B + np.arange(B)) % len(E_all)]] for s in range(args.warmup + args.steps)]
+    for s in range(args.warmup):
+        transmission_batch(engines, batches[s])
+    times, dev_ms = [], []
+    for s in range(args.steps):
+        t0 = time.perf_counter()
+        _, info, st = transmission_batch(engines, batches[args.warmup + s])
+        times.append(time.perf_counter() - t0)
+        dev_ms.append(st.device_ms)
+    njobs = B * len(probs)
+    ms = statistics.mean(dev_ms)
+    flops = sum(8.0 * p["N"] ** 3 * p["Nz"] for p in probs) * B
+    line = {"metric": METRIC, "value": njobs / (ms * 1e-3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": {"workload": "batched_uneven", "problems": len(probs),
+                       "N_range": [min(p["N"] for p in probs), max(p["N"] for p in probs)],
+                       "Nz": sorted({p["Nz"] for p in probs}), "energies_per_step": B},
+            "inverse_tflops": flops / (ms * 1e-3) / 1e12, "e2e_seconds_per_step": statistics.mean(times),
+            "singular": info}
+    print(json.dumps(line), flush=True)
+    for e in engines:
+        e.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batched_uneven":
+        run_batched(args)
     else:
         run_ours(args)
 
