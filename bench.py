@@ -29,6 +29,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "RGF energy-point solves/s"
+TRAFFIC_PER_JOB_SLICE_N221 = 65.513e9 / (296 * 16)   # profiles/k_transmission_n221.md
 UNIT = "solves/s"
 
 
@@ -296,7 +297,12 @@ def run_ours(args):
                        "l2": "256 MB buffer written between timed steps; per-job workspace "
                              f"{4 * ((N + 7) // 8 * 8) * N * 16 * min(B * nk, 148) / 1e6:.0f} MB > L2"},
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak,
+                         # ncu dram read+write of this kernel per job-slice at N = 221 (a 296-job,
+                         # 16-slice capture), scaled by the job-slices of one launch
+                         "traffic": (TRAFFIC_PER_JOB_SLICE_N221 * B * nk * Nz
+                                     if N == 221 and args.nz in (0, Nz) else None),
+                         "traffic_unit": "bytes per launch",
                          "peak_source": "measured in-run: cuBLAS FP64 GEMM 8192^3 (MEASURED_PEAKS.json "
                                         "has no FP64 figure)",
                          "flops_per_launch": fl,
