@@ -29,7 +29,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "RGF energy-point solves/s"
-TRAFFIC_PER_JOB_SLICE_N221 = 65.513e9 / (296 * 16)   # profiles/k_transmission_n221.md
+# ncu dram bytes (read + write) of k_transmission per job-slice at N = 221, measured on a
+# 296-job, 16-slice launch (same per-slice work as the full workload)
+TRAFFIC_PER_JOB_SLICE_N221 = 65.513e9 / (296 * 16)
 UNIT = "solves/s"
 
 

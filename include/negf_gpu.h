@@ -3,7 +3,7 @@
  *
  * Drop-in for the hot path of NEGFtrans: src/negf.f90 (the per-job drivers)
  * and src/math_kernel.f90 (the RGF solver), called from Fortran through
- * iso_c_binding (see INTEGRATION.md) or from C/C++/Python directly.
+ * iso_c_binding or from C/C++/Python directly.
  *
  * Conventions
  *  - Plain C types only.  Complex numbers are interleaved (re, im) doubles,
