@@ -132,8 +132,8 @@ struct Smem {
     double2 *sigR;  // [N] exp(i q_R dz)
     double *gL;     // [N] gamma_L  sin(q dz)/dz^2 (grid.f90:365)
     double *gR;     // [N] gamma_R
-    double2 *srow;  // [NBMAX] pivot row of the panel step
-    Red *red;       // [NWARP]
+    double2 *cand;  // [2][NWARP][32] each warp's pivot candidate row (double-buffered by step)
+    Red *red;       // [2][NWARP] each warp's candidate key and reciprocal
     double *fred;   // [NWARP] float reductions
     double2 *big;   // union: sub-panel + block | trailing rows + W tile | GEMM stages
     int ldw;
@@ -153,8 +153,8 @@ __host__ __device__ inline size_t smem_bytes(int N) {
     b += 6 * (size_t)round_up(N, 4) * sizeof(int) + 4 * sizeof(int);
     b += 2 * (size_t)round_up(N, 2) * sizeof(double2);
     b += 2 * (size_t)round_up(N, 2) * sizeof(double);
-    b += 32 * sizeof(double2);
-    b += NWARP * sizeof(Red) + NWARP * sizeof(double);
+    b += 2 * NWARP * 32 * sizeof(double2);
+    b += 2 * NWARP * sizeof(Red) + NWARP * sizeof(double);
     b = (b + 255) / 256 * 256;
     return b + big * sizeof(double2);
 }
@@ -174,9 +174,9 @@ __device__ inline Smem carve(unsigned char *base, int N) {
     s.sigR = s.sigL + n2;
     s.gL = (double *)(s.sigR + n2);
     s.gR = s.gL + n2;
-    s.srow = (double2 *)(s.gR + n2);
-    s.red = (Red *)(s.srow + 32);
-    s.fred = (double *)(s.red + NWARP);
+    s.cand = (double2 *)(s.gR + n2);
+    s.red = (Red *)(s.cand + 2 * NWARP * 32);
+    s.fred = (double *)(s.red + 2 * NWARP);
     size_t off = (size_t)((unsigned char *)(s.fred + NWARP) - base);
     off = (off + 255) / 256 * 256;
     s.big = (double2 *)(base + off);
@@ -537,8 +537,12 @@ __device__ inline void trailing_update(double2 *__restrict__ A, int N, int ld, i
 // next pivot column first and runs its warp-level argmax while the rest of
 // the row is updated; the winning lane of each warp computes the reciprocal
 // of its candidate before the barrier.
+// Warp-level pivot candidate for the column values f: writes the warp's best
+// key and the reciprocal of its value into red[buf][warp]; returns, in the
+// winning thread, the register row r of the candidate (-1 elsewhere).  That
+// thread publishes the candidate's updated row into cand[buf][warp] later.
 template <int NB, int RPT>
-__device__ inline void warp_pivot(const double2 (&f)[RPT], unsigned used, const Smem &s) {
+__device__ inline int warp_pivot(const double2 (&f)[RPT], unsigned used, int buf, const Smem &s) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     unsigned long long key = 0;
     int rbest = -1;
@@ -557,78 +561,98 @@ __device__ inline void warp_pivot(const double2 (&f)[RPT], unsigned used, const 
         const unsigned long long ok = __shfl_xor_sync(0xffffffffu, wk, o);
         wk = ok > wk ? ok : wk;
     }
-    if (lane == 0) s.red[warp].key = wk;
+    Red *red = s.red + buf * NWARP;
+    if (lane == 0) red[warp].key = wk;
     if (wk != 0 && key == wk) {
 #pragma unroll
         for (int r = 0; r < RPT; ++r)
-            if (r == rbest) s.red[warp].d = zrcp(f[r]);
+            if (r == rbest) red[warp].d = zrcp(f[r]);
+        return rbest;
     }
+    return -1;
 }
 
+// Gauss-Jordan elimination of the columns [kb, kb+nbe) of a register panel w
+// (row tid + NT*r of the block in w[r][.]) with implicit partial pivoting:
+// the pivot of each column is the unused row with the largest |re|+|im|
+// (lowest index on ties), as zgetf2 chooses.  Pivot rows get inP = tag.
+// One CTA barrier per step: every warp publishes its candidate (key,
+// reciprocal, updated row) into a slot double-buffered by step parity, so
+// after the barrier all threads read the winner's row directly.  The next
+// column is updated first and its warp argmax overlaps the rest of the row.
 template <int NB, int RPT>
 __device__ inline void factor_subpanel(double2 (&w)[RPT][NB], int kb, int nbe, unsigned &used, int &info,
                                        int tag, const Smem &s) {
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, warp = tid >> 5;
     double2 f[RPT];
 #pragma unroll
     for (int r = 0; r < RPT; ++r) f[r] = w[r][0];
-    warp_pivot<NB, RPT>(f, used, s);
-#pragma unroll 1
-    for (int kk = 0; kk < nbe; ++kk) {
-        __syncthreads();
-        unsigned long long key = s.red[0].key;
-        int q = 0;
+    int mine = warp_pivot<NB, RPT>(f, used, 0, s);
+    if (mine >= 0) {
 #pragma unroll
-        for (int j = 1; j < NWARP; ++j) {
-            const unsigned long long k = s.red[j].key;
-            if (k > key) { key = k; q = j; }
-        }
-        const double2 d = s.red[q].d;
-        const int p = 0x7FF - (int)(key & 0x7FFull);
-        if ((key >> 11) == 0 && info == 0) info = kb + kk + 1;
+        for (int r = 0; r < RPT; ++r)
+            if (r == mine) {
 #pragma unroll
-        for (int r = 0; r < RPT; ++r) {
-            if (tid + NT * r == p) {
-                used |= 1u << r;
-#pragma unroll
-                for (int jj = 0; jj < NB; ++jj) s.srow[jj] = w[r][jj];
+                for (int jj = 0; jj < NB; ++jj) s.cand[warp * 32 + jj] = w[r][jj];
             }
-        }
-        if (tid == 0) { s.prow[kb + kk] = p; s.inP[p] = tag; }
-        __syncthreads();
-        // column kk+1 first, then its pivot search overlaps the rest of the row
-        double2 gm[RPT], fn[RPT];
-        const bool more = kk + 1 < nbe;
-        double2 rn = make_double2(0.0, 0.0);
-        if (more) rn = s.srow[kk + 1];
+    }
+    // fully unrolled: every column index below is a compile-time constant
 #pragma unroll
-        for (int r = 0; r < RPT; ++r) {
-            const bool piv = (tid + NT * r == p);
-            gm[r] = piv ? make_double2(0.0, 0.0) : zmul(f[r], d);
-            double2 wn = make_double2(0.0, 0.0);
+    for (int kk = 0; kk < NB; ++kk) {
+        if (kk < nbe) {
+            const int buf = kk & 1;
+            __syncthreads();
+            const Red *red = s.red + buf * NWARP;
+            unsigned long long key = red[0].key;
+            int q = 0;
 #pragma unroll
-            for (int jj = 1; jj < NB; ++jj)
-                if (jj == kk + 1) wn = w[r][jj];
-            fn[r] = piv ? zmul(rn, d) : zfms(gm[r], rn, wn);
-        }
-        if (more) warp_pivot<NB, RPT>(fn, used, s);
+            for (int j = 1; j < NWARP; ++j) {
+                const unsigned long long k = red[j].key;
+                if (k > key) { key = k; q = j; }
+            }
+            const double2 d = red[q].d;
+            const double2 *srow = s.cand + (buf * NWARP + q) * 32;
+            const int p = 0x7FF - (int)(key & 0x7FFull);
+            if ((key >> 11) == 0 && info == 0) info = kb + kk + 1;
 #pragma unroll
-        for (int r = 0; r < RPT; ++r) {
-            const int i = tid + NT * r;
-            if (i == p) {
+            for (int r = 0; r < RPT; ++r)
+                if (tid + NT * r == p) used |= 1u << r;
+            if (tid == 0) { s.prow[kb + kk] = p; s.inP[p] = tag; }
+            // column kk+1 first, then its pivot search overlaps the rest of the row
+            const bool more = (kk + 1 < NB) && (kk + 1 < nbe);
+            double2 gm[RPT];
 #pragma unroll
-                for (int jj = 0; jj < NB; ++jj) {
-                    const double2 v = zmul(s.srow[jj], d);
-                    w[r][jj] = (jj == kk) ? d : v;
-                }
+            for (int r = 0; r < RPT; ++r) gm[r] = (tid + NT * r == p) ? make_double2(0.0, 0.0) : zmul(w[r][kk], d);
+            if (kk + 1 < NB) {
+                double2 fn[RPT];
+                const double2 rn = srow[(kk + 1) % NB];
+#pragma unroll
+                for (int r = 0; r < RPT; ++r)
+                    fn[r] = (tid + NT * r == p) ? zmul(rn, d) : zfms(gm[r], rn, w[r][(kk + 1) % NB]);
+                mine = more ? warp_pivot<NB, RPT>(fn, used, buf ^ 1, s) : -1;
             } else {
+                mine = -1;
+            }
 #pragma unroll
-                for (int jj = 0; jj < NB; ++jj) {
-                    const double2 v = zfms(gm[r], s.srow[jj], w[r][jj]);
-                    w[r][jj] = (jj == kk) ? make_double2(-gm[r].x, -gm[r].y) : v;
+            for (int r = 0; r < RPT; ++r) {
+                if (tid + NT * r == p) {
+#pragma unroll
+                    for (int jj = 0; jj < NB; ++jj) w[r][jj] = (jj == kk) ? d : zmul(srow[jj], d);
+                } else {
+#pragma unroll
+                    for (int jj = 0; jj < NB; ++jj)
+                        w[r][jj] = (jj == kk) ? make_double2(-gm[r].x, -gm[r].y) : zfms(gm[r], srow[jj], w[r][jj]);
                 }
             }
-            f[r] = fn[r];
+            if (mine >= 0) {
+                double2 *dst = s.cand + ((buf ^ 1) * NWARP + warp) * 32;
+#pragma unroll
+                for (int r = 0; r < RPT; ++r)
+                    if (r == mine) {
+#pragma unroll
+                        for (int jj = 0; jj < NB; ++jj) dst[jj] = w[r][jj];
+                    }
+            }
         }
     }
     __syncthreads();
@@ -666,44 +690,48 @@ __device__ int gj_invert(double2 *__restrict__ A, int N, int ld, const Smem &s) 
             for (int jj = 0; jj < NB; ++jj)
                 w[r][jj] = (i < N && jj < nba) ? A[i + (size_t)ld * (k0 + jj)] : make_double2(0.0, 0.0);
         }
-        factor_subpanel<NB, RPT>(w, k0, nba, used, info, 1, s);
-        if (nbb > 0) {
-            double2 *sWa = s.big;              // [NB][ldw] sub-panel a after step 1
-            double2 *sX = s.big + NB * ldw;    // [NB][NB]
-            const int kbb = k0 + nba;
+        double2 *sWa = s.big;              // [NB][ldw] sub-panel a after step 1
+        double2 *sX = s.big + NB * ldw;    // [NB][NB]
+        const int kbb = k0 + nba;
+        // one call site for both sub-panels keeps one copy of the unrolled steps
+        for (int half = 0; half < (nbb > 0 ? 2 : 1); ++half) {
+            if (half == 1) {
 #pragma unroll
-            for (int r = 0; r < RPT; ++r) {
-                const int i = tid + NT * r;
-                if (i < ldw) {
+                for (int r = 0; r < RPT; ++r) {
+                    const int i = tid + NT * r;
+                    if (i < ldw) {
 #pragma unroll
-                    for (int jj = 0; jj < NB; ++jj) sWa[jj * ldw + i] = (i < N) ? w[r][jj] : make_double2(0.0, 0.0);
+                        for (int jj = 0; jj < NB; ++jj) sWa[jj * ldw + i] = (i < N) ? w[r][jj] : make_double2(0.0, 0.0);
+                    }
                 }
-            }
-            // rows P_a of sub-panel b before a's steps
-            for (int e = tid; e < NB * NB; e += NT) {
-                const int kk = e / NB, c = e % NB;
-                sX[e] = (kk < nba && c < nbb) ? A[s.prow[k0 + kk] + (size_t)ld * (kbb + c)] : make_double2(0.0, 0.0);
-            }
-            __syncthreads();
-            // 2. b = mask_a(b) + W_a * b(P_a, :)
+                // rows P_a of sub-panel b before a's steps
+                for (int e = tid; e < NB * NB; e += NT) {
+                    const int kk = e / NB, c = e % NB;
+                    sX[e] = (kk < nba && c < nbb) ? A[s.prow[k0 + kk] + (size_t)ld * (kbb + c)] : make_double2(0.0, 0.0);
+                }
+                __syncthreads();
+                // 2. b = mask_a(b) + W_a * b(P_a, :)
 #pragma unroll
-            for (int r = 0; r < RPT; ++r) {
-                const int i = tid + NT * r;
-                const bool keep = (i < N) && s.inP[i] != 1;
+                for (int r = 0; r < RPT; ++r) {
+                    const int i = tid + NT * r;
+                    const bool keep = (i < N) && s.inP[i] != 1;
 #pragma unroll
-                for (int c = 0; c < NB; ++c)
-                    w[r][c] = (keep && c < nbb) ? A[i + (size_t)ld * (kbb + c)] : make_double2(0.0, 0.0);
-                if (i < N) {
+                    for (int c = 0; c < NB; ++c)
+                        w[r][c] = (keep && c < nbb) ? A[i + (size_t)ld * (kbb + c)] : make_double2(0.0, 0.0);
+                    if (i < N) {
 #pragma unroll 1
-                    for (int kk = 0; kk < nba; ++kk) {
-                        const double2 wa = sWa[kk * ldw + i];
+                        for (int kk = 0; kk < nba; ++kk) {
+                            const double2 wa = sWa[kk * ldw + i];
 #pragma unroll
-                        for (int c = 0; c < NB; ++c) w[r][c] = zfma(wa, sX[kk * NB + c], w[r][c]);
+                            for (int c = 0; c < NB; ++c) w[r][c] = zfma(wa, sX[kk * NB + c], w[r][c]);
+                        }
                     }
                 }
             }
-            // 3. eliminate b
-            factor_subpanel<NB, RPT>(w, kbb, nbb, used, info, 2, s);
+            // 1. / 3. eliminate the sub-panel
+            factor_subpanel<NB, RPT>(w, half ? kbb : k0, half ? nbb : nba, used, info, half + 1, s);
+        }
+        if (nbb > 0) {
             // rows P_b of sub-panel a after step 1
             for (int e = tid; e < NB * NB; e += NT) {
                 const int kk = e / NB, c = e % NB;
