@@ -55,6 +55,11 @@ typedef struct negf_problem {
     double eta;           /* atomic%ETA (Hartree)                                */
     int32_t nk;           /* size(kpoint)                                        */
     const double *kpt;    /* [nk][3] = kpoint(i)%kx, %ky, %weight                */
+    int32_t lead_model;   /* 0: the reference's lead term exp(i q dz) with the
+                           * continuum q (grid.f90:284-331) and gamma = sin(q dz)/dz^2
+                           * (grid.f90:355-365); 1: the exact surface Green's
+                           * function of the discretised flat lead (the fixed point
+                           * of Sancho-Rubio decimation, no reference counterpart)  */
 } negf_problem;
 
 typedef struct negf_stats {

@@ -35,7 +35,7 @@ class Problem(C.Structure):
     _fields_ = [("N", C.c_int32), ("Nz", C.c_int32), ("ngx", C.c_int32), ("ngy", C.c_int32),
                 ("nx", _ip), ("ny", _ip), ("vhat", _dp), ("Lx", C.c_double), ("Ly", C.c_double),
                 ("Lz", C.c_double), ("V_L", C.c_double), ("V_R", C.c_double), ("eta", C.c_double),
-                ("nk", C.c_int32), ("kpt", _dp)]
+                ("nk", C.c_int32), ("kpt", _dp), ("lead_model", C.c_int32)]
 
 
 class Stats(C.Structure):

@@ -418,6 +418,7 @@ struct negf_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int N = 0, Nz = 0, ld = 0, ngx = 0, ngy = 0, nk = 0;
     double Lx = 0, Ly = 0, Lz = 0, V_L = 0, V_R = 0, eta = 0;
+    int lead_model = 0;
     std::vector<double> kpt;  // nk x 3
     double2 *d_vhat = nullptr;
     int *d_nx = nullptr, *d_ny = nullptr;
@@ -451,6 +452,7 @@ Geo make_geo(const negf_ctx *c) {
     g.delta = c->Lz / c->Nz;
     g.c2 = 2 * (g.delta * g.delta);
     g.V_L = c->V_L; g.V_R = c->V_R; g.eta = c->eta;
+    g.lead_model = c->lead_model;
     return g;
 }
 
@@ -690,6 +692,7 @@ int check_problem(const negf_problem *p) {
             if (dx < -p->ngx || dx > p->ngx || dy < -p->ngy || dy > p->ngy) return NEGF_ERR_ARG;
         }
     if (pick_variant(p->N) == VNONE) return NEGF_ERR_UNSUPPORTED;
+    if (p->lead_model != 0 && p->lead_model != 1) return NEGF_ERR_ARG;
     return 0;
 }
 
@@ -712,6 +715,7 @@ int negf_ctx_create(const negf_problem *p, int32_t device, negf_ctx **out) {
     c->ngx = p->ngx; c->ngy = p->ngy; c->nk = p->nk;
     c->Lx = p->Lx; c->Ly = p->Ly; c->Lz = p->Lz;
     c->V_L = p->V_L; c->V_R = p->V_R; c->eta = p->eta;
+    c->lead_model = p->lead_model;
     c->kpt.assign(p->kpt, p->kpt + 3 * (size_t)p->nk);
     const size_t nv = (size_t)(2 * p->ngx + 1) * (2 * p->ngy + 1) * p->Nz;
     std::vector<double> ax((size_t)p->nk * p->N), ay((size_t)p->nk * p->N), kw(p->nk);
@@ -913,6 +917,7 @@ int negf_tri_solve(negf_ctx *ctx, const double *D, int32_t N, int32_t Nz, const 
     Geo g{};
     g.N = N; g.Nz = Nz; g.ld = round_up(N, 8);
     g.delta = 1.0; g.c2 = 1.0;
+    g.lead_model = 0;
     double2 *d_D = nullptr, *d_slab = nullptr, *d_first = nullptr, *d_last = nullptr;
     int *d_nx = nullptr, *d_ny = nullptr, *d_info = nullptr;
     int rc = 0, hinfo = 0;
@@ -1337,6 +1342,7 @@ extern "C" int negf_transmission_noalloc(int32_t N, int32_t Nz, int32_t ngx, int
     g.delta = Lz / Nz;
     g.c2 = 2 * (g.delta * g.delta);
     g.V_L = V_L; g.V_R = V_R; g.eta = eta;
+    g.lead_model = 0;
     switch (v) {
         case V16x1:
             k_transmission<16, 1, 2><<<grid, NT, smem, st>>>(g, d_energies, nE, (int)njobs, ws, wstride, tau_jobs, d_info);

@@ -360,7 +360,10 @@ int main(int argc, char **argv) {
         return 1;
     }
     negf_problem p{N, Nz, d.NGX, d.NGY, nxg.data(), nyg.data(), vhat.data(), aLX, aLY, aLZ, aV_L, aV_R, aETA,
-                   d.NKX * d.NKY, kpt.data()};
+                   d.NKX * d.NKY, kpt.data(), 0};
+    // engine option outside the reference's namelist: NEGF_LEAD_MODEL=1 selects the
+    // exact lattice surface Green's function of the leads
+    if (const char *lm = std::getenv("NEGF_LEAD_MODEL")) p.lead_model = std::atoi(lm);
     negf_ctx *ctx = nullptr;
     int rc = negf_ctx_create(&p, device, &ctx);
     if (rc) {

@@ -79,6 +79,26 @@ __device__ __forceinline__ double2 self_energy(double2 q, double delta) {
     return make_double2(m * c, m * s);
 }
 
+// Exact lead of the discretised model: the semi-infinite chain of diagonal
+// blocks d = 2 dz^2 (E - V - kin) - 2 with +1 couplings has the surface
+// Green's function g = 1/(d - g) (the fixed point of Sancho-Rubio
+// decimation), the root of g^2 - d g + 1 = 0 with |g| < 1; block 1 then
+// gets d_1 - g.  Returns -g, the term added to the end blocks.
+__device__ __forceinline__ double2 lattice_self_energy(double2 E, double V, double kin, double c2) {
+    const double2 d = make_double2(c2 * (E.x - V - kin) - 2.0, c2 * E.y);
+    const double2 disc = zsqrt(make_double2(d.x * d.x - d.y * d.y - 4.0, 2.0 * d.x * d.y));
+    const double2 g1 = make_double2(0.5 * (d.x + disc.x), 0.5 * (d.y + disc.y));
+    const double2 g2 = make_double2(0.5 * (d.x - disc.x), 0.5 * (d.y - disc.y));
+    const double2 gs = (g1.x * g1.x + g1.y * g1.y <= g2.x * g2.x + g2.y * g2.y) ? g1 : g2;
+    return make_double2(-gs.x, -gs.y);
+}
+// Im of that term at the real energy over dz^2: sin(theta)/dz^2 for an open
+// lattice channel (d = -2 cos(theta), |d| < 2), 0 for a closed one.
+__device__ __forceinline__ double lattice_gamma(double e, double V, double kin, double c2, double dz) {
+    const double d = c2 * (e - V - kin) - 2.0;
+    return fabs(d) < 2.0 ? sqrt(1.0 - 0.25 * d * d) / (dz * dz) : 0.0;
+}
+
 // ------------------------------------------------------------ cp.async
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool valid) {
     unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -102,6 +122,7 @@ struct Geo {
     double delta;           // Lz / Nz
     double c2;              // 2*delta**2 (grid.f90:311)
     double V_L, V_R, eta;
+    int lead_model;         // 0 reference continuum lead term, 1 exact lattice surface GF
 };
 
 // One warp's pivot candidate: a sortable key and the reciprocal of its value.
@@ -190,14 +211,22 @@ __device__ inline Smem carve(unsigned char *base, int N) {
 __device__ inline void job_vectors(const Geo &g, const Smem &s, double2 E, double e_t, int ik) {
     for (int i = threadIdx.x; i < g.N; i += NT) {
         const double ax = g.ax[ik * g.N + i], ay = g.ay[ik * g.N + i];
-        double2 zl = make_double2(2.0 * (E.x - g.V_L) - ax * ax - ay * ay, 2.0 * E.y);
-        double2 zr = make_double2(2.0 * (E.x - g.V_R) - ax * ax - ay * ay, 2.0 * E.y);
-        s.sigL[i] = self_energy(zsqrt(zl), g.delta);
-        s.sigR[i] = self_energy(zsqrt(zr), g.delta);
-        double ql = sqrt(fmax(2.0 * (e_t - g.V_L) - ax * ax - ay * ay, 0.0));
-        double qr = sqrt(fmax(2.0 * (e_t - g.V_R) - ax * ax - ay * ay, 0.0));
-        s.gL[i] = sin(ql * g.delta) / (g.delta * g.delta);
-        s.gR[i] = sin(qr * g.delta) / (g.delta * g.delta);
+        if (g.lead_model == 0) {
+            double2 zl = make_double2(2.0 * (E.x - g.V_L) - ax * ax - ay * ay, 2.0 * E.y);
+            double2 zr = make_double2(2.0 * (E.x - g.V_R) - ax * ax - ay * ay, 2.0 * E.y);
+            s.sigL[i] = self_energy(zsqrt(zl), g.delta);
+            s.sigR[i] = self_energy(zsqrt(zr), g.delta);
+            double ql = sqrt(fmax(2.0 * (e_t - g.V_L) - ax * ax - ay * ay, 0.0));
+            double qr = sqrt(fmax(2.0 * (e_t - g.V_R) - ax * ax - ay * ay, 0.0));
+            s.gL[i] = sin(ql * g.delta) / (g.delta * g.delta);
+            s.gR[i] = sin(qr * g.delta) / (g.delta * g.delta);
+        } else {
+            const double kin = (ax * ax + ay * ay) / 2;
+            s.sigL[i] = lattice_self_energy(E, g.V_L, kin, g.c2);
+            s.sigR[i] = lattice_self_energy(E, g.V_R, kin, g.c2);
+            s.gL[i] = lattice_gamma(e_t, g.V_L, kin, g.c2, g.delta);
+            s.gR[i] = lattice_gamma(e_t, g.V_R, kin, g.c2, g.delta);
+        }
     }
 }
 

@@ -31,7 +31,7 @@ class Engine:
     """
 
     def __init__(self, nx_grid, ny_grid, V_reciprocal_all, Lx, Ly, Lz, V_L, V_R, ETA, kpoint,
-                 device=0):
+                 device=0, lead_model=0):
         self.nx = np.ascontiguousarray(nx_grid, np.int32)
         self.ny = np.ascontiguousarray(ny_grid, np.int32)
         self.vhat = np.asfortranarray(V_reciprocal_all, np.complex128)
@@ -51,6 +51,7 @@ class Engine:
         p.V_L, p.V_R, p.eta = self.V_L, self.V_R, self.eta
         p.nk = len(self.kpt)
         p.kpt = self.kpt.ctypes.data_as(_dp)
+        p.lead_model = int(lead_model)   # 0 reference lead term, 1 exact lattice surface GF
         self._ctx = C.c_void_p()
         check("negf_ctx_create", lib().negf_ctx_create(C.byref(p), device, C.byref(self._ctx)))
         self.device = device

@@ -329,12 +329,15 @@ def _kin(n, L, k):
     return (2.0 * n) * PI / L + k
 
 
-def closed_form_modes(nx, ny, vz, Lx, Ly, Lz, V_L, V_R, eta, energy, kx, ky):
+def closed_form_modes(nx, ny, vz, Lx, Ly, Lz, V_L, V_R, eta, energy, kx, ky, lattice=False):
     """Scalar three-term recursion per plane-wave mode for a z-only potential.
 
     vz[k] is V_reciprocal(0,0,k) (the xy-average of slice k, Hartree).  Returns
     (G_first[N] = G_{Nz,1}, G_diag[N, Nz] = G_{kk}) rescaled by 2*Delta^2 as in
     negf.f90:159-165, computed in long double, plus sL, sR of grid.f90:355-365.
+    lattice=True replaces the lead term e^{iq dz} by -g, g the |g|<1 root of
+    g^2 - d g + 1 = 0 for the lead block d (the exact semi-infinite discretised
+    lead), and gamma by sqrt(1 - d^2/4)/dz^2 for |d| < 2 at the real energy.
     """
     ld = np.longdouble
     Nz = len(vz)
@@ -357,8 +360,15 @@ def closed_form_modes(nx, ny, vz, Lx, Ly, Lz, V_L, V_R, eta, energy, kx, ky):
         for k in range(Nz):
             d[k] = c2 * (np.clongdouble(e) + 1j * ld(eta) - ld(vz[k].real) - 1j * ld(vz[k].imag)
                          - eps) - 2
-        d[0] += np.exp(1j * qL * delta)
-        d[-1] += np.exp(1j * qR * delta)
+        if lattice:
+            for idx, V in ((0, V_L), (Nz - 1, V_R)):
+                dl = c2 * (np.clongdouble(e) + 1j * ld(eta) - ld(V) - eps) - 2
+                disc = np.sqrt(np.clongdouble(dl * dl - 4))
+                g1, g2 = (dl + disc) / 2, (dl - disc) / 2
+                d[idx] -= g1 if abs(g1) <= abs(g2) else g2
+        else:
+            d[0] += np.exp(1j * qL * delta)
+            d[-1] += np.exp(1j * qR * delta)
         # theta_k = det of leading k x k, phi_k = det of trailing block from k
         th = np.empty(Nz + 1, np.clongdouble)
         th[0] = 1
@@ -374,16 +384,21 @@ def closed_form_modes(nx, ny, vz, Lx, Ly, Lz, V_L, V_R, eta, energy, kx, ky):
         G_first[i] = complex(((-1) ** (Nz - 1)) / det * c2)
         for k in range(1, Nz + 1):
             G_diag[i, k - 1] = complex(th[k - 1] * ph[k + 1] / det * c2)
-        qr = np.sqrt(max(2 * (ld(e.real) - ld(V_L)) - 2 * eps, ld(0)))
-        qt = np.sqrt(max(2 * (ld(e.real) - ld(V_R)) - 2 * eps, ld(0)))
-        sL[i] = float(np.sin(qr * delta) / (delta * delta))
-        sR[i] = float(np.sin(qt * delta) / (delta * delta))
+        if lattice:
+            for arr, V in ((sL, V_L), (sR, V_R)):
+                dr = c2 * (ld(e.real) - ld(V) - eps) - 2
+                arr[i] = float(np.sqrt(1 - dr * dr / 4) / (delta * delta)) if abs(dr) < 2 else 0.0
+        else:
+            qr = np.sqrt(max(2 * (ld(e.real) - ld(V_L)) - 2 * eps, ld(0)))
+            qt = np.sqrt(max(2 * (ld(e.real) - ld(V_R)) - 2 * eps, ld(0)))
+            sL[i] = float(np.sin(qr * delta) / (delta * delta))
+            sR[i] = float(np.sin(qt * delta) / (delta * delta))
     return G_first, G_diag, sL, sR
 
 
-def closed_form_tau(nx, ny, vz, Lx, Ly, Lz, V_L, V_R, eta, energy, kx, ky):
+def closed_form_tau(nx, ny, vz, Lx, Ly, Lz, V_L, V_R, eta, energy, kx, ky, lattice=False):
     """tau of grid.f90:335-385 for a z-only potential (G diagonal in modes)."""
-    Gf, _, sL, sR = closed_form_modes(nx, ny, vz, Lx, Ly, Lz, V_L, V_R, eta, energy, kx, ky)
+    Gf, _, sL, sR = closed_form_modes(nx, ny, vz, Lx, Ly, Lz, V_L, V_R, eta, energy, kx, ky, lattice)
     return float(np.sum(sL * sR * np.abs(Gf) ** 2))
 
 

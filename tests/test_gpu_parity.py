@@ -253,3 +253,30 @@ def test_transmission_batch_uneven(oracle):
         ref, _ = oracle.transmission_jobs(oracle.Problem(nx, ny, vhat, lx, ly, lz, vl, vr, eta, kp), E,
                                           nthreads=8)
         np.testing.assert_allclose(t, ref, rtol=RTOL, atol=1e-12)
+
+
+@pytest.mark.parametrize("flat", [True, False])
+def test_lattice_lead_model(oracle, flat):
+    """lead_model = 1 (exact lattice surface Green's function of the leads)
+    against the closed form; a flat device transmits open channels fully."""
+    nz, grid = 20, 32
+    z = np.arange(nz) + 0.5 - nz / 2
+    vz = np.zeros(nz) if flat else 0.067 * 0.02 * np.exp(-z ** 2 / 18.0)
+    V = np.asfortranarray(np.broadcast_to(vz[None, None, :], (grid, grid, nz)))
+    d = W._deck(nz * 10.0, 1.2e-3, 30.0, 16)
+    d.ETA = 1e-13      # eta absorbs slow near-edge modes; keep it small for the unitarity check
+    pr = P.prepare(d, V)
+    a = pr.atomic
+    E = P.transmission_energies(a, 16)
+    with Engine(*pr.engine_args(), lead_model=1) as eng:
+        tau, info = eng.transmission(E)
+    assert info == 0
+    vz00 = pr.vhat[pr.NGX, pr.NGY, :]
+    cf = [oracle.closed_form_tau(pr.nx, pr.ny, vz00, a.LX, a.LY, a.LZ, a.V_L, a.V_R, a.ETA, e, 0, 0,
+                                 lattice=True) for e in E]
+    np.testing.assert_allclose(tau, cf, rtol=1e-9, atol=1e-12)
+    if flat:
+        dz = a.LZ / nz
+        eps = ((2.0 * pr.nx * np.pi / a.LX) ** 2 + (2.0 * pr.ny * np.pi / a.LY) ** 2) / 2
+        n_open = [np.sum(np.abs(2 * dz * dz * (e - eps) - 2) < 2) for e in E]
+        np.testing.assert_allclose(tau, n_open, atol=1e-4)

@@ -195,3 +195,23 @@ def test_golden_fixtures(oracle):
     dm, _ = oracle.density_jobs(p, int(g["n_circle"]), int(g["n_line"]), float(g["min_v"]),
                                 float(g["mu"]), float(g["gap"]), float(g["temperature"]))
     assert rel(dm, g["dm"]) < 1e-12
+
+
+def test_lattice_leads_closed_form_is_unitary(oracle):
+    """With the exact lattice lead term a flat device transmits every open
+    lattice channel fully: tau = number of modes with |d| < 2 (pins the closed
+    form used to check the engine's lead_model = 1)."""
+    lx = ly = 400 / A_0
+    nz = 12
+    lz = nz * 10 / A_0
+    nx, ny = oracle.basis(0.05 / HARTREE, lx, ly)
+    vz = np.zeros(nz)
+    dz = lz / nz
+    for e in (0.004 / HARTREE, 0.03 / HARTREE):
+        t = oracle.closed_form_tau(nx, ny, vz, lx, ly, lz, 0.0, 0.0, 1e-12, e, 0.0, 0.0, lattice=True)
+        eps = ((2.0 * nx * PI / lx) ** 2 + (2.0 * ny * PI / ly) ** 2) / 2
+        d = 2 * dz * dz * (e - eps) - 2
+        assert abs(t - np.sum(np.abs(d) < 2)) < 1e-4   # eta absorbs a little near band edges
+        # the reference's continuum lead term reflects a little at the ends
+        t_ref = oracle.closed_form_tau(nx, ny, vz, lx, ly, lz, 0.0, 0.0, 1e-12, e, 0.0, 0.0)
+        assert t_ref <= t + 1e-9
