@@ -36,7 +36,22 @@ struct Deck {
     double TRANSMISSION_GRID[3] = {0, 0, 0}, LDOS_ENERGY_GRID[3] = {0, 0, 0};
     int LDOS_GRID[3] = {-10, -10, -10};
     int NGX = 0, NGY = 0, NKX = 0, NKY = 0, N_circle = 40, N_line_per_eV = 500;
+    // Engine key with no reference counterpart: effective mass m*/m_e (the
+    // reference's kinetic term is |k+G|^2/2, i.e. m* = 1).
+    double EMASS = 1;
 };
+
+// Folds EMASS = m* into the energy scale: E' = m* E, V' = m* V, eta' = m* eta,
+// T' = m* T, ENCUT' = m* ENCUT (and N_line_per_eV' = N_line_per_eV / m*), the
+// m* = 1 problem with the same tau and density; G' = G / m*.
+void fold_emass(Deck &d) {
+    const double m = d.EMASS;
+    if (m == 1) return;
+    d.V_L *= m; d.V_R *= m; d.MU *= m; d.ETA *= m; d.TEMPERATURE *= m; d.ENCUT *= m; d.VDS *= m;
+    d.TRANSMISSION_GRID[0] *= m; d.TRANSMISSION_GRID[1] *= m;
+    d.LDOS_ENERGY_GRID[0] *= m; d.LDOS_ENERGY_GRID[1] *= m;
+    d.N_line_per_eV = (int)std::floor(d.N_line_per_eV / m + 0.5);
+}
 
 std::string lower(std::string s) {
     for (auto &c : s) c = (char)std::tolower((unsigned char)c);
@@ -173,6 +188,7 @@ bool read_namelist(const std::string &path, Deck &d, std::string &err) {
         else if (k == "nky") ok = int1(&d.NKY);
         else if (k == "n_circle") ok = int1(&d.N_circle);
         else if (k == "n_line_per_ev") ok = int1(&d.N_line_per_eV);
+        else if (k == "emass") ok = real1(&d.EMASS);
         else { err = "unknown namelist item " + k; return false; }
         if (!ok) return false;
     }
@@ -278,6 +294,14 @@ int main(int argc, char **argv) {
         std::fprintf(stderr, "INPUT: %s\n", err.c_str());
         return 1;
     }
+    const double emass = d.EMASS;
+    if (!(emass > 0)) {
+        std::fprintf(out, " ERROR: EMASS must be positive\n");
+        banner(out, "EXIT");
+        std::fclose(out);
+        return 1;
+    }
+    fold_emass(d);
     // NGX, NGY (main.f90:94-100; the NGX test reads LY as the reference does)
     const double s = std::sqrt(d.ENCUT / HARTREE / 2);
     if (d.NGX <= (int)std::ceil((d.LY / A_0) / PI * s * 2)) d.NGX = (int)std::ceil((d.LX / A_0) / PI * s * 2) + 1;
@@ -326,7 +350,7 @@ int main(int argc, char **argv) {
     const double aGAP = d.GAP * K_B * d.TEMPERATURE;
     double min_v = 1e300;
     for (auto &x : V) {
-        x /= HARTREE;
+        x = x * emass / HARTREE;
         min_v = std::min(min_v, x);
     }
     std::vector<double> kpt(3 * (size_t)d.NKX * d.NKY);
@@ -343,11 +367,12 @@ int main(int argc, char **argv) {
                     "\"if_density\": %d, \"if_transmission\": %d, \"if_LDOS\": %d, \"ETA\": %.17g, \"ENCUT\": %.17g, "
                     "\"LX\": %.17g, \"LY\": %.17g, \"LZ\": %.17g, \"TRANSMISSION_GRID\": [%.17g, %.17g, %.17g], "
                     "\"LDOS_GRID\": [%d, %d, %d], \"N_circle\": %d, \"N_line_per_eV\": %d, \"min_V\": %.17g, "
-                    "\"V_sum\": %.17g}\n",
+                    "\"V_sum\": %.17g, \"MU\": %.17g, \"TEMPERATURE\": %.17g, \"EMASS\": %.17g}\n",
                     N, Nz, Nx, Ny, d.NGX, d.NGY, d.NKX * d.NKY, d.if_density, d.if_transmission, d.if_LDOS, d.ETA,
                     d.ENCUT, d.LX, d.LY, d.LZ, d.TRANSMISSION_GRID[0], d.TRANSMISSION_GRID[1],
                     d.TRANSMISSION_GRID[2], d.LDOS_GRID[0], d.LDOS_GRID[1], d.LDOS_GRID[2], d.N_circle,
-                    d.N_line_per_eV, min_v, [&] { double t = 0; for (double x : V) t += x; return t; }());
+                    d.N_line_per_eV, min_v, [&] { double t = 0; for (double x : V) t += x; return t; }(), d.MU,
+                    d.TEMPERATURE, emass);
         std::fclose(out);
         return 0;
     }
@@ -403,7 +428,7 @@ int main(int argc, char **argv) {
         std::fprintf(out, " Transmission calculation DONE\n ----------\n");
         FILE *f = std::fopen("TRANSMISSION", "w");
         std::fprintf(f, " #   Energy (eV)    Transmission_coefficient\n");
-        for (int i = 0; i < nE; ++i) std::fprintf(f, "%s%s\n", gfmt(E[i] * HARTREE).c_str(), gfmt(tau[i]).c_str());
+        for (int i = 0; i < nE; ++i) std::fprintf(f, "%s%s\n", gfmt(E[i] * HARTREE / emass).c_str(), gfmt(tau[i]).c_str());
         std::fclose(f);
     }
     if (d.if_LDOS) {
@@ -417,7 +442,7 @@ int main(int argc, char **argv) {
         std::fprintf(out, " LDOS calculation start...\n Number of energy grid points: %d\n", nE);
         const auto a = std::chrono::steady_clock::now();
         rc = negf_ldos(ctx, d.LDOS_ENERGY_GRID[0] / HARTREE, d.LDOS_ENERGY_GRID[1] / HARTREE, nE, d.LDOS_GRID, Nx, Ny,
-                       dxyz, (double)Nz / (d.LX * d.LY * d.LZ) / HARTREE, ldos.data(), &st);
+                       dxyz, (double)Nz / (d.LX * d.LY * d.LZ) / HARTREE * emass, ldos.data(), &st);
         t_ldos = std::chrono::duration<double>(std::chrono::steady_clock::now() - a).count();
         if (rc < 0) { std::fprintf(out, " ERROR: LDOS failed (%d)\n", rc); negf_ctx_destroy(ctx); std::fclose(out); return 1; }
         std::fprintf(out, " LDOS calculation DONE\n ----------\n");

@@ -39,6 +39,12 @@ class InputDeck:
     NKY: int = 0
     N_circle: int = 40
     N_line_per_eV: int = 500
+    # Engine key with no reference counterpart: effective mass m*/m_e.  The
+    # reference's kinetic term is |k+G|^2/2 (m* = 1, grid.f90:258); EMASS = m*
+    # is applied as the exact scaling E' = m* E, V' = m* V, eta' = m* eta,
+    # T' = m* T, ENCUT' = m* ENCUT, under which tau and the density are
+    # unchanged and the LDOS per eV scales by 1/m*.
+    EMASS: float = 1.0
 
 
 def validate(d: InputDeck):
@@ -116,7 +122,24 @@ class Prepared:
         return (self.nx, self.ny, self.vhat, a.LX, a.LY, a.LZ, a.V_L, a.V_R, a.ETA, self.kpoint)
 
 
+def scaled_deck(d: InputDeck) -> InputDeck:
+    """The m* = 1 deck equivalent to d (EMASS folded into the energy scale)."""
+    import dataclasses
+    m = d.EMASS
+    if m == 1.0:
+        return d
+    if not m > 0:
+        raise ValueError("EMASS must be positive")
+    return dataclasses.replace(
+        d, V_L=m * d.V_L, V_R=m * d.V_R, MU=m * d.MU, ETA=m * d.ETA, TEMPERATURE=m * d.TEMPERATURE,
+        ENCUT=m * d.ENCUT, VDS=m * d.VDS,
+        TRANSMISSION_GRID=(m * d.TRANSMISSION_GRID[0], m * d.TRANSMISSION_GRID[1], d.TRANSMISSION_GRID[2]),
+        LDOS_ENERGY_GRID=(m * d.LDOS_ENERGY_GRID[0], m * d.LDOS_ENERGY_GRID[1], d.LDOS_ENERGY_GRID[2]),
+        N_line_per_eV=int(math.floor(d.N_line_per_eV / m + 0.5)), EMASS=1.0)
+
+
 def to_atomic(d: InputDeck) -> Atomic:
+    d = scaled_deck(d)
     return Atomic(
         V_L=d.V_L / HARTREE, V_R=d.V_R / HARTREE, MU=d.MU / HARTREE, ETA=d.ETA,
         TEMPERATURE=d.TEMPERATURE, LX=d.LX / A_0, LY=d.LY / A_0, LZ=d.LZ / A_0,
@@ -127,17 +150,22 @@ def to_atomic(d: InputDeck) -> Atomic:
 
 def prepare(d: InputDeck, V_real_eV) -> Prepared:
     """main.f90:94-249 for a deck and a POTENTIAL array (N_x, N_y, N_z) in eV."""
-    v = np.asfortranarray(V_real_eV, dtype=np.float64)
+    v = np.asfortranarray(V_real_eV, dtype=np.float64) * scaled_deck_factor(d)
     Nx, Ny, Nz = v.shape
     if Nx % 2 or Ny % 2:
         raise ValueError("The number of grid point in x & y direction must be even number")
     a = to_atomic(d)
-    ngx, ngy = ngrid(d)
+    ngx, ngy = ngrid(scaled_deck(d))
     vh = v / HARTREE
     kp = Kpoint_mesh_construction(d.NKX, d.NKY, a.LX, a.LY)
     nx, ny = PlaneWaveBasis_construction(a.ENCUT, a.LX, a.LY)
     vhat = V_reciprocal_all(vh, ngx, ngy)
     return Prepared(a, nx, ny, kp, vhat, ngx, ngy, float(vh.min()), (Nx, Ny, Nz))
+
+
+def scaled_deck_factor(d: InputDeck) -> float:
+    """Factor applied to POTENTIAL values by EMASS (1 for the reference)."""
+    return float(d.EMASS)
 
 
 def transmission_energies(atomic: Atomic, n_e: int):

@@ -174,3 +174,73 @@ def test_end_to_end_against_oracle(driver, tmp_path, oracle):
             oracle.local_density_of_state(p, ik + 1, ie + 1, 3, e_lo, e_hi, mat)
         ref = oracle.ldos_from_matrix(mat, pr.nx, pr.ny, 32, 32, deck.LX, deck.LY, deck.LZ, (-1, -1, 0))
         assert np.max(np.abs(ldos[..., ie] - ref)) <= 1e-7 * np.max(np.abs(ref))
+
+
+EMASS_DECK = """&INPUT
+ if_transmission=.true. if_density=.true. if_LDOS=.true.
+ LX=1000.0 LY=1000.0 LZ=60.0 ENCUT={encut!r} ETA={eta!r} EMASS={m!r}
+ NKX=1 NKY=2 TEMPERATURE={t!r} MU={mu!r} N_circle=5 N_line_per_eV={nl}
+ TRANSMISSION_GRID = {e1!r} {e2!r} 8
+ LDOS_ENERGY_GRID = {l1!r} {l2!r} 3
+ LDOS_GRID = -1 -1 0
+/
+
+"""
+M_EFF = 0.067
+PHYS = dict(encut=1.2e-3 / M_EFF, eta=1e-6 / HARTREE, t=1.0 / M_EFF, mu=1.0e-3 / M_EFF, nl=268,
+            e1=0.0, e2=2.01e-3 / M_EFF, l1=0.0, l2=2.0e-3 / M_EFF)
+
+
+def _emass_pair(tmp_path):
+    """The same device written with EMASS = m* (physical units) and as the
+    m*-scaled deck with m* = 1 (the reference's convention)."""
+    m = M_EFF
+    V = W.qpc_potential(32, 32, 6, 100.0, 6.0, 0.05, 15.0, 1.0, disorder=0.002)
+    scaled = {k: (v * m if k in ("encut", "eta", "t", "mu", "e1", "e2", "l1", "l2") else v) for k, v in PHYS.items()}
+    scaled["nl"] = int(math.floor(PHYS["nl"] / m + 0.5))
+    a, b = tmp_path / "phys", tmp_path / "scaled"
+    a.mkdir()
+    b.mkdir()
+    (a / "INPUT").write_text(EMASS_DECK.format(m=m, **PHYS))
+    (b / "INPUT").write_text(EMASS_DECK.format(m=1.0, **scaled))
+    _potential(a / "POTENTIAL", V)
+    _potential(b / "POTENTIAL", m * np.array((a / "POTENTIAL").read_text().split()[3:], float).reshape(V.shape, order="F"))
+    return a, b
+
+
+def test_emass_key_equals_scaled_deck(driver, tmp_path):
+    """EMASS = m* in the driver is the m*-scaled deck: same basis, grids, V table input."""
+    a, b = _emass_pair(tmp_path)
+    da = json.loads(_run(driver, a, "--check").stdout)
+    db = json.loads(_run(driver, b, "--check").stdout)
+    assert da["EMASS"] == M_EFF and db["EMASS"] == 1.0
+    for k in ("N", "Nz", "NGX", "NGY", "nk", "N_line_per_eV"):
+        assert da[k] == db[k], k
+    for k in ("ETA", "ENCUT", "MU", "TEMPERATURE", "min_V", "V_sum"):
+        assert math.isclose(da[k], db[k], rel_tol=1e-7), (k, da[k], db[k])
+    for x, y in zip(da["TRANSMISSION_GRID"], db["TRANSMISSION_GRID"]):
+        assert math.isclose(x, y, rel_tol=1e-12, abs_tol=1e-300)
+    (a / "INPUT").write_text(EMASS_DECK.format(m=-1.0, **PHYS))
+    r = _run(driver, a, "--check", check=False)
+    assert r.returncode == 1 and "EMASS must be positive" in (a / "OUTPUT").read_text()
+
+
+@pytest.mark.gpu
+def test_emass_end_to_end(driver, tmp_path):
+    """Driver outputs with EMASS = m*: tau and density equal those of the
+    scaled deck, energies are physical (scaled / m*), LDOS is per physical eV
+    (scaled x m*)."""
+    a, b = _emass_pair(tmp_path)
+    for d in (a, b):
+        r = _run(driver, d, check=False)
+        assert r.returncode == 0, (d / "OUTPUT").read_text()
+    ta = np.loadtxt(a / "TRANSMISSION", skiprows=1)
+    tb = np.loadtxt(b / "TRANSMISSION", skiprows=1)
+    np.testing.assert_allclose(ta[:, 0] * M_EFF, tb[:, 0], rtol=1e-7, atol=1e-15)
+    np.testing.assert_allclose(ta[:, 1], tb[:, 1], rtol=1e-6, atol=1e-9)
+    da = np.array((a / "DENSITY").read_text().split("\n", 1)[1].split(), float)
+    db = np.array((b / "DENSITY").read_text().split("\n", 1)[1].split(), float)
+    assert np.max(np.abs(da - db)) <= 1e-6 * np.max(np.abs(db))
+    la = np.array((a / "LDOS").read_text().split("\n", 1)[1].split(), float)
+    lb = np.array((b / "LDOS").read_text().split("\n", 1)[1].split(), float)
+    assert np.max(np.abs(la - M_EFF * lb)) <= 1e-6 * np.max(np.abs(M_EFF * lb))

@@ -124,3 +124,25 @@ def test_disorder_statistics():
     assert abs(np.sqrt(np.mean(V ** 2)) - 0.002) < 1e-12
     V2 = W.qpc_potential(32, 32, 64, 100.0, 64.0, 0.0, 15.0, 20.0, disorder=0.002, seed=7)
     assert np.array_equal(V, V2)
+
+
+def test_emass_key_is_the_input_scaling():
+    """EMASS = m* equals the m*-scaled deck with m* = 1 (same table, basis, energies)."""
+    import dataclasses
+    V = W.qpc_potential(32, 32, 8, 100.0, 8.0, 0.05, 15.0, 1.0, disorder=0.002)
+    phys = P.InputDeck(if_transmission=True, LX=1000.0, LY=1000.0, LZ=80.0, ENCUT=1.2e-3 / 0.067,
+                       ETA=1e-6 / HARTREE, NKX=1, NKY=2, TEMPERATURE=1.0, MU=0.02,
+                       TRANSMISSION_GRID=(0.0, 0.03, 16), EMASS=0.067)
+    scaled = dataclasses.replace(phys, ENCUT=1.2e-3, ETA=0.067e-6 / HARTREE, TEMPERATURE=0.067,
+                                 MU=0.067 * 0.02, TRANSMISSION_GRID=(0.0, 0.067 * 0.03, 16), EMASS=1.0)
+    a = P.prepare(phys, V)
+    b = P.prepare(scaled, 0.067 * V)
+    assert np.array_equal(a.nx, b.nx) and np.array_equal(a.ny, b.ny)
+    assert np.max(np.abs(a.vhat - b.vhat)) <= 1e-15 * np.max(np.abs(b.vhat))
+    np.testing.assert_allclose(P.transmission_energies(a.atomic, 16),
+                               P.transmission_energies(b.atomic, 16), rtol=1e-15)
+    assert math.isclose(a.atomic.ETA, b.atomic.ETA, rel_tol=1e-15)
+    assert math.isclose(a.atomic.MU, b.atomic.MU, rel_tol=1e-15)
+    assert math.isclose(a.atomic.GAP, b.atomic.GAP, rel_tol=1e-15)
+    with pytest.raises(ValueError):
+        P.to_atomic(dataclasses.replace(phys, EMASS=-1.0))
