@@ -364,6 +364,19 @@ def run_ours(args):
             line["density"] = {"jobs": njd, "seconds": el, "jobs_per_s": njd / el,
                                "device_ms": eng.last_stats.device_ms,
                                "flops_per_job": 24.0 * pr.N ** 3 * pr.Nz, "info": info_d}
+        # the biased density of the same configuration: 48-point Gauss-Legendre
+        # semicircle + 256-point real-axis window, 1 mV bias (left lead injecting)
+        from negftrans_b200 import HARTREE
+        vb = W.MSTAR * 1e-3 / HARTREE
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        _, info_n = eng.density_neq(nc, 256, pr.min_V, a.MU + vb, a.MU, a.GAP, a.TEMPERATURE)
+        el = time.perf_counter() - t0
+        if rank == 0:
+            njn = (nc + 256) * nk
+            line["density_neq"] = {"jobs": njn, "circle": nc, "window": 256, "bias_V": 1e-3,
+                                   "seconds": el, "jobs_per_s": njn / el,
+                                   "device_ms": eng.last_stats.device_ms, "info": info_n}
     if rank == 0:
         print(json.dumps(line), flush=True)
     eng.close()

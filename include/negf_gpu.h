@@ -169,6 +169,33 @@ int negf_transmission_noalloc(int32_t N, int32_t Nz, int32_t ngx, int32_t ngy, c
 int negf_density(negf_ctx *ctx, int32_t n_circle, int32_t n_line, double min_v, double mu,
                  double gap, double temperature, double *dm, negf_stats *stats);
 
+/* Non-equilibrium Density_Matrix under a bias mu_L != mu_R.  No reference
+ * counterpart: main.f90:129-132 rejects VDS != 0 and negf.f90:9-113 is
+ * equilibrium only.  With mu_lo = min(mu_L, mu_R), mu_hi = max, the lead at
+ * mu_hi injecting (s = its end slice, Gamma_s = diag(gamma) of its open
+ * channels, the transmission weights of grid.f90:362-365):
+ *   dm = (w 2/pi) [ sum over n_circle Gauss-Legendre nodes of theta in (0, pi)
+ *                   of c_theta i E_R e^{i theta} G(E_c + E_R e^{i theta})
+ *                   (the semicircle of negf.f90:37-65 from min_v - 1 eV to
+ *                   mu_lo - gap)
+ *                 - sum over n_window Gauss-Legendre nodes x of
+ *                   [mu_lo - gap, mu_hi + gap] of c_x f(x - mu_lo) G(x) ]
+ *      + i (w/pi) sum_x c_x (f(x - mu_hi) - f(x - mu_lo)) G_ks Gamma_s G_ks^H,
+ * every G at energy + i*eta and scaled by 2 dz^2 as in negf.f90:78, the
+ * spectral term by (2 dz^2)^2, summed over k-points with weights w.  So
+ * Im(PtoR(dm)) * scale is the electron density, as for negf_density; with
+ * mu_L == mu_R the spectral term vanishes and dm is the equilibrium
+ * Density_Matrix on Gauss-Legendre nodes.  Each window energy is one sweep
+ * that forms both terms.  gap, min_v, mu_L, mu_R in Hartree, temperature in
+ * K; dm (N,N,Nz) complex is overwritten. */
+int negf_density_neq(negf_ctx *ctx, int32_t n_circle, int32_t n_window, double min_v, double mu_L,
+                     double mu_R, double gap, double temperature, double *dm, negf_stats *stats);
+
+/* Greensfunction_PlanewaveToReal of any Density_Matrix on the GPU
+ * (main.f90:306-351): density (Nx,Ny,Nz) = Im(diag of PtoR(dm slice)) * scale. */
+int negf_dm_real(negf_ctx *ctx, const double *dm, int32_t Nx, int32_t Ny, double scale,
+                 double *density);
+
 /* Local_Density_Of_State, negf.f90:176-236, summed over k-points for the
  * energies i_e0 .. i_e0+n_chunk-1 (0-based) of the grid
  * E_i = e_lo + (e_hi-e_lo)*i/n_e.  ldos receives n_chunk consecutive

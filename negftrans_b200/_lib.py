@@ -25,6 +25,7 @@ EXPORTS = (
     "negf_ctx_destroy", "negf_tri_solve", "negf_transmission", "negf_transmission_device",
     "negf_density", "negf_ldos_matrix", "negf_ptor", "negf_version", "negf_transmission_noalloc",
     "negf_density_real", "negf_ldos", "negf_basis_k", "negf_transmission_batch",
+    "negf_density_neq", "negf_dm_real",
 )
 
 _dp = C.POINTER(C.c_double)
@@ -90,6 +91,9 @@ def lib():
     L.negf_transmission_batch.argtypes = [C.POINTER(C.c_void_p), C.c_int32, _dp, C.c_int32, _dp,
                                           C.POINTER(Stats)]
     L.negf_ptor.argtypes = [_dp, _ip, _ip, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _dp]
+    L.negf_density_neq.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
+                                   C.c_double, C.c_double, _dp, C.POINTER(Stats)]
+    L.negf_dm_real.argtypes = [C.c_void_p, _dp, C.c_int32, C.c_int32, C.c_double, _dp]
     _lib = L
     return L
 

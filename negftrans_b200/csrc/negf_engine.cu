@@ -34,6 +34,9 @@ struct RgfJob {
     double e_t;         // real energy of the transmission weights
     int ik;             // k-point
     int pad;
+    // WANT_A only: slice k of the output is cd * G_kk + ca * G_k,s Gamma_s G_k,s^H
+    // (s = the injecting lead's end slice, Gamma_s its open-channel widths)
+    double cd_re, cd_im, ca_re, ca_im;
 };
 
 // ------------------------------------------------------------------ kernels
@@ -157,11 +160,18 @@ __global__ void k_tau_reduce(const double *__restrict__ tau_jobs, const double *
     tau[ie] = t;
 }
 
-enum { WANT_D = 1, WANT_F = 2, WANT_L = 4 };
+enum { WANT_D = 1, WANT_F = 2, WANT_L = 4, WANT_A = 8, WANT_MIRROR = 16 };
 
 // One job per CTA.  slab (Nz blocks, leading dimension ld) first receives
 // the generator_r blocks; with WANT_D it ends up holding G_kk in block k.
 // out_first / out_last (leading dimension N) receive G_k1 / G_kNz.
+// WANT_A (with WANT_D): block k becomes cd * G_kk + ca * A_k, where
+// A_k = G_k1 Gamma_L G_k1^H is the spectral function injected by the left
+// lead, restricted to its open channels: Y_1 = G_11(:, open) sqrt(gamma_L),
+// Y_k = -gR(k-1) Y_{k-1}, A_k = Y_k Y_k^H (8 n_open N^2 flop per product).
+// WANT_MIRROR runs the same recursions with the slices numbered from the
+// right end (left-connected generators; the injecting lead is the right
+// one), writing every block at its own slice index.  Workspace: 6 blocks.
 template <int NB, int RPT, int MINB>
 __global__ void __launch_bounds__(NT, MINB)
     k_rgf_slab(Geo g, const RgfJob *__restrict__ jobs, int njobs, const double2 *__restrict__ Dexp,
@@ -177,8 +187,12 @@ __global__ void __launch_bounds__(NT, MINB)
     const int job = blockIdx.x;
     if (job >= njobs) return;
     double2 *A0 = ws + (size_t)blockIdx.x * wstride;
-    double2 *A1 = A0 + NB2, *T0 = A1 + NB2, *T1 = T0 + NB2, *T2 = T1 + NB2;
+    double2 *A1 = A0 + NB2, *T0 = A1 + NB2, *T1 = T0 + NB2, *T2 = T1 + NB2, *Zt = T2 + NB2;
     double2 *slab = slabs + (size_t)blockIdx.x * sstride;
+    const bool mirror = (want & WANT_MIRROR) != 0;
+    // slice of step x, and the slab block that holds it
+    auto sl = [&](int x) { return mirror ? Nz - 1 - x : x; };
+    auto blk = [&](int x) { return slab + NB2 * sl(x); };
     const RgfJob jb = jobs[job];
     const double2 E = make_double2(jb.e_re, jb.e_im);
     const int ik = jb.ik;
@@ -189,21 +203,21 @@ __global__ void __launch_bounds__(NT, MINB)
 
     if (want & (WANT_D | WANT_F)) {
         // generator_r, math_kernel.f90:81-91
-        form_block(cur, g, s, Nz - 1, E, ik, nullptr, Dexp);
+        form_block(cur, g, s, sl(Nz - 1), E, ik, nullptr, Dexp);
         __syncthreads();
         info = gj_invert<NB, RPT>(cur, N, ld, s);
-        unpermute(slab + NB2 * (Nz - 2), ld, cur, ld, N, s, 1.0);
+        unpermute(blk(Nz - 2), ld, cur, ld, N, s, 1.0);
         __syncthreads();
         for (int m = Nz - 3; m >= 0; --m) {
-            form_block(oth, g, s, m + 1, E, ik, cur, Dexp);
+            form_block(oth, g, s, sl(m + 1), E, ik, cur, Dexp);
             __syncthreads();
             r = gj_invert<NB, RPT>(oth, N, ld, s);
             if (r && !info) info = r;
-            unpermute(slab + NB2 * m, ld, oth, ld, N, s, 1.0);
+            unpermute(blk(m), ld, oth, ld, N, s, 1.0);
             __syncthreads();
             double2 *t = cur; cur = oth; oth = t;
         }
-        form_block(oth, g, s, 0, E, ik, cur, Dexp);
+        form_block(oth, g, s, sl(0), E, ik, cur, Dexp);
         __syncthreads();
         r = gj_invert<NB, RPT>(oth, N, ld, s);
         if (r && !info) info = r;
@@ -227,9 +241,43 @@ __global__ void __launch_bounds__(NT, MINB)
             // G_kk = gR(k-1) (I + G_{k-1,k-1} gR(k-1)), math_kernel.f90:94-109.
             // Block k-1 of the slab is replaced by G_{k-1,k-1} once gR(k-1)
             // has been used for the last time.
+            const bool wa = (want & WANT_A) != 0;
+            const double2 cd = wa ? make_double2(jb.cd_re, jb.cd_im) : make_double2(1.0, 0.0);
+            const double2 ca = make_double2(jb.ca_re, jb.ca_im);
+            int nA = 0;
+            double2 *Ya = A0, *Yb = A1;  // A0, A1 are free once the sweep is done
+            if (wa && (ca.x != 0.0 || ca.y != 0.0)) {
+                const double *gam = mirror ? s.gR : s.gL;
+                open_cols(N, s, gam);
+                __syncthreads();
+                nA = *s.nrows;
+                for (int e = threadIdx.x; e < N * nA; e += NT) {
+                    const int i = e % N, c = e / N, j = s.rows[c];
+                    const double sg = sqrt(gam[j]);
+                    const double2 v = T0[i + (size_t)ld * j];
+                    Ya[e] = make_double2(v.x * sg, v.y * sg);
+                }
+                __syncthreads();
+            }
+            // block += ca * Y Y^H, through Zt = Y^H (nA x N)
+            auto add_spectral = [&](double2 *dst, const double2 *Y) {
+                for (int e = threadIdx.x; e < N * nA; e += NT) {
+                    const int i = e % N, c = e / N;
+                    Zt[c + (size_t)nA * i] = make_double2(Y[e].x, -Y[e].y);
+                }
+                __syncthreads();
+                GemmArgs ga{dst, ld, Y, N, nullptr, Zt, nA, nullptr, N, N, nA, nullptr, ca};
+                cta_gemm(ga, s, GEMM_ADD_SCALED, g.delta);
+                __syncthreads();
+            };
             double2 *Gc = T0, *Gn = T2;
             for (int k = 1; k < Nz; ++k) {
-                double2 *gRk = slab + NB2 * (k - 1);
+                double2 *gRk = blk(k - 1);
+                if (nA) {
+                    GemmArgs gy{Yb, N, gRk, ld, nullptr, Ya, N, nullptr, N, nA, N, nullptr};
+                    cta_gemm(gy, s, GEMM_STORE_NEG, g.delta);
+                    __syncthreads();
+                }
                 GemmArgs g1{T1, ld, Gc, ld, nullptr, gRk, ld, nullptr, N, N, N, nullptr};
                 cta_gemm(g1, s, GEMM_STORE_ADD_EYE, g.delta);
                 __syncthreads();
@@ -238,17 +286,22 @@ __global__ void __launch_bounds__(NT, MINB)
                 __syncthreads();
                 for (int e = threadIdx.x; e < N * N; e += NT) {
                     const int i = e % N, j = e / N;
-                    gRk[i + (size_t)ld * j] = Gc[i + (size_t)ld * j];
+                    gRk[i + (size_t)ld * j] = zmul(cd, Gc[i + (size_t)ld * j]);
                 }
                 __syncthreads();
+                if (nA) {
+                    add_spectral(gRk, Ya);
+                    double2 *t = Ya; Ya = Yb; Yb = t;
+                }
                 double2 *t = Gc; Gc = Gn; Gn = t;
             }
-            double2 *last = slab + NB2 * (Nz - 1);
+            double2 *last = blk(Nz - 1);
             for (int e = threadIdx.x; e < N * N; e += NT) {
                 const int i = e % N, j = e / N;
-                last[i + (size_t)ld * j] = Gc[i + (size_t)ld * j];
+                last[i + (size_t)ld * j] = zmul(cd, Gc[i + (size_t)ld * j]);
             }
             __syncthreads();
+            if (nA) add_spectral(last, Ya);
         }
     }
     if ((want & WANT_L) && out_last) {
@@ -567,7 +620,7 @@ int slab_launch(negf_ctx *c, const Geo &g, const RgfJob *d_jobs, int njobs, cons
     const Variant v = pick_variant(g.N);
     if (v == VNONE) return NEGF_ERR_UNSUPPORTED;
     const size_t smem = variant_smem(v, g.N);
-    const size_t wstride = 5 * (size_t)g.ld * g.N;
+    const size_t wstride = 6 * (size_t)g.ld * g.N;
     int rc = ensure_ws(c, sizeof(double2) * wstride * njobs);
     if (rc) return rc;
     double2 *ws = (double2 *)c->d_ws;
@@ -628,12 +681,15 @@ int slab_jobs_in_flight(negf_ctx *c, size_t per_job_bytes, int njobs) {
 // their diagonal blocks, 2 dz^2 G_kk scaled by coef[job]:
 //   gsz == 0: every job sums into out[0] (density; chunks accumulate);
 //   gsz  > 0: jobs [o*gsz, (o+1)*gsz) sum into out[o] (LDOS per energy).
+// want selects the slab mode (WANT_D, or WANT_D | WANT_A [| WANT_MIRROR] with
+// the per-job cd / ca).
 int diag_accumulate(negf_ctx *c, const std::vector<RgfJob> &jobs, const std::vector<double2> &coef,
-                    int gsz, double2 *d_out, std::vector<int> &info_all, double &ms_total) {
+                    int gsz, double2 *d_out, std::vector<int> &info_all, double &ms_total,
+                    int want = WANT_D) {
     const int njobs = (int)jobs.size();
     const int N = c->N, Nz = c->Nz, ld = c->ld;
     const size_t sstride = (size_t)ld * N * Nz;
-    const size_t per_job = sizeof(double2) * (sstride + 5 * (size_t)ld * N);
+    const size_t per_job = sizeof(double2) * (sstride + 6 * (size_t)ld * N);
     int b = slab_jobs_in_flight(c, per_job, njobs);
     if (gsz > 0) b = (b / gsz) * gsz;
     if (b < std::max(gsz, 1)) return NEGF_ERR_NOMEM;
@@ -660,7 +716,7 @@ int diag_accumulate(negf_ctx *c, const std::vector<RgfJob> &jobs, const std::vec
         if (cudaMemcpyAsync(d_jobs, jobs.data() + j0, sizeof(RgfJob) * nb, cudaMemcpyHostToDevice, c->stream) ||
             cudaMemcpyAsync(d_coef, coef.data() + j0, sizeof(double2) * nb, cudaMemcpyHostToDevice, c->stream) ||
             cudaEventRecord(c->ev0, c->stream)) { rc = NEGF_ERR_CUDA; break; }
-        rc = slab_launch(c, g, d_jobs, nb, nullptr, d_slabs, sstride, WANT_D, nullptr, nullptr, d_info, c->stream);
+        rc = slab_launch(c, g, d_jobs, nb, nullptr, d_slabs, sstride, want, nullptr, nullptr, d_info, c->stream);
         if (rc) break;
         const size_t tot = (size_t)N * N * Nz * nout;
         const int blocks = (int)std::min<size_t>((tot + 255) / 256, (size_t)c->num_sms * 8);
@@ -680,6 +736,38 @@ int diag_accumulate(negf_ctx *c, const std::vector<RgfJob> &jobs, const std::vec
     cudaFree(d_jobs);
     cudaFree(d_info);
     return rc;
+}
+
+// n-point Gauss-Legendre rule on [-1, 1], nodes ascending.  Newton's method on
+// P_n from the guesses cos(pi (i + 3/4) / (n + 1/2)); P_n by the three-term
+// recurrence (k P_k = (2k-1) x P_{k-1} - (k-1) P_{k-2}), P_n' = n (x P_n - P_{n-1})
+// / (x^2 - 1), weights 2 / ((1 - x^2) P_n'(x)^2).
+void gauss_legendre(int n, std::vector<double> &x, std::vector<double> &w) {
+    x.assign(n, 0.0);
+    w.assign(n, 0.0);
+    auto eval = [n](double z, double *dp) {
+        double p0 = 1.0, p1 = z;
+        for (int k = 2; k <= n; ++k) {
+            const double p2 = ((2.0 * k - 1.0) * z * p1 - (k - 1.0) * p0) / k;
+            p0 = p1;
+            p1 = p2;
+        }
+        *dp = n * (z * p1 - p0) / (z * z - 1.0);
+        return p1;
+    };
+    for (int i = 0; i < (n + 1) / 2; ++i) {
+        double z = std::cos(PI * (i + 0.75) / (n + 0.5)), dp = 1.0;
+        for (int it = 0; it < 100; ++it) {
+            const double pn = eval(z, &dp);
+            const double step = pn / dp;
+            z -= step;
+            if (std::fabs(step) <= 1e-15) break;
+        }
+        eval(z, &dp);
+        x[i] = -z;
+        x[n - 1 - i] = z;
+        w[i] = w[n - 1 - i] = 2.0 / ((1.0 - z * z) * dp * dp);
+    }
 }
 
 int check_problem(const negf_problem *p) {
@@ -856,6 +944,72 @@ int negf_density(negf_ctx *c, int32_t n_circle, int32_t n_line, double min_v, do
         cudaError_t e = cudaMemcpy(dm, d_out, sizeof(double2) * per, cudaMemcpyDeviceToHost);
         if (e != cudaSuccess) rc = NEGF_ERR_CUDA;
     }
+    cudaFree(d_out);
+    if (rc) return rc;
+    fill_stats(stats, info, ms);
+    return first_info(info);
+}
+
+int negf_density_neq(negf_ctx *c, int32_t n_circle, int32_t n_window, double min_v, double mu_L,
+                     double mu_R, double gap, double temperature, double *dm, negf_stats *stats) {
+    if (!c || !dm || n_circle < 1 || n_window < 1 || !(temperature > 0) || !(gap > 0)) return NEGF_ERR_ARG;
+    if (cudaSetDevice(c->device) != cudaSuccess) return NEGF_ERR_CUDA;
+    const double mu_lo = std::min(mu_L, mu_R), mu_hi = std::max(mu_L, mu_R);
+    const bool right_injects = mu_R > mu_L;
+    const double kT = K_B * temperature, dz = c->Lz / c->Nz;
+    // semicircle from below the band bottom (negf.f90:37-41) to mu_lo - gap
+    const double circle_L = min_v - 1.0 / HARTREE, circle_R = mu_lo - gap;
+    if (!(circle_R > circle_L)) return NEGF_ERR_ARG;
+    const double E_c = (circle_R + circle_L) / 2, E_R = (circle_R - circle_L) / 2;
+    const double win_L = mu_lo - gap, win_R = mu_hi + gap;
+    std::vector<double> xc, wc, xw, ww;
+    gauss_legendre(n_circle, xc, wc);
+    gauss_legendre(n_window, xw, ww);
+    auto fermi = [kT](double e, double mu) { return 1.0 / (std::exp((e - mu) / kT) + 1.0); };
+    // One job list (semicircle nodes, then window nodes, per k-point) so that both
+    // kinds share the chunks the device memory allows; every job carries its own
+    // cd (and ca) and k_accumulate sums them with unit weight.
+    const int nk = c->nk, per_k = n_circle + n_window;
+    std::vector<RgfJob> jobs((size_t)per_k * nk);
+    for (int ik = 0; ik < nk; ++ik) {
+        const double w = c->kpt[3 * ik + 2];
+        for (int i = 0; i < n_circle; ++i) {
+            const double th = PI / 2 * (xc[i] + 1.0), cth = PI / 2 * wc[i];
+            RgfJob jb{};
+            jb.e_re = E_c + E_R * std::cos(th);
+            jb.e_im = E_R * std::sin(th) + c->eta;
+            jb.e_t = jb.e_re;
+            jb.ik = ik;
+            // w * 2/pi * c_theta * i * E_R * exp(i theta)
+            const double sc = w * 2.0 / PI * cth * E_R;
+            jb.cd_re = -sc * std::sin(th);
+            jb.cd_im = sc * std::cos(th);
+            jobs[(size_t)ik * per_k + i] = jb;
+        }
+        for (int i = 0; i < n_window; ++i) {
+            const double x = (win_L + win_R) / 2 + (win_R - win_L) / 2 * xw[i];
+            const double cx = (win_R - win_L) / 2 * ww[i];
+            const double flo = fermi(x, mu_lo), fhi = fermi(x, mu_hi);
+            RgfJob jb{};
+            jb.e_re = x;
+            jb.e_im = c->eta;
+            jb.e_t = x;
+            jb.ik = ik;
+            jb.cd_re = -(w * 2.0 / PI * cx * flo);
+            jb.ca_im = w / PI * cx * (fhi - flo) * (2.0 * dz * dz);
+            jobs[(size_t)ik * per_k + n_circle + i] = jb;
+        }
+    }
+    const std::vector<double2> unit(jobs.size(), make_double2(1.0, 0.0));
+    const size_t per = (size_t)c->N * c->N * c->Nz;
+    double2 *d_out = nullptr;
+    if (cudaMalloc(&d_out, sizeof(double2) * per) != cudaSuccess) { cudaGetLastError(); return NEGF_ERR_NOMEM; }
+    std::vector<int> info;
+    double ms = 0;
+    int rc = diag_accumulate(c, jobs, unit, 0, d_out, info, ms,
+                             WANT_D | WANT_A | (right_injects ? WANT_MIRROR : 0));
+    if (!rc && cudaMemcpy(dm, d_out, sizeof(double2) * per, cudaMemcpyDeviceToHost) != cudaSuccess)
+        rc = NEGF_ERR_CUDA;
     cudaFree(d_out);
     if (rc) return rc;
     fill_stats(stats, info, ms);
@@ -1153,6 +1307,26 @@ extern "C" int negf_density_real(negf_ctx *c, int32_t n_circle, int32_t n_line, 
     cudaFree(d_G);
     cudaFree(d_dens);
     return rc ? rc : info;
+}
+
+extern "C" int negf_dm_real(negf_ctx *c, const double *dm, int32_t Nx, int32_t Ny, double scale,
+                            double *density) {
+    if (!c || !dm || !density || Nx < 1 || Ny < 1) return NEGF_ERR_ARG;
+    if (cudaSetDevice(c->device) != cudaSuccess) return NEGF_ERR_CUDA;
+    const size_t per = (size_t)c->N * c->N * c->Nz, nd = (size_t)Nx * Ny * c->Nz;
+    double2 *d_G = nullptr;
+    double *d_dens = nullptr;
+    if (cudaMalloc(&d_G, sizeof(double2) * per) != cudaSuccess) { cudaGetLastError(); return NEGF_ERR_NOMEM; }
+    if (cudaMalloc(&d_dens, sizeof(double) * nd) != cudaSuccess) { cudaGetLastError(); cudaFree(d_G); return NEGF_ERR_NOMEM; }
+    int rc = 0;
+    if (cudaMemcpyAsync(d_G, dm, sizeof(double2) * per, cudaMemcpyHostToDevice, c->stream) != cudaSuccess) rc = NEGF_ERR_CUDA;
+    if (!rc) rc = launch_ptor(c, d_G, c->Nz, Nx, Ny, scale, d_dens, nullptr, c->stream);
+    if (!rc && (cudaMemcpyAsync(density, d_dens, sizeof(double) * nd, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+                cudaStreamSynchronize(c->stream) != cudaSuccess))
+        rc = NEGF_ERR_CUDA;
+    cudaFree(d_G);
+    cudaFree(d_dens);
+    return rc;
 }
 
 extern "C" int negf_ldos(negf_ctx *c, double e_lo, double e_hi, int32_t n_e, const int32_t *ldos_grid,

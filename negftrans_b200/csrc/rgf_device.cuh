@@ -300,6 +300,16 @@ __device__ inline void open_rows(int N, const Smem &s) {
     }
 }
 
+// rows[0..n) = the modes with gam[i] != 0 (open channels of one lead), ascending.
+__device__ inline void open_cols(int N, const Smem &s, const double *gam) {
+    if (threadIdx.x == 0) {
+        int n = 0;
+        for (int i = 0; i < N; ++i)
+            if (gam[i] != 0.0) s.rows[n++] = i;
+        *s.nrows = n;
+    }
+}
+
 // out(r, j) = inv(R)(rows[r], j) = R(prow[rows[r]], iprow[j]), r < n.
 __device__ inline void unpermute_rows(double2 *__restrict__ out, int ldo, const double2 *__restrict__ R,
                                       int ld, int N, int n, const Smem &s) {
@@ -363,7 +373,7 @@ struct WarpAcc {
 
 // C(i,j) = sum_k A(i, acol[k]) * B(k, bcol[j]) for one CTA, complex FP64.
 // acol/bcol == nullptr means identity.  Modes of the epilogue:
-enum GemmOut { GEMM_STORE = 0, GEMM_STORE_NEG = 1, GEMM_TAU = 2, GEMM_STORE_ADD_EYE = 3 };
+enum GemmOut { GEMM_STORE = 0, GEMM_STORE_NEG = 1, GEMM_TAU = 2, GEMM_STORE_ADD_EYE = 3, GEMM_ADD_SCALED = 4 };
 
 struct GemmArgs {
     double2 *C;
@@ -376,6 +386,7 @@ struct GemmArgs {
     const int *bcol;
     int M, Ncol, K;
     const int *rowmap;  // GEMM_TAU: row i of C is basis row rowmap[i] (nullptr = identity)
+    double2 beta;       // GEMM_ADD_SCALED: C += beta * (A B)
 };
 
 // Returns, for GEMM_TAU, this thread's partial sum of
@@ -451,7 +462,9 @@ __device__ inline double cta_gemm(const GemmArgs &a, const Smem &s, int mode, do
                             } else {
                                 if (mode == GEMM_STORE_NEG) v = make_double2(-v.x, -v.y);
                                 if (mode == GEMM_STORE_ADD_EYE && i == j) v.x += 1.0;
-                                a.C[i + (size_t)a.ldc * j] = v;
+                                double2 *cp = a.C + i + (size_t)a.ldc * j;
+                                if (mode == GEMM_ADD_SCALED) v = zfma(a.beta, v, *cp);
+                                *cp = v;
                             }
                         }
                     }

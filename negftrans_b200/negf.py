@@ -123,6 +123,27 @@ class Engine:
         self.last_stats = st
         return dens, dm, rc
 
+    def density_neq(self, n_circle, n_window, min_V, MU_L, MU_R, GAP, TEMPERATURE):
+        """Non-equilibrium Density_Matrix (N, N, N_z) under a bias MU_L != MU_R: a
+        Gauss-Legendre semicircle up to min(MU) - GAP plus a real-axis window
+        [min(MU) - GAP, max(MU) + GAP] whose sweeps also form the spectral
+        function injected by the higher lead (no reference counterpart)."""
+        dm = np.zeros((self.N, self.N, self.Nz), np.complex128, order="F")
+        st = Stats()
+        rc = check("negf_density_neq", lib().negf_density_neq(
+            self._ctx, n_circle, n_window, min_V, MU_L, MU_R, GAP, TEMPERATURE, dm.ctypes.data_as(_dp),
+            C.byref(st)))
+        self.last_stats = st
+        return dm, rc
+
+    def dm_real(self, dm, N_x, N_y, LX_A, LY_A, LZ_A):
+        """Density (N_x, N_y, N_z) in Angstrom^-3 of any Density_Matrix (main.f90:306-351, GPU)."""
+        dm = np.asfortranarray(dm, dtype=np.complex128)
+        dens = np.zeros((N_x, N_y, self.Nz), np.float64, order="F")
+        check("negf_dm_real", lib().negf_dm_real(self._ctx, dm.ctypes.data_as(_dp), N_x, N_y,
+                                                 self.Nz / (LX_A * LY_A * LZ_A), dens.ctypes.data_as(_dp)))
+        return dens
+
     def ldos(self, e_lo, e_hi, N_E, LDOS_GRID, N_x, N_y, LX_A, LY_A, LZ_A):
         """LDOS (M_x, M_y, M_z, N_E) after main.f90:417-554 (Angstrom^-n eV^-1)."""
         from .constants import HARTREE

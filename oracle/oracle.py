@@ -404,3 +404,73 @@ def closed_form_tau(nx, ny, vz, Lx, Ly, Lz, V_L, V_R, eta, energy, kx, ky, latti
 
 lapack_path = _build.lapack_path
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "liboracle.so")
+
+
+# ------------------------------------------- non-equilibrium density (no reference counterpart)
+def lead_gammas(p: Problem, energy, kx, ky):
+    """gamma_L, gamma_R = sin(q dz)/dz^2 of grid.f90:355-365 at a real energy."""
+    delta = p.Lz / p.Nz
+    ax = _kin(p.nx.astype(np.float64), p.Lx, kx)
+    ay = _kin(p.ny.astype(np.float64), p.Ly, ky)
+    qL = np.sqrt(np.maximum(2 * (energy - p.V_L) - ax * ax - ay * ay, 0.0))
+    qR = np.sqrt(np.maximum(2 * (energy - p.V_R) - ax * ax - ay * ay, 0.0))
+    return np.sin(qL * delta) / (delta * delta), np.sin(qR * delta) / (delta * delta)
+
+
+def density_neq_contour(p: Problem, n_circle, n_window, min_v, mu_L, mu_R, gap, temperature):
+    """The jobs of the biased density: list of (kind, energy, kx, ky, c_D, c_A).
+
+    Semicircle (negf.f90:37-65 geometry) from min_v - 1 eV to mu_lo - gap with
+    Gauss-Legendre nodes in theta, coefficient w 2/pi c_theta i E_R e^{i theta};
+    real-axis window [mu_lo - gap, mu_hi + gap] with Gauss-Legendre nodes x:
+    c_D = -w 2/pi c_x f(x - mu_lo) on G and c_A = i w/pi c_x (f(x - mu_hi) -
+    f(x - mu_lo)) (2 dz^2) on G_ks Gamma_s G_ks^H (s = the lead at mu_hi).
+    Both are then scaled by 2 dz^2 like every G of negf.f90:78."""
+    mu_lo, mu_hi = min(mu_L, mu_R), max(mu_L, mu_R)
+    kT = K_B * temperature
+    dz = p.Lz / p.Nz
+    cl, cr = min_v - 1.0 / HARTREE, mu_lo - gap
+    E_c, E_R = (cr + cl) / 2, (cr - cl) / 2
+    wl, wr = mu_lo - gap, mu_hi + gap
+    xc, wc = np.polynomial.legendre.leggauss(n_circle)
+    xw, ww = np.polynomial.legendre.leggauss(n_window)
+    fermi = lambda e, mu: 1.0 / (np.exp((e - mu) / kT) + 1.0)
+    jobs = []
+    for kx, ky, w in p.kpt:
+        for x, c in zip(xc, wc):
+            th, cth = PI / 2 * (x + 1), PI / 2 * c
+            z = E_c + E_R * np.exp(1j * th)
+            jobs.append(("circle", z, kx, ky, w * 2 / PI * cth * 1j * E_R * np.exp(1j * th), 0.0))
+        for x, c in zip(xw, ww):
+            e = (wl + wr) / 2 + (wr - wl) / 2 * x
+            cx = (wr - wl) / 2 * c
+            flo, fhi = fermi(e, mu_lo), fermi(e, mu_hi)
+            jobs.append(("window", complex(e), kx, ky, -(w * 2 / PI * cx * flo),
+                         1j * w / PI * cx * (fhi - flo) * (2 * dz * dz)))
+    return jobs
+
+
+def density_neq(p: Problem, n_circle, n_window, min_v, mu_L, mu_R, gap, temperature):
+    """Density_Matrix (N, N, Nz) under a bias, from the oracle's tri_solver
+    (math_kernel.f90:44-165: D blocks, and the F or L column for the injecting
+    lead) per job of density_neq_contour."""
+    dz = p.Lz / p.Nz
+    right = mu_R > mu_L
+    dm = np.zeros((p.N, p.N, p.Nz), np.complex128, order="F")
+    info_all = 0
+    for kind, z, kx, ky, cd, ca in density_neq_contour(p, n_circle, n_window, min_v, mu_L, mu_R,
+                                                       gap, temperature):
+        H = hamiltonian(p, kx, ky)
+        D = e_minus_h(p, H, z + 1j * p.eta, kx, ky)
+        want = "D" + (("L" if right else "F") if ca != 0 else "")
+        outs, info = tri_solver(D, want)
+        info_all = info_all or info
+        term = cd * outs["D"]
+        if ca != 0:
+            gL, gR = lead_gammas(p, z.real, kx, ky)
+            gam = gR if right else gL
+            C = outs["L" if right else "F"]
+            for k in range(p.Nz):
+                term[:, :, k] += ca * (C[:, :, k] * gam[None, :]) @ C[:, :, k].conj().T
+        dm += term * (2 * dz * dz)
+    return dm, info_all

@@ -280,3 +280,42 @@ def test_lattice_lead_model(oracle, flat):
         eps = ((2.0 * pr.nx * np.pi / a.LX) ** 2 + (2.0 * pr.ny * np.pi / a.LY) ** 2) / 2
         n_open = [np.sum(np.abs(2 * dz * dz * (e - eps) - 2) < 2) for e in E]
         np.testing.assert_allclose(tau, n_open, atol=1e-4)
+
+
+@pytest.mark.parametrize("bias", ["left", "right", "none"])
+def test_density_neq_small(oracle, bias):
+    """Biased density matrix (Gauss-Legendre semicircle + real-axis window with the
+    spectral function of the injecting lead) against the oracle's tri_solver
+    restatement; 'right' runs the mirrored sweep."""
+    pr = small_problem(nz=8, nk=2)
+    a = pr.atomic
+    vb = W.MSTAR * 1e-3 / HARTREE  # 1 mV
+    mu_L, mu_R = {"left": (a.MU + vb, a.MU), "right": (a.MU, a.MU + vb), "none": (a.MU, a.MU)}[bias]
+    n_c, n_w = 6, 10
+    dm_ref, _ = oracle.density_neq(oracle_problem(oracle, pr), n_c, n_w, pr.min_V, mu_L, mu_R, a.GAP,
+                                   a.TEMPERATURE)
+    with Engine(*pr.engine_args()) as eng:
+        dm, info = eng.density_neq(n_c, n_w, pr.min_V, mu_L, mu_R, a.GAP, a.TEMPERATURE)
+        assert info == 0
+        assert rel_err(dm, dm_ref) < RTOL
+        if bias == "left":
+            Nx = Ny = 32
+            dens = eng.dm_real(dm, Nx, Ny, 1000.0, 1000.0, pr.Nz * 10.0)
+            ref = oracle.density_from_matrix(dm_ref, pr.nx, pr.ny, Nx, Ny, 1000.0, 1000.0, pr.Nz * 10.0)
+            assert rel_err(dens, ref) < RTOL
+
+
+def test_density_neq_wide_basis(oracle):
+    """N > 256 (the 2-rows-per-thread slab variant) with many open channels."""
+    nz = 4
+    V = W.MSTAR * W.qpc_potential(64, 64, nz, 100.0, nz * 1.0, 0.050, 15.0, 1.0, disorder=0.002)
+    pr = P.prepare(W._deck(nz * 10.0, 14.5e-3, 30.0, 16), V)
+    assert pr.N > 256
+    a = pr.atomic
+    vb = W.MSTAR * 1e-3 / HARTREE
+    dm_ref, _ = oracle.density_neq(oracle_problem(oracle, pr), 2, 3, pr.min_V, a.MU + vb, a.MU, a.GAP,
+                                   a.TEMPERATURE)
+    with Engine(*pr.engine_args()) as eng:
+        dm, info = eng.density_neq(2, 3, pr.min_V, a.MU + vb, a.MU, a.GAP, a.TEMPERATURE)
+    assert info == 0
+    assert rel_err(dm, dm_ref) < RTOL

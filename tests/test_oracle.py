@@ -215,3 +215,55 @@ def test_lattice_leads_closed_form_is_unitary(oracle):
         # the reference's continuum lead term reflects a little at the ends
         t_ref = oracle.closed_form_tau(nx, ny, vz, lx, ly, lz, 0.0, 0.0, 1e-12, e, 0.0, 0.0)
         assert t_ref <= t + 1e-9
+
+
+def _xy_problem(oracle, nz=6, eta=1e-6 / HARTREE, symmetric=True, vl=0.0, vr=0.0, nk=(1, 2)):
+    """A small device whose potential varies in x, y and z (plane-wave blocks are dense);
+    symmetric=True makes it even under slice reversal."""
+    lx = ly = 400 / A_0
+    lz = nz * 10 / A_0
+    nx, ny = oracle.basis(0.03 / HARTREE, lx, ly)
+    g = 16
+    x = (np.arange(g) - g / 2) / g
+    z = np.arange(nz) + 0.5 - nz / 2 if symmetric else np.arange(nz) * 0.7 - 1.0
+    V = (0.02 / HARTREE * (1 - np.exp(-x[:, None, None] ** 2 / 0.02)) * np.exp(-z[None, None, :] ** 2 / 4.0)
+         * (1 + 0.3 * np.cos(2 * PI * x[None, :, None])))
+    vh = oracle.vhat_all(np.asfortranarray(V), 5, 5)
+    kp = oracle.kmesh(nk[0], nk[1], lx, ly)
+    return oracle.Problem(nx, ny, vh, lx, ly, lz, vl, vr, eta, kp)
+
+
+def test_spectral_functions_sum_to_the_diagonal(oracle):
+    """i (G_kk - G_kk^H) = 2 dz^2 (G_k1 Gamma_L G_k1^H + G_kNz Gamma_R G_kNz^H) as eta -> 0:
+    the spectral-function term of density_neq has the right lead widths and scale."""
+    p = _xy_problem(oracle, nz=5, eta=1e-13, symmetric=False, vl=0.001 / HARTREE)
+    assert p.N > 4
+    dz = p.Lz / p.Nz
+    for e in (0.004 / HARTREE, 0.012 / HARTREE):
+        kx, ky, _ = p.kpt[1]
+        D = oracle.e_minus_h(p, oracle.hamiltonian(p, kx, ky), e + 1j * p.eta, kx, ky)
+        outs, info = oracle.tri_solver(D, "DFL")
+        assert info == 0
+        gL, gR = oracle.lead_gammas(p, e, kx, ky)
+        assert np.count_nonzero(gL) > 0
+        for k in range(p.Nz):
+            G, F, L = outs["D"][:, :, k], outs["F"][:, :, k], outs["L"][:, :, k]
+            lhs = 1j * (G - G.conj().T)
+            rhs = 2 * dz * dz * ((F * gL) @ F.conj().T + (L * gR) @ L.conj().T)
+            assert np.max(np.abs(lhs - rhs)) <= 1e-7 * np.max(np.abs(lhs)), k
+
+
+def test_density_neq_mirror_symmetry(oracle):
+    """On a device even under slice reversal, swapping mu_L and mu_R mirrors the
+    density matrix in z (left-injected F column vs right-injected L column)."""
+    p = _xy_problem(oracle, nz=6)
+    mu = 0.008 / HARTREE
+    T = 0.5
+    gap = 6 * (8.617333262e-5 / HARTREE) * T
+    a, _ = oracle.density_neq(p, 6, 10, 0.0, mu + 0.002 / HARTREE, mu, gap, T)
+    b, _ = oracle.density_neq(p, 6, 10, 0.0, mu, mu + 0.002 / HARTREE, gap, T)
+    assert np.max(np.abs(a - b[:, :, ::-1])) <= 1e-9 * np.max(np.abs(a))
+    # the bias term is present: differs from the zero-bias matrix
+    c, _ = oracle.density_neq(p, 6, 10, 0.0, mu, mu, gap, T)
+    assert np.max(np.abs(a - c)) > 1e-4 * np.max(np.abs(a))
+
