@@ -422,12 +422,57 @@ def run_batched(args):
         e.close()
 
 
+def run_surrogate(args):
+    """Surrogate-guided energy sampling on seeded QPC + disorder devices (N = 69,
+    100 slices of 1 nm): RGF training data, GPU training of the 4 x 256 GELU
+    network, then per unseen device the RGF solves needed for the integral of
+    T over [0, 30) meV to 1e-4 with uniform nodes and with surrogate-placed
+    nodes (every node an RGF solve)."""
+    from negftrans_b200 import surrogate as S
+    n_train, n_test, n_e = 512, 32, 256
+    t0 = time.perf_counter()
+    train = S.sample_devices(n_train, seed=11, nz=100)
+    e_train = np.linspace(0.0, S.E_MAX_MEV, n_e)
+    T = S.training_set(train, e_train)
+    t1 = time.perf_counter()
+    sur = S.Surrogate(seed=0)
+    steps, batch = (3000, 1500), 4096
+    hist = sur.fit(train, e_train, T, steps=steps, lr=(1e-3, 2e-4), batch=batch)
+    t2 = time.perf_counter()
+    rows = S.compare(sur, S.sample_devices(n_test, seed=99, nz=100), tol=1e-4)
+    t3 = time.perf_counter()
+    sur.close()
+    w = S.WIDTHS
+    # forward + backward ~ 3x the forward MACs, 2 flop each
+    flop_step = 6.0 * batch * sum(a * b for a, b in zip(w[:-1], w[1:]))
+    n_u = [r["uniform"] for r in rows]
+    n_a = [r["adaptive"] for r in rows]
+    ok = [i for i in range(len(rows)) if n_u[i] and n_a[i]]
+    line = {"metric": "RGF solves for the T(E) integral to 1e-4 (uniform / surrogate-placed)",
+            "value": (sum(n_u[i] for i in ok) / sum(n_a[i] for i in ok)) if ok else None,
+            "unit": "ratio", "higher_is_better": True, "n_gpus": 1, "data": "synthetic",
+            "config": {"workload": "qpc_disorder_surrogate", "N": 69, "Nz": 100, "train_devices": n_train,
+                       "energies_per_device": n_e, "test_devices": n_test, "network": w,
+                       "precision": "bf16 operands, fp32 accumulate, fp32 Adam"},
+            "uniform_solves_mean": float(np.mean([n_u[i] for i in ok])) if ok else None,
+            "surrogate_solves_mean": float(np.mean([n_a[i] for i in ok])) if ok else None,
+            "surrogate_max_abs_err_median": float(np.median([r["surrogate_max_abs_err"] for r in rows])),
+            "train": {"steps": sum(steps), "batch": batch, "seconds": t2 - t1,
+                      "tflops": flop_step * sum(steps) / (t2 - t1) / 1e12,
+                      "loss_first": float(hist[:50].mean()), "loss_last": float(hist[-50:].mean())},
+            "datagen_seconds": t1 - t0, "datagen_solves": n_train * n_e, "eval_seconds": t3 - t2,
+            "unreached": len(rows) - len(ok)}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "batched_uneven":
         run_batched(args)
+    elif args.workload == "surrogate":
+        run_surrogate(args)
     else:
         run_ours(args)
 

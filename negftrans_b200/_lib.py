@@ -27,6 +27,11 @@ EXPORTS = (
     "negf_density_real", "negf_ldos", "negf_basis_k", "negf_transmission_batch",
     "negf_density_neq", "negf_dm_real",
 )
+# every symbol include/negf_mlp.h declares
+MLP_EXPORTS = (
+    "negf_mlp_create", "negf_mlp_destroy", "negf_mlp_param_count", "negf_mlp_set_params",
+    "negf_mlp_get_params", "negf_mlp_forward", "negf_mlp_grad", "negf_mlp_train",
+)
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -94,6 +99,17 @@ def lib():
     L.negf_density_neq.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
                                    C.c_double, C.c_double, _dp, C.POINTER(Stats)]
     L.negf_dm_real.argtypes = [C.c_void_p, _dp, C.c_int32, C.c_int32, C.c_double, _dp]
+    _fp = C.POINTER(C.c_float)
+    L.negf_mlp_create.argtypes = [C.c_int32, _ip, C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]
+    L.negf_mlp_destroy.argtypes = [C.c_void_p]
+    L.negf_mlp_param_count.argtypes = [C.c_void_p]
+    L.negf_mlp_param_count.restype = C.c_int64
+    L.negf_mlp_set_params.argtypes = [C.c_void_p, _fp]
+    L.negf_mlp_get_params.argtypes = [C.c_void_p, _fp]
+    L.negf_mlp_forward.argtypes = [C.c_void_p, _fp, C.c_int32, _fp]
+    L.negf_mlp_grad.argtypes = [C.c_void_p, _fp, _fp, _fp, C.c_int32, _dp, _fp]
+    L.negf_mlp_train.argtypes = [C.c_void_p, _fp, _fp, _fp, C.c_int64, C.c_int32, C.c_int32, C.c_float,
+                                 C.c_uint64, _dp]
     _lib = L
     return L
 

@@ -13,8 +13,10 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libnegfgpu.so")
 DRIVER = os.path.join(PKG, "negftrans")   # the main.f90-style executable
-SOURCES = ["negf_engine.cu", "negf_host.cpp"]
+SOURCES = ["negf_engine.cu", "negf_host.cpp", "mlp.cu"]
 HEADERS = ["rgf_device.cuh"]
+PUBLIC_HEADERS = ["negf_gpu.h", "negf_mlp.h"]
+OBJDIR = os.path.join(PKG, "_build")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -24,7 +26,7 @@ def _stale() -> bool:
         return True
     t = os.path.getmtime(LIB)
     deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
-    deps.append(os.path.join(ROOT, "include", "negf_gpu.h"))
+    deps += [os.path.join(ROOT, "include", h) for h in PUBLIC_HEADERS]
     return any(os.path.getmtime(d) > t for d in deps)
 
 
@@ -43,12 +45,21 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not _stale():
         build_driver()
         return LIB
-    cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
-           "-I", os.path.join(ROOT, "include"), "-I", CSRC, "-cudart", "static", "-o", LIB]
+    # one object per source, compiled in parallel, then one link
+    os.makedirs(OBJDIR, exist_ok=True)
+    base = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+            "-I", os.path.join(ROOT, "include"), "-I", CSRC]
     if verbose:
-        cmd += ["-Xptxas", "-v"]
-    cmd += [os.path.join(CSRC, f) for f in SOURCES]
-    subprocess.run(cmd, check=True)
+        base += ["-Xptxas", "-v"]
+    procs, objs = [], []
+    for f in SOURCES:
+        obj = os.path.join(OBJDIR, os.path.splitext(f)[0] + ".o")
+        objs.append(obj)
+        procs.append((f, subprocess.Popen(base + ["-c", os.path.join(CSRC, f), "-o", obj])))
+    bad = [f for f, p in procs if p.wait() != 0]
+    if bad:
+        raise RuntimeError("nvcc failed on " + ", ".join(bad))
+    subprocess.run([NVCC, *ARCH, "-shared", "-cudart", "static", *objs, "-o", LIB], check=True)
     build_driver(force=True)
     return LIB
 

@@ -1,5 +1,5 @@
-"""The C-ABI library loads and exports every symbol include/negf_gpu.h
-declares; argument errors come back as status codes (no GPU needed)."""
+"""The C-ABI library loads and exports every symbol include/negf_gpu.h and
+include/negf_mlp.h declare; argument errors come back as status codes (no GPU needed)."""
 import ctypes as C
 import os
 import re
@@ -8,21 +8,22 @@ import pytest
 
 from negftrans_b200 import _lib
 
-HDR = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "negf_gpu.h")
+INC = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
 
 
-def declared_symbols():
-    src = open(HDR).read()
-    return sorted(set(re.findall(r"^\s*(?:int|const char \*)\s*(negf_\w+)\s*\(", src, re.M)))
+def declared_symbols(header="negf_gpu.h"):
+    src = open(os.path.join(INC, header)).read()
+    return sorted(set(re.findall(r"^\s*(?:int|int64_t|const char \*)\s*(negf_\w+)\s*\(", src, re.M)))
 
 
 def test_header_and_binding_agree():
     assert sorted(_lib.EXPORTS) == declared_symbols()
+    assert sorted(_lib.MLP_EXPORTS) == declared_symbols("negf_mlp.h")
 
 
 def test_library_exports_all(built_lib):
     L = C.CDLL(built_lib)
-    for name in declared_symbols():
+    for name in declared_symbols() + declared_symbols("negf_mlp.h"):
         assert hasattr(L, name), name
 
 

@@ -267,3 +267,30 @@ def test_density_neq_mirror_symmetry(oracle):
     c, _ = oracle.density_neq(p, 6, 10, 0.0, mu, mu, gap, T)
     assert np.max(np.abs(a - c)) > 1e-4 * np.max(np.abs(a))
 
+
+def test_mlp_oracle_bf16_rounding():
+    from oracle import mlp_oracle as M
+    x = np.array([1.0, 1 + 2.0 ** -8, 1 + 3 * 2.0 ** -8, -2.5, 3.0e-5, 1 + 2.0 ** -9])
+    np.testing.assert_array_equal(M.bf16(x), [1.0, 1.0, 1 + 2.0 ** -6, -2.5, M.bf16(3.0e-5), 1.0])
+    assert abs(M.bf16(3.0e-5) - 3.0e-5) <= 2.0 ** -9 * 3.0e-5
+
+
+def test_mlp_oracle_gradient_finite_differences():
+    """The FP64 network's backward pass against central differences of its loss."""
+    from oracle import mlp_oracle as M
+    rng = np.random.default_rng(7)
+    widths = [5, 7, 6, 3]
+    n = sum(a * b + b for a, b in zip(widths[:-1], widths[1:]))
+    p = rng.standard_normal(n) * 0.5
+    x = rng.standard_normal((9, 5))
+    t = rng.standard_normal((9, 3))
+    w = rng.uniform(0.5, 1.5, (9, 3))
+    _, g = M.loss_and_grad(p, widths, x, t, w, bf16_ops=False)
+    eps = 1e-6
+    fd = np.empty(n)
+    for i in range(n):
+        e = np.zeros(n)
+        e[i] = eps
+        fd[i] = (M.loss_and_grad(p + e, widths, x, t, w, False)[0]
+                 - M.loss_and_grad(p - e, widths, x, t, w, False)[0]) / (2 * eps)
+    assert np.max(np.abs(fd - g)) <= 1e-7 * max(1.0, np.max(np.abs(g)))
