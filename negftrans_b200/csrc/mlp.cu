@@ -52,9 +52,12 @@ struct Gemm {
     const float *bias;  // [N]            (EPI_BIAS, EPI_BIAS_GELU)
     float *Z;           // pre-activation (EPI_BIAS_GELU), ld = ldc
     const float *gate;  // gelu'(gate) multiplies C (EPI_GELU_GRAD), ld = ldc
+    int kchunk;         // split K: block z covers k in [z*kchunk, (z+1)*kchunk) (0 = all of K)
+    long cz;            // split K: block z stores its partial C at C + z*cz (EPI_STORE only)
 };
 
-// C = A B with BF16 operands and FP32 accumulation.  Grid (ceil(N/BN), ceil(M/BM)).
+// C = A B with BF16 operands and FP32 accumulation.  Grid (ceil(N/BN), ceil(M/BM),
+// K splits); with splits, each z-slice of the grid writes its partial product.
 __global__ void __launch_bounds__(GT) k_gemm_bf16(Gemm g) {
     __shared__ __align__(16) __nv_bfloat16 sA[BM * KP];  // [m][k]
     __shared__ __align__(16) __nv_bfloat16 sB[BN * KP];  // [n][k]
@@ -69,25 +72,33 @@ __global__ void __launch_bounds__(GT) k_gemm_bf16(Gemm g) {
         for (int b = 0; b < 4; ++b)
 #pragma unroll
             for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.f;
-    for (int k0 = 0; k0 < g.K; k0 += BK) {
-        // stage: pairs of k so that each shared word holds two BF16 values
+    const int kbeg = g.kchunk ? blockIdx.z * g.kchunk : 0;
+    const int kend = g.kchunk ? min(g.K, kbeg + g.kchunk) : g.K;
+    float *C = g.C + (g.kchunk ? blockIdx.z * g.cz : 0);
+    for (int k0 = kbeg; k0 < kend; k0 += BK) {
+        // stage: pairs of k so that each shared word holds two BF16 values;
+        // consecutive threads walk the operand's unit-stride index (coalesced)
         for (int e = tid; e < BM * BK / 2; e += GT) {
-            const int mm = e / (BK / 2), kk = 2 * (e % (BK / 2));
+            const bool mfast = g.sam == 1;
+            const int mm = mfast ? e % BM : e / (BK / 2);
+            const int kk = 2 * (mfast ? e / BM : e % (BK / 2));
             const int m = m0 + mm, k = k0 + kk;
             float x0 = 0.f, x1 = 0.f;
             if (m < g.M) {
-                if (k < g.K) x0 = g.A[m * g.sam + k * g.sak];
-                if (k + 1 < g.K) x1 = g.A[m * g.sam + (k + 1) * g.sak];
+                if (k < kend) x0 = g.A[m * g.sam + k * g.sak];
+                if (k + 1 < kend) x1 = g.A[m * g.sam + (k + 1) * g.sak];
             }
             *(uint32_t *)&sA[mm * KP + kk] = pack_bf16(x0, x1);
         }
         for (int e = tid; e < BN * BK / 2; e += GT) {
-            const int nn = e / (BK / 2), kk = 2 * (e % (BK / 2));
+            const bool nfast = g.sbn == 1;
+            const int nn = nfast ? e % BN : e / (BK / 2);
+            const int kk = 2 * (nfast ? e / BN : e % (BK / 2));
             const int n = n0 + nn, k = k0 + kk;
             float x0 = 0.f, x1 = 0.f;
             if (n < g.N) {
-                if (k < g.K) x0 = g.B[k * g.sbk + n * g.sbn];
-                if (k + 1 < g.K) x1 = g.B[(k + 1) * g.sbk + n * g.sbn];
+                if (k < kend) x0 = g.B[k * g.sbk + n * g.sbn];
+                if (k + 1 < kend) x1 = g.B[(k + 1) * g.sbk + n * g.sbn];
             }
             *(uint32_t *)&sB[nn * KP + kk] = pack_bf16(x0, x1);
         }
@@ -139,7 +150,7 @@ __global__ void __launch_bounds__(GT) k_gemm_bf16(Gemm g) {
                     v = gelu(v);
                 }
                 if (g.epi == EPI_GELU_GRAD) v *= gelu_grad(g.gate[o]);
-                g.C[o] = v;
+                C[o] = v;
             }
 }
 
@@ -177,13 +188,14 @@ __global__ void __launch_bounds__(1024) k_mse(const float *y, const float *t, co
     for (long i = threadIdx.x; i < n; i += blockDim.x) dy[i] = sc * w[i] * (y[i] - t[i]);
 }
 
-// db[n] = sum_m dz[m, n]
-__global__ void k_colsum(const float *dz, int M, int N, float *db) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= N) return;
-    float s = 0.f;
-    for (int m = 0; m < M; ++m) s += dz[(long)m * N + n];
-    db[n] = s;
+// C[m*ldc + n] = sum over z < nz of ws[z*M*N + m*N + n]  (split-K partials, fixed order)
+__global__ void k_splitk_sum(const float *ws, int nz, int M, int N, float *C, int ldc) {
+    const long tot = (long)M * N;
+    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < tot; e += (long)gridDim.x * blockDim.x) {
+        float s = 0.f;
+        for (int z = 0; z < nz; ++z) s += ws[z * tot + e];
+        C[(e / N) * ldc + e % N] = s;
+    }
 }
 
 // Adam on the packed parameters (FP32 master copy).
@@ -223,6 +235,8 @@ struct negf_mlp {
     std::vector<float *> Z, Y;  // per layer: pre-activation and output [max_batch x width[l+1]]
     float *d0 = nullptr, *d1 = nullptr;  // gradient ping-pong [max_batch x max width]
     float *xb = nullptr, *tb = nullptr, *wb = nullptr, *dy = nullptr;
+    float *ws = nullptr;    // split-K partial products
+    float *ones = nullptr;  // [max_batch] of 1.0: bias gradients as products
     double *loss = nullptr;
     long step = 0;
     cudaStream_t st = nullptr;
@@ -230,11 +244,37 @@ struct negf_mlp {
 
 namespace {
 
-int gemm(cudaStream_t st, const Gemm &g) {
-    if (g.M <= 0 || g.N <= 0) return 0;
-    dim3 grid((g.N + BN - 1) / BN, (g.M + BM - 1) / BM);
-    k_gemm_bf16<<<grid, GT, 0, st>>>(g);
-    return cudaGetLastError() == cudaSuccess ? 0 : NEGF_MLP_ERR_CUDA;
+constexpr int MAX_SPLITS = 16;
+
+// Launches C = A B; a product with few output tiles and a long K (the weight
+// gradients, K = batch) is split along K into partial products that one more
+// kernel sums in a fixed order.
+int gemm(negf_mlp *mm, const Gemm &g0) {
+    if (g0.M <= 0 || g0.N <= 0) return 0;
+    Gemm g = g0;
+    g.kchunk = 0;
+    g.cz = 0;
+    const int tiles = ((g.N + BN - 1) / BN) * ((g.M + BM - 1) / BM);
+    int splits = 1;
+    if (g.epi == EPI_STORE && tiles < 148 && g.K >= 8 * BK)
+        splits = std::min({MAX_SPLITS, (2 * 148 + tiles - 1) / tiles, g.K / (4 * BK)});
+    if (splits > 1) {
+        const int kc = ((g.K + splits - 1) / splits + BK - 1) / BK * BK;
+        splits = (g.K + kc - 1) / kc;
+        g.kchunk = kc;
+        g.C = mm->ws;
+        g.ldc = g.N;
+        g.cz = (long)g.M * g.N;
+    }
+    dim3 grid((g.N + BN - 1) / BN, (g.M + BM - 1) / BM, splits);
+    k_gemm_bf16<<<grid, GT, 0, mm->st>>>(g);
+    if (cudaGetLastError() != cudaSuccess) return NEGF_MLP_ERR_CUDA;
+    if (splits > 1) {
+        const int blocks = (int)std::min<long>(((long)g.M * g.N + 255) / 256, 148 * 4);
+        k_splitk_sum<<<blocks, 256, 0, mm->st>>>(mm->ws, splits, g.M, g.N, g0.C, g0.ldc);
+        if (cudaGetLastError() != cudaSuccess) return NEGF_MLP_ERR_CUDA;
+    }
+    return 0;
 }
 
 // Forward pass of B rows of m->xb; the outputs are m->Y[L-1].
@@ -245,7 +285,7 @@ int forward(negf_mlp *m, const float *x, int B) {
         const bool last = l == m->L - 1;
         Gemm g{in, K, 1, m->p + m->woff[l], 1, K, m->Y[l], N, B, N, K,
                last ? EPI_BIAS : EPI_BIAS_GELU, m->p + m->boff[l], m->Z[l], nullptr};
-        if (int rc = gemm(m->st, g)) return rc;
+        if (int rc = gemm(m, g)) return rc;
         in = m->Y[l];
     }
     return 0;
@@ -262,14 +302,15 @@ int backward(negf_mlp *m, const float *x, const float *t, const float *w, int B)
         const float *in = l ? m->Y[l - 1] : x;
         // dW_l (N x K) = dz^T (N x B) * in (B x K)
         Gemm gw{dz, 1, N, in, K, 1, m->g + m->woff[l], K, N, K, B, EPI_STORE, nullptr, nullptr, nullptr};
-        if (int rc = gemm(m->st, gw)) return rc;
-        k_colsum<<<(N + 127) / 128, 128, 0, m->st>>>(dz, B, N, m->g + m->boff[l]);
-        if (cudaGetLastError() != cudaSuccess) return NEGF_MLP_ERR_CUDA;
+        if (int rc = gemm(m, gw)) return rc;
+        // db_l (N x 1) = dz^T (N x B) * ones (B x 1)
+        Gemm gb{dz, 1, N, m->ones, 1, 0, m->g + m->boff[l], 1, N, 1, B, EPI_STORE, nullptr, nullptr, nullptr};
+        if (int rc = gemm(m, gb)) return rc;
         if (l == 0) break;
         // dz_{l-1} (B x K) = (dz (B x N) * W_l (N x K)) * gelu'(Z_{l-1})
         float *dn = (dz == m->d0) ? m->d1 : m->d0;
         Gemm gd{dz, N, 1, m->p + m->woff[l], K, 1, dn, K, B, K, N, EPI_GELU_GRAD, nullptr, nullptr, m->Z[l - 1]};
-        if (int rc = gemm(m->st, gd)) return rc;
+        if (int rc = gemm(m, gd)) return rc;
         dz = dn;
     }
     return 0;
@@ -327,6 +368,14 @@ int negf_mlp_create(int32_t n_layers, const int32_t *widths, int32_t max_batch, 
     alloc(&m->tb, (size_t)max_batch * widths[n_layers]);
     alloc(&m->wb, (size_t)max_batch * widths[n_layers]);
     alloc(&m->dy, (size_t)max_batch * widths[n_layers]);
+    size_t mn = 0;
+    for (int l = 0; l < n_layers; ++l) mn = std::max(mn, (size_t)widths[l + 1] * widths[l]);
+    alloc(&m->ws, MAX_SPLITS * mn);
+    alloc(&m->ones, (size_t)max_batch);
+    if (ok) {
+        std::vector<float> one((size_t)max_batch, 1.0f);
+        ok = cudaMemcpy(m->ones, one.data(), sizeof(float) * max_batch, cudaMemcpyHostToDevice) == cudaSuccess;
+    }
     if (ok) ok = cudaMalloc(&m->loss, sizeof(double)) == cudaSuccess;
     if (ok) ok = cudaMemsetAsync(m->p, 0, sizeof(float) * m->np, m->st) == cudaSuccess &&
                  cudaMemsetAsync(m->m1, 0, sizeof(float) * m->np, m->st) == cudaSuccess &&
@@ -345,7 +394,7 @@ int negf_mlp_destroy(negf_mlp *m) {
     if (!m) return NEGF_MLP_OK;
     cudaSetDevice(m->device);
     if (m->st) cudaStreamSynchronize(m->st);
-    for (float *q : {m->p, m->g, m->m1, m->m2, m->d0, m->d1, m->xb, m->tb, m->wb, m->dy}) cudaFree(q);
+    for (float *q : {m->p, m->g, m->m1, m->m2, m->d0, m->d1, m->xb, m->tb, m->wb, m->dy, m->ws, m->ones}) cudaFree(q);
     for (float *q : m->Z) cudaFree(q);
     for (float *q : m->Y) cudaFree(q);
     cudaFree(m->loss);

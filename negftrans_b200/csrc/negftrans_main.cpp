@@ -39,6 +39,10 @@ struct Deck {
     // Engine key with no reference counterpart: effective mass m*/m_e (the
     // reference's kinetic term is |k+G|^2/2, i.e. m* = 1).
     double EMASS = 1;
+    // Engine key with no reference counterpart: NEQ = .true. accepts VDS != 0
+    // (rejected by main.f90:129-132) and computes the biased density with
+    // mu_L = MU + VDS/2, mu_R = MU - VDS/2 (negf_density_neq).
+    bool NEQ = false;
 };
 
 // Folds EMASS = m* into the energy scale: E' = m* E, V' = m* V, eta' = m* eta,
@@ -189,6 +193,7 @@ bool read_namelist(const std::string &path, Deck &d, std::string &err) {
         else if (k == "n_circle") ok = int1(&d.N_circle);
         else if (k == "n_line_per_ev") ok = int1(&d.N_line_per_eV);
         else if (k == "emass") ok = real1(&d.EMASS);
+        else if (k == "neq") ok = log1(&d.NEQ);
         else { err = "unknown namelist item " + k; return false; }
         if (!ok) return false;
     }
@@ -318,7 +323,8 @@ int main(int argc, char **argv) {
         bad.push_back("ERROR: LDOS_ENERGY_GRID must be specified for (if_LDOS = .true.)");
     if (d.if_LDOS && (d.LDOS_GRID[0] < -1 || d.LDOS_GRID[1] < -1 || d.LDOS_GRID[2] < -1))
         bad.push_back("ERROR: LDOS_GRID must be specified for (if_LDOS = .true.)");
-    if (d.VDS != 0) bad.push_back("ERROR: VDS must be zero in this version, please upgrade to higher version.");
+    if (d.VDS != 0 && !d.NEQ)
+        bad.push_back("ERROR: VDS must be zero in this version, please upgrade to higher version.");
     std::fprintf(out, " Checking Parameters...\n");
     for (auto &b : bad) std::fprintf(out, " %s\n", b.c_str());
     if (!bad.empty()) {
@@ -367,12 +373,13 @@ int main(int argc, char **argv) {
                     "\"if_density\": %d, \"if_transmission\": %d, \"if_LDOS\": %d, \"ETA\": %.17g, \"ENCUT\": %.17g, "
                     "\"LX\": %.17g, \"LY\": %.17g, \"LZ\": %.17g, \"TRANSMISSION_GRID\": [%.17g, %.17g, %.17g], "
                     "\"LDOS_GRID\": [%d, %d, %d], \"N_circle\": %d, \"N_line_per_eV\": %d, \"min_V\": %.17g, "
-                    "\"V_sum\": %.17g, \"MU\": %.17g, \"TEMPERATURE\": %.17g, \"EMASS\": %.17g}\n",
+                    "\"V_sum\": %.17g, \"MU\": %.17g, \"TEMPERATURE\": %.17g, \"EMASS\": %.17g, \"NEQ\": %d, "
+                    "\"VDS\": %.17g}\n",
                     N, Nz, Nx, Ny, d.NGX, d.NGY, d.NKX * d.NKY, d.if_density, d.if_transmission, d.if_LDOS, d.ETA,
                     d.ENCUT, d.LX, d.LY, d.LZ, d.TRANSMISSION_GRID[0], d.TRANSMISSION_GRID[1],
                     d.TRANSMISSION_GRID[2], d.LDOS_GRID[0], d.LDOS_GRID[1], d.LDOS_GRID[2], d.N_circle,
                     d.N_line_per_eV, min_v, [&] { double t = 0; for (double x : V) t += x; return t; }(), d.MU,
-                    d.TEMPERATURE, emass);
+                    d.TEMPERATURE, emass, (int)d.NEQ, d.VDS);
         std::fclose(out);
         return 0;
     }
@@ -401,7 +408,27 @@ int main(int argc, char **argv) {
     double t_dens = 0, t_trans = 0, t_ldos = 0;
     std::vector<double> density, tau, ldos;
     int ldos_m[4] = {0, 0, 0, 0};
-    if (d.if_density) {
+    if (d.if_density && d.NEQ) {
+        // biased density: Gauss-Legendre semicircle (N_circle nodes) and a real-axis
+        // window [min(mu) - GAP, max(mu) + GAP] with N_line_per_eV nodes per eV
+        const double aVDS = d.VDS / HARTREE;
+        const int n_window = std::max(1, nint(d.N_line_per_eV * ((2 * aGAP + std::fabs(aVDS)) * HARTREE)));
+        std::fprintf(out, " Density calculation start (bias VDS = %s eV)...\n Number of energy points for integration: %d\n",
+                     gfmt(d.VDS / emass).c_str(), d.N_circle + n_window);
+        density.assign((size_t)Nx * Ny * Nz, 0.0);
+        std::vector<double> dm(2 * (size_t)N * N * Nz);
+        const auto a = std::chrono::steady_clock::now();
+        rc = negf_density_neq(ctx, d.N_circle, n_window, min_v, aMU + aVDS / 2, aMU - aVDS / 2, aGAP, d.TEMPERATURE,
+                              dm.data(), &st);
+        if (rc >= 0) {
+            const int r2 = negf_dm_real(ctx, dm.data(), Nx, Ny, (double)Nz / (d.LX * d.LY * d.LZ), density.data());
+            if (r2 < 0) rc = r2;
+        }
+        t_dens = std::chrono::duration<double>(std::chrono::steady_clock::now() - a).count();
+        if (rc < 0) { std::fprintf(out, " ERROR: density failed (%d)\n", rc); negf_ctx_destroy(ctx); std::fclose(out); return 1; }
+        if (rc > 0) std::fprintf(out, " WARNING: zero pivot in %d contour jobs (first job %d)\n", st.n_singular, st.first_bad_job);
+        std::fprintf(out, " Density calculation DONE\n ----------\n");
+    } else if (d.if_density) {
         const int n_line = nint(d.N_line_per_eV * ((2 * aGAP) * HARTREE));  // main.f90:261
         std::fprintf(out, " Density calculation start...\n Number of energy points for integration: %d\n", d.N_circle + n_line);
         density.assign((size_t)Nx * Ny * Nz, 0.0);

@@ -72,7 +72,7 @@ def loss_and_grad(params, widths, x, t, w, bf16_ops=True):
         h, _ = cache[l]
         W, _ = layers[l]
         gW = q(dz).T @ q(h)
-        gb = dz.sum(axis=0)
+        gb = q(dz).sum(axis=0)
         grads[l] = (gW, gb)
         if l:
             dz = (q(dz) @ q(W)) * gelu_grad(cache[l - 1][1])

@@ -244,3 +244,40 @@ def test_emass_end_to_end(driver, tmp_path):
     la = np.array((a / "LDOS").read_text().split("\n", 1)[1].split(), float)
     lb = np.array((b / "LDOS").read_text().split("\n", 1)[1].split(), float)
     assert np.max(np.abs(la - M_EFF * lb)) <= 1e-6 * np.max(np.abs(M_EFF * lb))
+
+
+def test_neq_key_accepts_a_bias(driver, tmp_path):
+    """VDS != 0 is the reference's error unless the engine key NEQ is set."""
+    (tmp_path / "INPUT").write_text("&INPUT\n LX=1 LY=1 LZ=1 NKX=1 NKY=1 if_density=.true. VDS=0.001 NEQ=.true.\n/\n")
+    _potential(tmp_path / "POTENTIAL", np.zeros((4, 4, 2)))
+    d = json.loads(_run(driver, tmp_path, "--check").stdout)
+    assert d["NEQ"] == 1 and d["VDS"] == 0.001
+
+
+@pytest.mark.gpu
+def test_neq_density_end_to_end(driver, tmp_path, oracle):
+    """DENSITY under a bias (NEQ = .true., VDS = 1 mV x m*) against the oracle's
+    biased density matrix and PtoR."""
+    nz = 6
+    V = W.MSTAR * W.qpc_potential(32, 32, nz, 100.0, nz * 1.0, 0.05, 15.0, 1.0, disorder=0.002)
+    vds = W.MSTAR * 1e-3
+    (tmp_path / "INPUT").write_text(
+        "&INPUT\n if_density=.true. NEQ=.true.\n"
+        f" LX=1000.0 LY=1000.0 LZ={nz * 10.0} ENCUT=1.2E-3 ETA=2.4622D-9 VDS={vds!r}\n"
+        " NKX=1 NKY=2 TEMPERATURE=1.0 MU=1.0E-3 N_circle=5 N_line_per_eV=4000\n/\n\n")
+    _potential(tmp_path / "POTENTIAL", V)
+    r = _run(driver, tmp_path, check=False)
+    assert r.returncode == 0, (tmp_path / "OUTPUT").read_text()
+    Vf = np.array((tmp_path / "POTENTIAL").read_text().split()[3:], float).reshape(V.shape, order="F")
+    deck = P.InputDeck(if_density=True, LX=1000.0, LY=1000.0, LZ=nz * 10.0, ENCUT=1.2e-3, ETA=2.4622e-9,
+                       NKX=1, NKY=2, TEMPERATURE=1.0, MU=1.0e-3, N_circle=5, N_line_per_eV=4000)
+    pr = P.prepare(deck, Vf)
+    a = pr.atomic
+    p = oracle.Problem(pr.nx, pr.ny, pr.vhat, a.LX, a.LY, a.LZ, a.V_L, a.V_R, a.ETA, pr.kpoint)
+    avds = vds / HARTREE
+    n_window = int(math.floor(4000 * ((2 * a.GAP + abs(avds)) * HARTREE) + 0.5))
+    dm, _ = oracle.density_neq(p, 5, n_window, pr.min_V, a.MU + avds / 2, a.MU - avds / 2, a.GAP, a.TEMPERATURE)
+    ref = oracle.density_from_matrix(dm, pr.nx, pr.ny, 32, 32, 1000.0, 1000.0, nz * 10.0)
+    dtext = (tmp_path / "DENSITY").read_text().split("\n", 1)
+    dens = np.array(dtext[1].split(), float).reshape((32, 32, nz), order="F")
+    assert np.max(np.abs(dens - ref)) <= 1e-7 * np.max(np.abs(ref))
