@@ -395,6 +395,17 @@ def run_batched(args):
     probs = W.batched_uneven()
     engines = [Engine(*p["args"]) for p in probs]
     E_all = np.linspace(0.0, W.MSTAR * 0.030 / 27.211386245988, 1024, endpoint=False)
+    # tile shapes by the autotuner: per basis size, time the variants on a full
+    # wave (296 energies) of the shortest device of that size and use the winner
+    # for all of them
+    tuned = {}
+    for N in sorted({p["N"] for p in probs}):
+        idx = min((i for i, p in enumerate(probs) if p["N"] == N), key=lambda i: probs[i]["Nz"])
+        v, rates = engines[idx].autotune(E_all[:296])
+        tuned[N] = {"variant": v, "solves_per_s": [round(float(r), 2) for r in rates]}
+        for i, p in enumerate(probs):
+            if p["N"] == N:
+                engines[i].set_variant(v)
     perm = np.random.default_rng(2024).permutation(len(E_all))
     B = args.batch
     batches = [E_all[perm[(s * B + np.arange(B)) % len(E_all)]] for s in range(args.warmup + args.steps)]
@@ -414,7 +425,8 @@ def run_batched(args):
             "vs_baseline": None, "dtype": "c128", "data": "synthetic",
             "config": {"workload": "batched_uneven", "problems": len(probs),
                        "N_range": [min(p["N"] for p in probs), max(p["N"] for p in probs)],
-                       "Nz": sorted({p["Nz"] for p in probs}), "energies_per_step": B},
+                       "Nz": sorted({p["Nz"] for p in probs}), "energies_per_step": B,
+                       "tuned_variants": tuned},
             "inverse_tflops": flops / (ms * 1e-3) / 1e12, "e2e_seconds_per_step": statistics.mean(times),
             "singular": info}
     print(json.dumps(line), flush=True)

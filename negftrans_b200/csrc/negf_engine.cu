@@ -472,6 +472,8 @@ struct negf_ctx {
     int N = 0, Nz = 0, ld = 0, ngx = 0, ngy = 0, nk = 0;
     double Lx = 0, Ly = 0, Lz = 0, V_L = 0, V_R = 0, eta = 0;
     int lead_model = 0;
+    int variant = -1;         // transmission kernel variant forced by negf_set_variant /
+                              // negf_autotune; -1 = chosen by N
     std::vector<double> kpt;  // nk x 3
     double2 *d_vhat = nullptr;
     int *d_nx = nullptr, *d_ny = nullptr;
@@ -546,6 +548,12 @@ Variant pick_variant(int N) {
     if (N <= 4 * NT) return V8x4;
     return VNONE;
 }
+bool variant_fits(int v, int N) {
+    return (v == V16x1 && N <= NT) || (v == V16x2 && N <= 2 * NT) || (v == V8x4 && N <= 4 * NT);
+}
+Variant ctx_variant(const negf_ctx *c) {
+    return (c->variant >= 0 && variant_fits(c->variant, c->N)) ? (Variant)c->variant : pick_variant(c->N);
+}
 size_t variant_smem(Variant v, int N) {
     switch (v) {
         case V16x1: return smem_bytes<16>(N);
@@ -581,7 +589,7 @@ int resident_ctas(int N) {
 int transmission_launch(negf_ctx *c, const double *d_E, int nE, double *d_tau, double *d_tau_jobs,
                         int *d_info, cudaStream_t st) {
     const int njobs = nE * c->nk;
-    const Variant v = pick_variant(c->N);
+    const Variant v = ctx_variant(c);
     if (v == VNONE) return NEGF_ERR_UNSUPPORTED;
     const size_t smem = variant_smem(v, c->N);
     int occ = 1, rc = 0;
@@ -885,6 +893,36 @@ int negf_transmission(negf_ctx *c, const double *energies, int32_t nE, int32_t p
     return first_info(info);
 }
 
+int negf_set_variant(negf_ctx *c, int32_t variant) {
+    if (!c || variant < -1 || variant > V8x4) return NEGF_ERR_ARG;
+    if (variant >= 0 && !variant_fits(variant, c->N)) return NEGF_ERR_UNSUPPORTED;
+    c->variant = variant;
+    return NEGF_OK;
+}
+
+int negf_autotune(negf_ctx *c, const double *energies, int32_t nE, int32_t *chosen, double *rates) {
+    if (!c || !energies || nE < 1) return NEGF_ERR_ARG;
+    std::vector<double> tau(nE);
+    double best = -1.0;
+    int bv = -1;
+    const int keep = c->variant;
+    for (int v = V16x1; v <= V8x4; ++v) {
+        if (rates) rates[v] = 0.0;
+        if (!variant_fits(v, c->N)) continue;
+        c->variant = v;
+        negf_stats st{};
+        int rc = negf_transmission(c, energies, nE, NEGF_FP64, tau.data(), &st);  // first use: set-up
+        if (rc >= 0) rc = negf_transmission(c, energies, nE, NEGF_FP64, tau.data(), &st);
+        if (rc < 0) { c->variant = keep; return rc; }
+        const double r = st.device_ms > 0 ? (double)nE * c->nk / (st.device_ms * 1e-3) : 0.0;
+        if (rates) rates[v] = r;
+        if (r > best) { best = r; bv = v; }
+    }
+    c->variant = bv;
+    if (chosen) *chosen = bv;
+    return bv >= 0 ? NEGF_OK : NEGF_ERR_UNSUPPORTED;
+}
+
 int negf_density(negf_ctx *c, int32_t n_circle, int32_t n_line, double min_v, double mu, double gap,
                  double temperature, double *dm, negf_stats *stats) {
     if (!c || !dm || n_circle < 2 || n_line < 2) return NEGF_ERR_ARG;
@@ -1155,7 +1193,7 @@ extern "C" int negf_transmission_batch(negf_ctx *const *ctxs, int32_t nctx, cons
     for (int v = V16x1; v <= V8x4 && !rc; ++v) {
         std::vector<int> members;
         for (int p = 0; p < nctx; ++p)
-            if (pick_variant(ctxs[p]->N) == v) members.push_back(p);
+            if (ctx_variant(ctxs[p]) == v) members.push_back(p);
         if (members.empty()) continue;
         std::vector<Geo> geos;
         std::vector<BatchJob> jobs;

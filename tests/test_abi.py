@@ -38,6 +38,9 @@ def test_argument_errors_without_gpu(built_lib):
     assert L.negf_ctx_create(None, 0, C.byref(C.c_void_p())) == _lib.NEGF_ERR_ARG
     assert L.negf_transmission(None, None, 0, 0, None, None) == _lib.NEGF_ERR_ARG
     assert L.negf_density(None, 4, 4, 0.0, 0.0, 0.0, 1.0, None, None) == _lib.NEGF_ERR_ARG
+    assert L.negf_set_variant(None, 0) == _lib.NEGF_ERR_ARG
+    assert L.negf_autotune(None, None, 0, None, None) == _lib.NEGF_ERR_ARG
+    assert L.negf_density_neq(None, 4, 4, 0.0, 0.0, 0.0, 1.0, 1.0, None, None) == _lib.NEGF_ERR_ARG
     buf = (C.c_double * 8)()
     # N_z = 1: the reference indexes generator_r(:,:,0); rejected here
     assert L.negf_tri_solve(None, buf, 1, 1, b"F", buf, None, None) == _lib.NEGF_ERR_ARG

@@ -319,3 +319,23 @@ def test_density_neq_wide_basis(oracle):
         dm, info = eng.density_neq(2, 3, pr.min_V, a.MU + vb, a.MU, a.GAP, a.TEMPERATURE)
     assert info == 0
     assert rel_err(dm, dm_ref) < RTOL
+
+
+@pytest.mark.gpu
+def test_every_variant_and_the_autotuner(oracle):
+    """Each transmission kernel variant that can hold N (forced per context)
+    matches the oracle; the autotuner keeps the fastest of them."""
+    pr = small_problem(nz=8, nk=2)
+    E = P.transmission_energies(pr.atomic, 16)[::2]
+    tau_ref, _ = oracle.transmission_jobs(oracle_problem(oracle, pr), E, nthreads=4)
+    with Engine(*pr.engine_args()) as eng:
+        for v in (0, 1, 2):
+            eng.set_variant(v)
+            tau, info = eng.transmission(E)
+            assert info == 0
+            np.testing.assert_allclose(tau, tau_ref, rtol=RTOL, atol=1e-12)
+        v, rates = eng.autotune(E)
+        assert v in (0, 1, 2) and rates[v] == rates.max() > 0
+        tau, _ = eng.transmission(E)
+        np.testing.assert_allclose(tau, tau_ref, rtol=RTOL, atol=1e-12)
+        eng.set_variant(-1)
