@@ -254,9 +254,12 @@ __device__ inline void form_block(double2 *__restrict__ M, const Geo &g, const S
     const double2 *vs = g.vhat ? g.vhat + (size_t)g.W * g.H * k : nullptr;
     const double2 *Dk = Dexp ? Dexp + (size_t)N * N * k : nullptr;
     for (int j0 = 0; j0 < N; j0 += 4) {
-        for (int i = threadIdx.x; i < N; i += NT) {
+        // thread t reads row t of R (coalesced) and writes the row i of M it
+        // belongs to, i = iprow[t] (prow[i] = t): scattered stores instead of
+        // scattered loads
+        for (int t = threadIdx.x; t < N; t += NT) {
             double2 d[4], r[4];
-            const int pi = R ? s.prow[i] : 0;
+            const int i = R ? s.iprow[t] : t;
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 const int j = j0 + q;
@@ -265,7 +268,7 @@ __device__ inline void form_block(double2 *__restrict__ M, const Geo &g, const S
                 if (j < N) {
                     if (Dk) d[q] = Dk[i + (size_t)N * j];
                     else d[q] = d_element(g, s, vs, k, E, ik, i, j, s.nx[j], s.ny[j]);
-                    if (R) r[q] = R[pi + (size_t)ld * s.iprow[j]];
+                    if (R) r[q] = R[t + (size_t)ld * s.iprow[j]];
                 }
             }
 #pragma unroll
@@ -280,9 +283,9 @@ __device__ inline void unpermute(double2 *__restrict__ out, int ldo, const doubl
                                  int ld, int N, const Smem &s, double scale) {
     for (int j = 0; j < N; ++j) {
         const int jc = s.iprow[j];
-        for (int i = threadIdx.x; i < N; i += NT) {
-            double2 v = R[s.prow[i] + (size_t)ld * jc];
-            out[i + (size_t)ldo * j] = make_double2(v.x * scale, v.y * scale);
+        for (int t = threadIdx.x; t < N; t += NT) {  // coalesced loads, scattered stores
+            double2 v = R[t + (size_t)ld * jc];
+            out[s.iprow[t] + (size_t)ldo * j] = make_double2(v.x * scale, v.y * scale);
         }
     }
 }
