@@ -436,23 +436,35 @@ def run_batched(args):
 
 def run_surrogate(args):
     """Surrogate-guided energy sampling on seeded QPC + disorder devices (N = 69,
-    100 slices of 1 nm): RGF training data, GPU training of the 4 x 256 GELU
-    network, then per unseen device the RGF solves needed for the integral of
+    100 slices of 1 nm): RGF training data (T and the probe LDOS), GPU training
+    of the 4 x 256 GELU network, then per unseen device the RGF solves needed for the integral of
     T over [0, 30) meV to 1e-4 with uniform nodes and with surrogate-placed
     nodes (every node an RGF solve)."""
     from negftrans_b200 import surrogate as S
     n_train, n_test, n_e = 512, 32, 256
     t0 = time.perf_counter()
     train = S.sample_devices(n_train, seed=11, nz=100)
-    e_train = np.linspace(0.0, S.E_MAX_MEV, n_e)
-    T = S.training_set(train, e_train)
+    e_train = S.training_energies(n_e)
+    T, L = S.training_set(train, n_e)
     t1 = time.perf_counter()
     sur = S.Surrogate(seed=0)
     steps, batch = (3000, 1500), 4096
-    hist = sur.fit(train, e_train, T, steps=steps, lr=(1e-3, 2e-4), batch=batch)
+    hist = sur.fit(train, e_train, T, L, steps=steps, lr=(1e-3, 2e-4), batch=batch)
     t2 = time.perf_counter()
-    rows = S.compare(sur, S.sample_devices(n_test, seed=99, nz=100), tol=1e-4)
+    test = S.sample_devices(n_test, seed=99, nz=100)
+    rows = S.compare(sur, test, tol=1e-4)
     t3 = time.perf_counter()
+    # probe LDOS of 4 unseen devices: the network against RGF (median relative error)
+    errs = []
+    for d in test[:4]:
+        rgf = S.RGF(d)
+        try:
+            ref = rgf.ldos_probes(n_e)
+        finally:
+            rgf.close()
+        pred = sur.predict_ldos(d.desc, e_train)
+        errs.append(np.median(np.abs(pred - ref) / np.maximum(ref, 1e-30)))
+    ldos_err = float(np.median(errs))
     sur.close()
     w = S.WIDTHS
     # forward + backward ~ 3x the forward MACs, 2 flop each
@@ -472,7 +484,8 @@ def run_surrogate(args):
             "train": {"steps": sum(steps), "batch": batch, "seconds": t2 - t1,
                       "tflops": flop_step * sum(steps) / (t2 - t1) / 1e12,
                       "loss_first": float(hist[:50].mean()), "loss_last": float(hist[-50:].mean())},
-            "datagen_seconds": t1 - t0, "datagen_solves": n_train * n_e, "eval_seconds": t3 - t2,
+            "ldos_probe_median_rel_err": ldos_err,
+            "datagen_seconds": t1 - t0, "datagen_solves": n_train * n_e * 2, "eval_seconds": t3 - t2,
             "unreached": len(rows) - len(ok)}
     print(json.dumps(line), flush=True)
 

@@ -4,10 +4,11 @@ No counterpart in the reference: NEGFtrans evaluates T(E) on the uniform grid
 E_i = E1 + (E2 - E1)(i - 1)/N_E (main.f90:369-375) and every point costs one
 RGF sweep.  Here a small network, trained on the GPU by this package's own
 kernels (include/negf_mlp.h) on RGF outputs of seeded QPC + disorder
-devices, predicts log T(E) for an unseen device from 16 descriptors of its
-potential; the prediction only decides WHERE the RGF is evaluated (node
-density from the predicted curvature), and every reported point, as well as
-the integral, comes from RGF solves.
+devices, predicts log T(E) and the LDOS at 8 probe sites of the constriction
+plane for an unseen device from 16 descriptors of its potential; the
+prediction only decides WHERE the RGF is evaluated (node density from the
+predicted curvature), and every reported point, as well as the integral,
+comes from RGF solves.
 
 Devices: the split-gate QPC of ``workloads.qpc_potential`` in the 100 x 100 nm
 cell (GaAs by input scaling), V_g ~ U[20, 80] meV, w ~ U[8, 25] nm, 2 meV /
@@ -24,7 +25,7 @@ import numpy as np
 
 from . import _lib
 from . import prepare as P
-from .constants import HARTREE
+from .constants import A_0, HARTREE
 from .negf import Engine
 from .workloads import MSTAR, _deck, qpc_potential
 
@@ -33,7 +34,16 @@ E_MAX_MEV = 30.0               # energy window [0, E_MAX_MEV) meV
 T_FLOOR = 0.01                 # the network predicts log(T + T_FLOOR)
 MODES = [(0, 0), (1, 0), (0, 1), (1, 1), (2, 0), (0, 2), (2, 1), (1, 2), (2, 2), (3, 0), (0, 3), (3, 1),
          (1, 3), (4, 0)]
-WIDTHS = [17, 256, 256, 256, 256, 1]   # energy + 16 descriptors -> 4 GELU layers of 256 -> log T
+N_PROBES = 8
+WIDTHS = [17, 256, 256, 256, 256, 1 + N_PROBES]  # energy + 16 descriptors -> 4 GELU layers -> log T, log LDOS
+LDOS_FLOOR = 1e-3              # the network predicts log(LDOS / LDOS_ref + LDOS_FLOOR)
+GRID = 64                      # real-space grid of the POTENTIAL (x, y)
+
+
+def probe_sites(grid=GRID):
+    """(x, y) grid indices of the 8 LDOS probes: along x from the channel axis
+    outwards (0 ... 22 nm in steps of 3.1 nm) at the cell's centre line in y."""
+    return [(grid // 2 + 2 * i, grid // 2) for i in range(N_PROBES)]
 _fp = C.POINTER(C.c_float)
 _dp = C.POINTER(C.c_double)
 
@@ -170,31 +180,57 @@ class RGF:
             raise RuntimeError(f"zero pivot in the RGF sweep (info {info})")
         return np.asarray(tau)
 
+    def ldos_probes(self, n_e):
+        """LDOS (Angstrom^-3 eV^-1, physical units) at the probe sites of the
+        constriction slice z = N_z/2 on the grid E_i = E_MAX i / n_e, i < n_e
+        (main.f90:417-554 with LDOS_GRID = 0 0 N_z/2+1): shape (n_e, 8)."""
+        a = self.pr.atomic
+        Nx, Ny, Nz = self.pr.shape
+        L = self.eng.ldos(0.0, float(energies_hartree(E_MAX_MEV)), n_e, (0, 0, Nz // 2 + 1), Nx, Ny,
+                          a.LX * A_0, a.LY * A_0, a.LZ * A_0)[0]
+        self.solves += n_e * len(self.pr.kpoint)
+        # LDOS per scaled eV -> per physical eV (E' = m* E)
+        return np.stack([L[x, y, 0, :] for x, y in probe_sites(Nx)], axis=1) * MSTAR
+
     def close(self):
         self.eng.close()
 
 
 # ------------------------------------------------------------------ surrogate
 class Surrogate:
-    """Normalisation + network: (E, descriptors) -> log(T + T_FLOOR)."""
+    """Normalisation + network: (E, descriptors) -> log(T + T_FLOOR) and
+    log(LDOS / LDOS_ref + LDOS_FLOOR) at the probe sites."""
 
     def __init__(self, device=0, seed=0, widths=WIDTHS, max_batch=8192):
         self.net = MLP(widths, max_batch=max_batch, device=device, seed=seed)
         self.mu = None
         self.sd = None
+        self.ldos_ref = 1.0
 
     def features(self, desc, e_mev):
         e = np.asarray(e_mev, np.float64)
         d = np.broadcast_to((desc - self.mu) / self.sd, (len(e), len(desc)))
         return np.concatenate([(e[:, None] / E_MAX_MEV) * 2 - 1, d], axis=1).astype(np.float32)
 
-    def fit(self, devices, e_mev, T, steps=(2000, 1000), lr=(1e-3, 2e-4), batch=4096, seed=0):
-        """T[i, j] = RGF transmission of devices[i] at e_mev[j]; returns the loss history."""
+    def fit(self, devices, e_mev, T, ldos=None, steps=(2000, 1000), lr=(1e-3, 2e-4), batch=4096, seed=0):
+        """T[i, j] = RGF transmission of devices[i] at e_mev[j], ldos[i, j, p] the
+        probe LDOS there (None: the LDOS outputs get zero weight); returns the
+        loss history."""
         D = np.stack([d.desc for d in devices])
         self.mu, self.sd = D.mean(axis=0), D.std(axis=0) + 1e-9
         X = np.concatenate([self.features(d.desc, e_mev) for d in devices])
-        Y = np.log(np.asarray(T, np.float64).reshape(-1, 1) + T_FLOOR).astype(np.float32)
-        Wt = np.ones_like(Y)
+        yt = np.log(np.asarray(T, np.float64).reshape(-1, 1) + T_FLOOR)
+        n_out = self.net.widths[-1]
+        if ldos is not None and n_out > 1:
+            L = np.asarray(ldos, np.float64).reshape(-1, n_out - 1)
+            self.ldos_ref = float(np.median(L[L > 0])) if np.any(L > 0) else 1.0
+            yl = np.log(np.maximum(L, 0.0) / self.ldos_ref + LDOS_FLOOR)
+            Wt = np.ones((len(yt), n_out), np.float32)
+        else:
+            yl = np.zeros((len(yt), n_out - 1))
+            Wt = np.zeros((len(yt), n_out), np.float32)
+            Wt[:, 0] = 1.0
+        Y = np.concatenate([yt, yl], axis=1).astype(np.float32)
         hist = []
         for s, (n, r) in enumerate(zip(steps, lr)):
             hist.append(self.net.train(X, Y, Wt, n, batch=batch, lr=r, seed=seed + s))
@@ -203,6 +239,11 @@ class Surrogate:
     def predict(self, desc, e_mev):
         y = self.net.forward(self.features(desc, e_mev))[:, 0].astype(np.float64)
         return np.maximum(np.exp(y) - T_FLOOR, 0.0)
+
+    def predict_ldos(self, desc, e_mev):
+        """Probe LDOS (n_e, 8) in the units of RGF.ldos_probes."""
+        y = self.net.forward(self.features(desc, e_mev))[:, 1:].astype(np.float64)
+        return np.maximum(np.exp(y) - LDOS_FLOOR, 0.0) * self.ldos_ref
 
     def close(self):
         self.net.close()
@@ -292,12 +333,22 @@ def compare(sur: Surrogate, devices, tol=1e-4, n_dense=4096, device=0):
     return rows
 
 
-def training_set(devices, e_mev, device=0):
-    T = np.zeros((len(devices), len(e_mev)))
+def training_energies(n_e):
+    """The grid E_i = E_MAX i / n_e (i < n_e) of both training targets (meV)."""
+    return E_MAX_MEV * np.arange(n_e) / n_e
+
+
+def training_set(devices, n_e, device=0, with_ldos=True):
+    """RGF transmission (n_dev, n_e) and probe LDOS (n_dev, n_e, 8) on training_energies(n_e)."""
+    e_mev = training_energies(n_e)
+    T = np.zeros((len(devices), n_e))
+    L = np.zeros((len(devices), n_e, N_PROBES)) if with_ldos else None
     for i, dev in enumerate(devices):
         rgf = RGF(dev, device=device)
         try:
             T[i] = rgf.T(e_mev)
+            if with_ldos:
+                L[i] = rgf.ldos_probes(n_e)
         finally:
             rgf.close()
-    return T
+    return T, L

@@ -99,20 +99,23 @@ def test_mlp_training_fits_a_smooth_function():
 
 @pytest.mark.gpu
 def test_surrogate_guided_sampling_on_unseen_devices():
-    """Trained on RGF transmission of 48 seeded QPC + disorder devices, the
+    """Trained on RGF transmission and probe LDOS of 48 seeded QPC + disorder devices, the
     surrogate places the nodes of unseen devices.  Every node is an RGF solve,
     both node sets reach the 1e-4 integral tolerance, and the solve counts of
     the two methods are what the comparison reports (the measured ratio on
     this device family is recorded by bench.py --surrogate)."""
     train = S.sample_devices(48, seed=11, nz=60)
-    e_train = np.linspace(0.0, S.E_MAX_MEV, 96)
-    T = S.training_set(train, e_train)
+    e_train = S.training_energies(96)
+    T, L = S.training_set(train, 96)
     assert T.shape == (48, 96) and np.all(T >= -1e-9)
+    assert L.shape == (48, 96, S.N_PROBES) and np.all(np.isfinite(L)) and np.all(L > 0)
     sur = S.Surrogate(seed=0)
     try:
-        hist = sur.fit(train, e_train, T, steps=(800, 200), lr=(1e-3, 2e-4), batch=2048)
+        hist = sur.fit(train, e_train, T, L, steps=(800, 200), lr=(1e-3, 2e-4), batch=2048)
         assert np.all(np.isfinite(hist)) and hist[-50:].mean() < 0.2 * hist[:50].mean()
         test = S.sample_devices(2, seed=99, nz=60)
+        lp = sur.predict_ldos(test[0].desc, e_train)
+        assert lp.shape == (96, S.N_PROBES) and np.all(np.isfinite(lp)) and np.all(lp >= 0)
         rows = S.compare(sur, test, tol=1e-4)
         for d in test:
             rgf = S.RGF(d)
