@@ -90,6 +90,11 @@ int negf_kmesh(int32_t nkx, int32_t nky, double lx, double ly, double *out);
  * reference).  Errors if 2*ngx > Nx or 2*ngy > Ny (grid.f90:33-37). */
 int negf_vhat(const double *vreal, int32_t Nx, int32_t Ny, int32_t Nz, int32_t ngx, int32_t ngy,
               double *vhat);
+/* negf_vhat on GPU `device` (one CTA per slice, the same separable sums and
+ * twiddles): same arguments and result up to rounding; host pointers, blocks
+ * until done.  For set-ups over many potentials (a batch of devices). */
+int negf_vhat_gpu(const double *vreal, int32_t Nx, int32_t Ny, int32_t Nz, int32_t ngx, int32_t ngy,
+                  int32_t device, double *vhat);
 
 /* -------------------------------------------------------------- context */
 

@@ -445,6 +445,59 @@ size_t ptor_smem(int mx, int my, int Nx, int Ny) {
 
 // LDOS_grid_converter (tools.f90:18-40) applied to one energy's real-space
 // diagonal: LDOS(ii,jj,kk) += Im(diag(i,j,k)) * scale * factors (main.f90:510-526).
+// LocalPotential_RealToPlanewave + the truncated copy of main.f90:239-247 on
+// the GPU, one CTA per slice: V_hat(i,j) = (1/(Nx Ny)) sum_xy V(x,y)
+// e^{-2 pi i (x i/Nx + y j/Ny)} on the window |i| <= ngx/2, |j| <= ngy/2 (zero
+// elsewhere), as the separable transform of negf_vhat: the slice in shared
+// memory, the x transform for i >= 0, the y transform, and V_hat(i,j) =
+// conj(V_hat(-i,-j)) for i < 0 (grid.f90:64-68).  tx, ty: e^{-2 pi i m/N}.
+constexpr int VH_THREADS = 256;
+__global__ void __launch_bounds__(VH_THREADS)
+    k_vhat(const double *__restrict__ vreal, int Nx, int Ny, int ngx, int ngy, const double2 *__restrict__ tx,
+           const double2 *__restrict__ ty, double2 *__restrict__ vhat) {
+    extern __shared__ __align__(16) unsigned char vsm[];
+    const int W = 2 * ngx + 1, H = 2 * ngy + 1, hx = ngx / 2, hy = ngy / 2;
+    double *v = (double *)vsm;                           // [Ny][Nx]
+    double2 *X = (double2 *)(v + (size_t)Nx * Ny);        // [Ny][hx + 1]
+    const double *src = vreal + (size_t)Nx * Ny * blockIdx.x;
+    for (int e = threadIdx.x; e < Nx * Ny; e += VH_THREADS) v[e] = src[e];
+    __syncthreads();
+    for (int e = threadIdx.x; e < (hx + 1) * Ny; e += VH_THREADS) {
+        const int i = e % (hx + 1), y = e / (hx + 1);
+        double2 acc = make_double2(0.0, 0.0);
+        int m = 0;  // (x * i) mod Nx
+        for (int x = 0; x < Nx; ++x) {
+            const double a = v[x + Nx * y];
+            const double2 t = tx[m];
+            acc.x += a * t.x;
+            acc.y += a * t.y;
+            m += i;
+            if (m >= Nx) m -= Nx;
+        }
+        X[e] = acc;
+    }
+    __syncthreads();
+    double2 *o = vhat + (size_t)W * H * blockIdx.x;
+    const double inv = 1.0 / ((double)Nx * Ny);
+    for (int e = threadIdx.x; e < W * H; e += VH_THREADS) {
+        const int ii = e % W - ngx, jj = e / W - ngy;
+        double2 r = make_double2(0.0, 0.0);
+        if (ii >= -hx && ii <= hx && jj >= -hy && jj <= hy) {
+            const int i = ii >= 0 ? ii : -ii, j = ii >= 0 ? jj : -jj;
+            const int step = ((j % Ny) + Ny) % Ny;
+            double2 acc = make_double2(0.0, 0.0);
+            int m = 0;  // (y * j) mod Ny
+            for (int y = 0; y < Ny; ++y) {
+                acc = zfma(X[i + (hx + 1) * y], ty[m], acc);
+                m += step;
+                if (m >= Ny) m -= Ny;
+            }
+            r = make_double2(acc.x * inv, ii >= 0 ? acc.y * inv : -(acc.y * inv));
+        }
+        o[e] = r;
+    }
+}
+
 __global__ void k_ldos_convert(const double2 *__restrict__ diag, int Nx, int Ny, int Nz, int gx, int gy,
                                int gz, double dx, double dy, double dz, double scale, int Mx, int My,
                                double *__restrict__ out) {
@@ -1345,6 +1398,47 @@ extern "C" int negf_density_real(negf_ctx *c, int32_t n_circle, int32_t n_line, 
     cudaFree(d_G);
     cudaFree(d_dens);
     return rc ? rc : info;
+}
+
+extern "C" int negf_vhat_gpu(const double *vreal, int32_t Nx, int32_t Ny, int32_t Nz, int32_t ngx, int32_t ngy,
+                             int32_t device, double *vhat) {
+    if (!vreal || !vhat || Nx < 1 || Ny < 1 || Nz < 1 || ngx < 0 || ngy < 0) return NEGF_ERR_ARG;
+    if (2 * ngx > Nx || 2 * ngy > Ny) return NEGF_ERR_ARG;  // grid.f90:33-37
+    if (cudaSetDevice(device) != cudaSuccess) return NEGF_ERR_CUDA;
+    const int W = 2 * ngx + 1, H = 2 * ngy + 1, hx = ngx / 2;
+    const size_t smem = sizeof(double) * (size_t)Nx * Ny + sizeof(double2) * (size_t)(hx + 1) * Ny;
+    if (smem > 200 * 1024) return NEGF_ERR_UNSUPPORTED;
+    std::vector<double2> tx(Nx), ty(Ny);  // e^{-2 pi i m/N}, as the host transform
+    for (int m = 0; m < Nx; ++m) { const double a = -2.0 * PI * (double)m / Nx; tx[m] = make_double2(std::cos(a), std::sin(a)); }
+    for (int m = 0; m < Ny; ++m) { const double a = -2.0 * PI * (double)m / Ny; ty[m] = make_double2(std::cos(a), std::sin(a)); }
+    const size_t nv = (size_t)Nx * Ny * Nz, nh = (size_t)W * H * Nz;
+    double *d_v = nullptr;
+    double2 *d_t = nullptr, *d_h = nullptr;
+    cudaStream_t st = nullptr;
+    int rc = 0;
+    if (cudaMalloc(&d_v, sizeof(double) * nv) != cudaSuccess || cudaMalloc(&d_t, sizeof(double2) * (Nx + Ny)) != cudaSuccess ||
+        cudaMalloc(&d_h, sizeof(double2) * nh) != cudaSuccess) {
+        cudaGetLastError();
+        rc = NEGF_ERR_NOMEM;
+    }
+    if (!rc && cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) rc = NEGF_ERR_CUDA;
+    if (!rc && (cudaMemcpyAsync(d_v, vreal, sizeof(double) * nv, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+                cudaMemcpyAsync(d_t, tx.data(), sizeof(double2) * Nx, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+                cudaMemcpyAsync(d_t + Nx, ty.data(), sizeof(double2) * Ny, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+                cudaFuncSetAttribute(k_vhat, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess))
+        rc = NEGF_ERR_CUDA;
+    if (!rc) {
+        k_vhat<<<Nz, VH_THREADS, smem, st>>>(d_v, Nx, Ny, ngx, ngy, d_t, d_t + Nx, d_h);
+        if (cudaGetLastError() != cudaSuccess ||
+            cudaMemcpyAsync(vhat, d_h, sizeof(double2) * nh, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            rc = NEGF_ERR_CUDA;
+    }
+    if (st) cudaStreamDestroy(st);
+    cudaFree(d_v);
+    cudaFree(d_t);
+    cudaFree(d_h);
+    return rc;
 }
 
 extern "C" int negf_dm_real(negf_ctx *c, const double *dm, int32_t Nx, int32_t Ny, double scale,

@@ -51,6 +51,16 @@ def V_reciprocal_all(V_real, NGX, NGY):
     return out
 
 
+def V_reciprocal_all_gpu(V_real, NGX, NGY, device=0):
+    """V_reciprocal_all computed on GPU `device` (negf_vhat_gpu): same table up to rounding."""
+    v = np.asfortranarray(V_real, dtype=np.float64)
+    Nx, Ny, Nz = v.shape
+    out = np.zeros((2 * NGX + 1, 2 * NGY + 1, Nz), np.complex128, order="F")
+    check("negf_vhat_gpu", lib().negf_vhat_gpu(v.ctypes.data_as(_dp), Nx, Ny, Nz, NGX, NGY, device,
+                                               out.ctypes.data_as(_dp)))
+    return out
+
+
 def Greensfunction_PlanewaveToReal(subGreenFunc, nx_grid, ny_grid, N_x, N_y):
     """grid.f90:71-135 for one or more slices: (N,N[,Nz]) -> (N_x,N_y[,Nz]) complex."""
     g = np.asfortranarray(subGreenFunc, dtype=np.complex128)

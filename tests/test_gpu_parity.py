@@ -339,3 +339,19 @@ def test_every_variant_and_the_autotuner(oracle):
         tau, _ = eng.transmission(E)
         np.testing.assert_allclose(tau, tau_ref, rtol=RTOL, atol=1e-12)
         eng.set_variant(-1)
+
+
+@pytest.mark.parametrize("grid,ng,nz", [(64, 9, 5), (64, 17, 3), (128, 34, 2), (32, 3, 4)])
+@pytest.mark.gpu
+def test_vhat_gpu_matches_host(grid, ng, nz):
+    """The V table computed on the GPU against the host transform (and its
+    conjugate symmetry and zero window) on a seeded disordered QPC."""
+    from negftrans_b200.grid import V_reciprocal_all, V_reciprocal_all_gpu
+    V = W.MSTAR * W.qpc_potential(grid, grid, nz, 100.0, nz * 1.0, 0.05, 15.0, 1.0, disorder=0.002) / HARTREE
+    ref = V_reciprocal_all(V, ng, ng)
+    got = V_reciprocal_all_gpu(V, ng, ng)
+    assert np.max(np.abs(got - ref)) <= 1e-13 * np.max(np.abs(ref))
+    h = ng // 2
+    assert np.all(got[: ng - h] == 0) and np.all(got[ng + h + 1:] == 0)
+    np.testing.assert_allclose(got[ng - h:ng + h + 1, ng - h:ng + h + 1][::-1, ::-1],
+                               np.conj(got[ng - h:ng + h + 1, ng - h:ng + h + 1]), rtol=0, atol=1e-14 * np.max(np.abs(ref)))
