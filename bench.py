@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--density", action="store_true", help="also time the density contour once")
+    ap.add_argument("--ldos", action="store_true", help="also time one LDOS pass (LDOS_GRID = -1 -1 0)")
     return ap.parse_args()
 
 
@@ -377,6 +378,19 @@ def run_ours(args):
             line["density_neq"] = {"jobs": njn, "circle": nc, "window": 256, "bias_V": 1e-3,
                                    "seconds": el, "jobs_per_s": njn / el,
                                    "device_ms": eng.last_stats.device_ms, "info": info_n}
+    if args.ldos:
+        # LDOS (main.f90:417-554) on B energies of the transmission window, integrated over
+        # x and y (LDOS_GRID = -1 -1 0): D-mode sweeps + PtoR per slice on the GPU
+        a = pr.atomic
+        Nx, Ny, Nz_ = pr.shape
+        e_hi = float(E_all[-1])
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        _, info_l = eng.ldos(0.0, e_hi, B, (-1, -1, 0), Nx, Ny, w.deck.LX, w.deck.LY, w.deck.LZ)
+        el = time.perf_counter() - t0
+        if rank == 0:
+            line["ldos"] = {"jobs": B * nk, "seconds": el, "jobs_per_s": B * nk / el,
+                            "device_ms": eng.last_stats.device_ms, "info": info_l}
     if rank == 0:
         print(json.dumps(line), flush=True)
     eng.close()

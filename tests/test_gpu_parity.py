@@ -355,3 +355,25 @@ def test_vhat_gpu_matches_host(grid, ng, nz):
     assert np.all(got[: ng - h] == 0) and np.all(got[ng + h + 1:] == 0)
     np.testing.assert_allclose(got[ng - h:ng + h + 1, ng - h:ng + h + 1][::-1, ::-1],
                                np.conj(got[ng - h:ng + h + 1, ng - h:ng + h + 1]), rtol=0, atol=1e-14 * np.max(np.abs(ref)))
+
+
+@pytest.mark.gpu
+def test_transmission_near_the_maximum_basis(oracle):
+    """N = 997 (the largest variant holds N <= 1024), two slices; and N = 1041
+    is refused with NEGF_ERR_UNSUPPORTED rather than run."""
+    from negftrans_b200._lib import NEGF_ERR_UNSUPPORTED, NegfError
+    nz = 2
+    V = W.MSTAR * W.qpc_potential(128, 128, nz, 100.0, nz * 1.0, 0.050, 15.0, 1.0, disorder=0.002)
+    pr = P.prepare(W._deck(nz * 10.0, 0.048, 30.0, 16), V)
+    assert pr.N == 997
+    E = P.transmission_energies(pr.atomic, 16)[::5]
+    tau_ref, _ = oracle.transmission_jobs(oracle_problem(oracle, pr), E, nthreads=8)
+    with Engine(*pr.engine_args()) as eng:
+        tau, info = eng.transmission(E)
+    assert info == 0
+    np.testing.assert_allclose(tau, tau_ref, rtol=RTOL, atol=1e-12)
+    big = P.prepare(W._deck(nz * 10.0, 0.05, 30.0, 16), V)
+    assert big.N == 1041
+    with pytest.raises(NegfError) as exc:
+        Engine(*big.engine_args())
+    assert exc.value.code == NEGF_ERR_UNSUPPORTED
