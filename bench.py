@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--batch", type=int, default=296, help="energies per step and GPU")
     ap.add_argument("--nz", type=int, default=0,
                     help="profiling only: rebuild the workload with this many slices (same dz)")
-    ap.add_argument("--cpu-threads", type=int, default=0, help="0 = all host cores (max 16)")
+    ap.add_argument("--cpu-threads", type=int, default=0, help="0 = all host cores (as many as host memory holds)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--density", action="store_true", help="also time the density contour once")
@@ -53,9 +53,26 @@ def parse():
     return ap.parse_args()
 
 
-def host_threads(req):
+def host_threads(req, per_job_bytes=0):
+    """Host threads for the CPU arm: all cores (or --cpu-threads), fewer only if
+    that many concurrent jobs (per_job_bytes each) would not fit in 60 % of the
+    available host memory."""
     n = os.cpu_count() or 1
-    return max(1, min(req or n, 16, n))
+    t = min(req or n, n)
+    if per_job_bytes:
+        try:
+            import psutil
+            avail = psutil.virtual_memory().available
+            t = min(t, max(1, int(0.6 * avail // per_job_bytes)))
+        except Exception:
+            pass
+    return max(1, t)
+
+
+def oracle_job_bytes(pr):
+    """Peak memory of one oracle F-mode job: H, D, first column and generator_r
+    (four N x N x N_z complex arrays)."""
+    return 4 * 16 * pr.N * pr.N * pr.Nz
 
 
 def flops_per_solve(N, Nz):
@@ -182,7 +199,7 @@ def run_reference(args):
     w = W.config(args.workload)
     pr = P.prepare(w.deck, w.V_eV)
     E = P.transmission_energies(pr.atomic, w.n_energy)
-    nth = host_threads(args.cpu_threads)
+    nth = host_threads(args.cpu_threads, oracle_job_bytes(pr))
     for _ in range(args.warmup):
         cpu_rate(pr, E, nth)
     times = []
@@ -346,7 +363,7 @@ def run_ours(args):
             line["e2e_matches_device"] = bool(np.allclose(tau_h, tau_dev, rtol=1e-12, atol=1e-14))
 
     if rank == 0 and not args.no_cpu_baseline and world == 1:
-        nth = host_threads(args.cpu_threads)
+        nth = host_threads(args.cpu_threads, oracle_job_bytes(pr))
         r, t = cpu_rate(pr, E_all[::7], nth)
         line["cpu_baseline"] = {"value": r, "unit": UNIT, "cores": nth, "kind": "port",
                                 "sample": f"{nth} sweeps of this workload, one per thread, {t[0]:.1f} s"}
