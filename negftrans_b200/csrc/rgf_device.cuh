@@ -166,7 +166,7 @@ template <int NB>
 __host__ __device__ inline size_t smem_bytes(int N) {
     int ldw = round_up(N, CM);
     size_t big = (size_t)NB * ldw + (size_t)NB * NB;         // sub-panel a + 16x16 block
-    size_t trail = 2 * (size_t)NB * (BP + AP);               // gathered rows + W tile
+    size_t trail = 32 * (size_t)(BP + AP);                    // rank-32 update: gathered rows + W tile
     size_t gemm = 2 * (size_t)KC * (AP + BP);
     if (trail > big) big = trail;
     if (gemm > big) big = gemm;
@@ -712,7 +712,7 @@ __device__ inline void factor_subpanel(double2 (&w)[RPT][NB], int kb, int nbe, u
 // A(prow[r], iprow[c])).  Returns the LAPACK-style info (1-based column of
 // the first zero pivot, 0 if none); identical in every thread.
 template <int NB, int RPT>
-__device__ int gj_invert(double2 *__restrict__ A, int N, int ld, const Smem &s) {
+__device__ int gj_invert_pair(double2 *__restrict__ A, int N, int ld, const Smem &s) {
     const int tid = threadIdx.x;
     const int ldw = s.ldw;
     int info = 0;
@@ -820,6 +820,107 @@ __device__ int gj_invert(double2 *__restrict__ A, int N, int ld, const Smem &s) 
     for (int k = tid; k < N; k += NT) s.iprow[s.prow[k]] = k;
     __syncthreads();
     return info;
+}
+
+// The same inverse with panels of P sub-panels of NB columns each (one
+// rank-P*NB trailing update per panel) for blocks whose sub-panels do not fit
+// the shared-memory buffer of gj_invert_pair: the finished sub-panels stay in
+// A.  Per sub-panel p: (i) bring its columns up to date with sub-panels < p,
+// b = mask_{<p}(b) + W_{<p} b(P_{<p}); (ii) eliminate it in registers; (iii)
+// apply its steps to the earlier columns, W_{<p} = mask_p(W_{<p}) +
+// W_p W_{<p}(P_p); the trailing update then applies the whole panel at once,
+// the single-panel formula of trailing_update with W = A(:, panel).
+template <int NB, int RPT, int P>
+__device__ int gj_invert_multi(double2 *__restrict__ A, int N, int ld, const Smem &s) {
+    const int tid = threadIdx.x;
+    const double2 zero = make_double2(0.0, 0.0);
+    int info = 0;
+    unsigned used = 0;
+#pragma unroll
+    for (int r = 0; r < RPT; ++r)
+        if (tid + NT * r >= N) used |= 1u << r;
+    for (int i = tid; i < N; i += NT) s.inP[i] = 0;
+    __syncthreads();
+    double2 *sX = s.big;                // [P*NB][NB]: rows P_{<p} of sub-panel p before (i)
+    double2 *sY = s.big + P * NB * NB;  // [NB][P*NB]: rows P_p of the earlier columns before (iii)
+    for (int k0 = 0; k0 < N; k0 += P * NB) {
+        const int nbt = min(P * NB, N - k0);
+        for (int p = 0; p * NB < nbt; ++p) {
+            const int cp = k0 + p * NB, kprev = p * NB;
+            const int nbp = min(NB, nbt - kprev);
+            if (p > 0) {
+                for (int e = tid; e < kprev * NB; e += NT) {
+                    const int kk = e / NB, c = e % NB;
+                    sX[e] = (c < nbp) ? A[s.prow[k0 + kk] + (size_t)ld * (cp + c)] : zero;
+                }
+                __syncthreads();
+            }
+            double2 w[RPT][NB];
+#pragma unroll
+            for (int r = 0; r < RPT; ++r) {
+                const int i = tid + NT * r;
+                const bool keep = (i < N) && !(s.inP[i] >= 1 && s.inP[i] <= p);
+#pragma unroll
+                for (int c = 0; c < NB; ++c) w[r][c] = (keep && c < nbp) ? A[i + (size_t)ld * (cp + c)] : zero;
+                if (i < N) {
+#pragma unroll 1
+                    for (int kk = 0; kk < kprev; ++kk) {
+                        const double2 wa = A[i + (size_t)ld * (k0 + kk)];
+#pragma unroll
+                        for (int c = 0; c < NB; ++c) w[r][c] = zfma(wa, sX[kk * NB + c], w[r][c]);
+                    }
+                }
+            }
+            factor_subpanel<NB, RPT>(w, cp, nbp, used, info, p + 1, s);
+            if (p > 0) {
+                for (int e = tid; e < NB * kprev; e += NT) {
+                    const int c = e / kprev, q = e % kprev;
+                    sY[e] = (c < nbp) ? A[s.prow[cp + c] + (size_t)ld * (k0 + q)] : zero;
+                }
+                __syncthreads();
+#pragma unroll
+                for (int r = 0; r < RPT; ++r) {
+                    const int i = tid + NT * r;
+                    if (i < N) {
+                        const bool keep = s.inP[i] != p + 1;
+#pragma unroll 1
+                        for (int q = 0; q < kprev; ++q) {
+                            double2 v = keep ? A[i + (size_t)ld * (k0 + q)] : zero;
+#pragma unroll
+                            for (int c = 0; c < NB; ++c) v = zfma(w[r][c], sY[c * kprev + q], v);
+                            A[i + (size_t)ld * (k0 + q)] = v;
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < RPT; ++r) {
+                const int i = tid + NT * r;
+                if (i < N) {
+#pragma unroll
+                    for (int c = 0; c < NB; ++c)
+                        if (c < nbp) A[i + (size_t)ld * (cp + c)] = w[r][c];
+                }
+            }
+            __syncthreads();
+        }
+        if (nbt < N) trailing_update<P * NB>(A, N, ld, k0, nbt, s);
+        __syncthreads();
+        if (tid < nbt) s.inP[s.prow[k0 + tid]] = 0;
+        __syncthreads();
+    }
+    for (int k = tid; k < N; k += NT) s.iprow[s.prow[k]] = k;
+    __syncthreads();
+    return info;
+}
+
+// The inverse used by the kernels: 16-column sub-panels in pairs through
+// shared memory; 8-column sub-panels (the large-N variant) four per panel
+// through A, so that every variant applies rank-32 trailing updates.
+template <int NB, int RPT>
+__device__ int gj_invert(double2 *__restrict__ A, int N, int ld, const Smem &s) {
+    if constexpr (NB == 8) return gj_invert_multi<8, RPT, 4>(A, N, ld, s);
+    else return gj_invert_pair<NB, RPT>(A, N, ld, s);
 }
 
 }  // namespace negf
