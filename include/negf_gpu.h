@@ -188,6 +188,14 @@ int negf_transmission_noalloc(int32_t N, int32_t Nz, int32_t ngx, int32_t ngy, c
 int negf_density(negf_ctx *ctx, int32_t n_circle, int32_t n_line, double min_v, double mu,
                  double gap, double temperature, double *dm, negf_stats *stats);
 
+/* The accumulation step of Equilibrium_Density (negf.f90:77-111) for any
+ * contour: dm = sum_k w_k sum_i weights[i] * 2 dz^2 G_kk(energies[i] + i*eta)
+ * for every slice k (w_k the k-point weights).  energies and weights are
+ * complex [nE] (interleaved re, im); dm (N,N,Nz) complex is overwritten.
+ * negf_density is this sum over the reference's Simpson contour. */
+int negf_density_accumulate(negf_ctx *ctx, const double *energies, const double *weights, int32_t nE,
+                            double *dm, negf_stats *stats);
+
 /* Non-equilibrium Density_Matrix under a bias mu_L != mu_R.  No reference
  * counterpart: main.f90:129-132 rejects VDS != 0 and negf.f90:9-113 is
  * equilibrium only.  With mu_lo = min(mu_L, mu_R), mu_hi = max, the lead at

@@ -26,6 +26,7 @@ EXPORTS = (
     "negf_density", "negf_ldos_matrix", "negf_ptor", "negf_version", "negf_transmission_noalloc",
     "negf_density_real", "negf_ldos", "negf_basis_k", "negf_transmission_batch",
     "negf_density_neq", "negf_dm_real", "negf_set_variant", "negf_autotune", "negf_vhat_gpu",
+    "negf_density_accumulate",
 )
 # every symbol include/negf_mlp.h declares
 MLP_EXPORTS = (
@@ -100,6 +101,7 @@ def lib():
                                    C.c_double, C.c_double, _dp, C.POINTER(Stats)]
     L.negf_dm_real.argtypes = [C.c_void_p, _dp, C.c_int32, C.c_int32, C.c_double, _dp]
     L.negf_set_variant.argtypes = [C.c_void_p, C.c_int32]
+    L.negf_density_accumulate.argtypes = [C.c_void_p, _dp, _dp, C.c_int32, _dp, C.POINTER(Stats)]
     L.negf_vhat_gpu.argtypes = [_dp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _dp]
     L.negf_autotune.argtypes = [C.c_void_p, _dp, C.c_int32, _ip, _dp]
     _fp = C.POINTER(C.c_float)

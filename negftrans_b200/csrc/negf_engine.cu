@@ -1041,6 +1041,38 @@ int negf_density(negf_ctx *c, int32_t n_circle, int32_t n_line, double min_v, do
     return first_info(info);
 }
 
+int negf_density_accumulate(negf_ctx *c, const double *energies, const double *weights, int32_t nE, double *dm,
+                            negf_stats *stats) {
+    if (!c || !energies || !weights || !dm || nE < 1) return NEGF_ERR_ARG;
+    if (cudaSetDevice(c->device) != cudaSuccess) return NEGF_ERR_CUDA;
+    const int nk = c->nk;
+    std::vector<RgfJob> jobs((size_t)nE * nk);
+    std::vector<double2> coef((size_t)nE * nk);
+    for (int ik = 0; ik < nk; ++ik) {
+        const double wk = c->kpt[3 * ik + 2];
+        for (int i = 0; i < nE; ++i) {
+            RgfJob jb{};
+            jb.e_re = energies[2 * i];
+            jb.e_im = energies[2 * i + 1] + c->eta;  // + i*eta as negf.f90:77
+            jb.e_t = jb.e_re;
+            jb.ik = ik;
+            jobs[(size_t)ik * nE + i] = jb;
+            coef[(size_t)ik * nE + i] = make_double2(wk * weights[2 * i], wk * weights[2 * i + 1]);
+        }
+    }
+    const size_t per = (size_t)c->N * c->N * c->Nz;
+    double2 *d_out = nullptr;
+    if (cudaMalloc(&d_out, sizeof(double2) * per) != cudaSuccess) { cudaGetLastError(); return NEGF_ERR_NOMEM; }
+    std::vector<int> info;
+    double ms = 0;
+    int rc = diag_accumulate(c, jobs, coef, 0, d_out, info, ms);
+    if (!rc && cudaMemcpy(dm, d_out, sizeof(double2) * per, cudaMemcpyDeviceToHost) != cudaSuccess) rc = NEGF_ERR_CUDA;
+    cudaFree(d_out);
+    if (rc) return rc;
+    fill_stats(stats, info, ms);
+    return first_info(info);
+}
+
 int negf_density_neq(negf_ctx *c, int32_t n_circle, int32_t n_window, double min_v, double mu_L,
                      double mu_R, double gap, double temperature, double *dm, negf_stats *stats) {
     if (!c || !dm || n_circle < 1 || n_window < 1 || !(temperature > 0) || !(gap > 0)) return NEGF_ERR_ARG;

@@ -137,6 +137,20 @@ class Engine:
         self.last_stats = st
         return dens, dm, rc
 
+    def density_accumulate(self, energies, weights):
+        """Density_Matrix of any contour: sum_k w_k sum_i weights[i] 2 dz^2 G_kk(E_i + i eta)
+        (the accumulation of negf.f90:77-111); energies, weights complex (Hartree)."""
+        e = np.ascontiguousarray(energies, np.complex128)
+        w = np.ascontiguousarray(weights, np.complex128)
+        assert e.shape == w.shape and e.ndim == 1
+        dm = np.zeros((self.N, self.N, self.Nz), np.complex128, order="F")
+        st = Stats()
+        rc = check("negf_density_accumulate", lib().negf_density_accumulate(
+            self._ctx, e.ctypes.data_as(_dp), w.ctypes.data_as(_dp), len(e), dm.ctypes.data_as(_dp),
+            C.byref(st)))
+        self.last_stats = st
+        return dm, rc
+
     def density_neq(self, n_circle, n_window, min_V, MU_L, MU_R, GAP, TEMPERATURE):
         """Non-equilibrium Density_Matrix (N, N, N_z) under a bias MU_L != MU_R: a
         Gauss-Legendre semicircle up to min(MU) - GAP plus a real-axis window

@@ -474,3 +474,19 @@ def density_neq(p: Problem, n_circle, n_window, min_v, mu_L, mu_R, gap, temperat
                 term[:, :, k] += ca * (C[:, :, k] * gam[None, :]) @ C[:, :, k].conj().T
         dm += term * (2 * dz * dz)
     return dm, info_all
+
+
+def density_accumulate(p: Problem, energies, weights):
+    """sum_k w_k sum_i weights[i] 2 dz^2 G_kk(E_i + i eta), with G_kk from the
+    restated tri_solver (D mode, math_kernel.f90:94-109): the accumulation of
+    negf.f90:77-111 for an arbitrary contour."""
+    dz = p.Lz / p.Nz
+    dm = np.zeros((p.N, p.N, p.Nz), np.complex128, order="F")
+    info_all = 0
+    for kx, ky, wk in p.kpt:
+        H = hamiltonian(p, kx, ky)
+        for e, w in zip(np.asarray(energies, np.complex128), np.asarray(weights, np.complex128)):
+            outs, info = tri_solver(e_minus_h(p, H, e + 1j * p.eta, kx, ky), "D")
+            info_all = info_all or info
+            dm += (wk * w * 2 * dz * dz) * outs["D"]
+    return dm, info_all

@@ -39,6 +39,7 @@ def test_argument_errors_without_gpu(built_lib):
     assert L.negf_transmission(None, None, 0, 0, None, None) == _lib.NEGF_ERR_ARG
     assert L.negf_density(None, 4, 4, 0.0, 0.0, 0.0, 1.0, None, None) == _lib.NEGF_ERR_ARG
     assert L.negf_set_variant(None, 0) == _lib.NEGF_ERR_ARG
+    assert L.negf_density_accumulate(None, None, None, 0, None, None) == _lib.NEGF_ERR_ARG
     assert L.negf_autotune(None, None, 0, None, None) == _lib.NEGF_ERR_ARG
     assert L.negf_density_neq(None, 4, 4, 0.0, 0.0, 0.0, 1.0, 1.0, None, None) == _lib.NEGF_ERR_ARG
     buf = (C.c_double * 8)()

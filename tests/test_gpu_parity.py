@@ -377,3 +377,37 @@ def test_transmission_near_the_maximum_basis(oracle):
     with pytest.raises(NegfError) as exc:
         Engine(*big.engine_args())
     assert exc.value.code == NEGF_ERR_UNSUPPORTED
+
+
+@pytest.mark.gpu
+def test_density_accumulate_any_contour(oracle):
+    """Arbitrary complex energies and weights against the oracle; and the
+    reference's own Simpson contour through this entry equals negf_density."""
+    pr = small_problem(nz=8, nk=2)
+    a = pr.atomic
+    rng = np.random.default_rng(7)
+    E = a.MU * rng.uniform(0.2, 1.2, 6) + 1j * a.MU * rng.uniform(0.0, 0.5, 6)
+    w = rng.standard_normal(6) + 1j * rng.standard_normal(6)
+    ref, _ = oracle.density_accumulate(oracle_problem(oracle, pr), E, w)
+    with Engine(*pr.engine_args()) as eng:
+        dm, info = eng.density_accumulate(E, w)
+        assert info == 0
+        assert rel_err(dm, ref) < RTOL
+        # negf.f90:37-65 contour and weights restated here (Simpson, n_circle = 6, n_line = 5)
+        n_c, n_l = 6, 5
+        cl, cr = pr.min_V - 1.0 / HARTREE, a.MU - a.GAP
+        Ec, ER = (cr + cl) / 2, (cr - cl) / 2
+        sx = lambda i, n, lo, hi: (i - 1) * (hi - lo) / (n - 1) + lo
+        EE, WW = [], []
+        for i in range(1, n_c + 1):
+            th = sx(i, n_c, 0.0, np.pi)
+            EE.append(Ec + ER * np.exp(1j * th))
+            WW.append(2 / np.pi * oracle.coefficient_simpson(i, n_c, 0.0, np.pi) * 1j * ER * np.exp(1j * th))
+        for i in range(1, n_l + 1):
+            x = sx(i, n_l, a.MU - a.GAP, a.MU + a.GAP)
+            EE.append(x)
+            WW.append(-2 / np.pi * oracle.coefficient_simpson(i, n_l, a.MU - a.GAP, a.MU + a.GAP)
+                      * oracle.fermi_func(x, a.MU, a.TEMPERATURE))
+        dm2, _ = eng.density_accumulate(np.array(EE), np.array(WW))
+        dm_ref, _ = eng.equilibrium_density(n_c, n_l, pr.min_V, a.MU, a.GAP, a.TEMPERATURE)
+        assert rel_err(dm2, dm_ref) < RTOL
