@@ -1089,9 +1089,10 @@ int negf_density_neq(negf_ctx *c, int32_t n_circle, int32_t n_window, double min
     gauss_legendre(n_circle, xc, wc);
     gauss_legendre(n_window, xw, ww);
     auto fermi = [kT](double e, double mu) { return 1.0 / (std::exp((e - mu) / kT) + 1.0); };
-    // One job list (semicircle nodes, then window nodes, per k-point) so that both
-    // kinds share the chunks the device memory allows; every job carries its own
-    // cd (and ca) and k_accumulate sums them with unit weight.
+    // One job list (window nodes, then semicircle nodes, per k-point) so that both
+    // kinds share the chunks the device memory allows and a short last chunk
+    // holds the cheaper semicircle sweeps (no spectral term); every job carries
+    // its own cd (and ca) and k_accumulate sums them with unit weight.
     const int nk = c->nk, per_k = n_circle + n_window;
     std::vector<RgfJob> jobs((size_t)per_k * nk);
     for (int ik = 0; ik < nk; ++ik) {
@@ -1107,7 +1108,7 @@ int negf_density_neq(negf_ctx *c, int32_t n_circle, int32_t n_window, double min
             const double sc = w * 2.0 / PI * cth * E_R;
             jb.cd_re = -sc * std::sin(th);
             jb.cd_im = sc * std::cos(th);
-            jobs[(size_t)ik * per_k + i] = jb;
+            jobs[(size_t)ik * per_k + n_window + i] = jb;
         }
         for (int i = 0; i < n_window; ++i) {
             const double x = (win_L + win_R) / 2 + (win_R - win_L) / 2 * xw[i];
@@ -1120,7 +1121,7 @@ int negf_density_neq(negf_ctx *c, int32_t n_circle, int32_t n_window, double min
             jb.ik = ik;
             jb.cd_re = -(w * 2.0 / PI * cx * flo);
             jb.ca_im = w / PI * cx * (fhi - flo) * (2.0 * dz * dz);
-            jobs[(size_t)ik * per_k + n_circle + i] = jb;
+            jobs[(size_t)ik * per_k + i] = jb;
         }
     }
     const std::vector<double2> unit(jobs.size(), make_double2(1.0, 0.0));
@@ -1390,7 +1391,7 @@ int basis_extent(const negf_ctx *c, int *mx, int *my) {
 }
 
 int launch_ptor(negf_ctx *c, const double2 *d_G, int nslices, int Nx, int Ny, double scale, double *d_dens,
-                double2 *d_cdiag, cudaStream_t st) {
+                double2 *d_cdiag, cudaStream_t st, int ldg = 0, size_t gstride = 0) {
     int mx, my;
     int rc = basis_extent(c, &mx, &my);
     if (rc) return rc;
@@ -1398,8 +1399,8 @@ int launch_ptor(negf_ctx *c, const double2 *d_G, int nslices, int Nx, int Ny, do
     const size_t smem = ptor_smem(mx, my, Nx, Ny);
     if (smem > 200 * 1024) return NEGF_ERR_UNSUPPORTED;
     CK(cudaFuncSetAttribute(k_ptor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_ptor<<<nslices, PT_THREADS, smem, st>>>(d_G, c->N, c->N, (size_t)c->N * c->N, c->d_nx, c->d_ny, mx, my,
-                                              Nx, Ny, scale, d_dens, d_cdiag);
+    k_ptor<<<nslices, PT_THREADS, smem, st>>>(d_G, c->N, ldg ? ldg : c->N, gstride ? gstride : (size_t)c->N * c->N,
+                                              c->d_nx, c->d_ny, mx, my, Nx, Ny, scale, d_dens, d_cdiag);
     CK(cudaGetLastError());
     return 0;
 }
@@ -1493,6 +1494,79 @@ extern "C" int negf_dm_real(negf_ctx *c, const double *dm, int32_t Nx, int32_t N
     return rc;
 }
 
+namespace {
+// negf_ldos with a single k-point: the LDOS_Matrix of an energy is then one
+// job's G_kk times -(w/pi) 2 dz^2, so the slabs go to PtoR directly and no
+// (N,N,Nz) matrix per energy is held: as many energies run at once as the
+// slabs allow.
+int ldos_one_kpoint(negf_ctx *c, double e_lo, double e_hi, int n_e, const int32_t *ldos_grid, int Nx, int Ny,
+                    const double *dxyz, double scale, double *ldos, negf_stats *stats) {
+    const int N = c->N, Nz = c->Nz, ld = c->ld;
+    const int Mx = ldos_grid[0] == 0 ? Nx : 1, My = ldos_grid[1] == 0 ? Ny : 1, Mz = ldos_grid[2] == 0 ? Nz : 1;
+    const size_t nreal = (size_t)Nx * Ny * Nz, nout = (size_t)Mx * My * Mz;
+    const size_t sstride = (size_t)ld * N * Nz;
+    const size_t per_job = sizeof(double2) * (sstride + 6 * (size_t)ld * N + nreal);
+    const int b = slab_jobs_in_flight(c, per_job, n_e);
+    if (b < 1) return NEGF_ERR_NOMEM;
+    double2 *d_slabs = nullptr, *d_diag = nullptr;
+    double *d_out = nullptr;
+    RgfJob *d_jobs = nullptr;
+    int *d_info = nullptr;
+    int rc = 0;
+    if (cudaMalloc(&d_slabs, sizeof(double2) * sstride * b) != cudaSuccess ||
+        cudaMalloc(&d_diag, sizeof(double2) * nreal * b) != cudaSuccess ||
+        cudaMalloc(&d_out, sizeof(double) * nout * n_e) != cudaSuccess ||
+        cudaMalloc(&d_jobs, sizeof(RgfJob) * b) != cudaSuccess || cudaMalloc(&d_info, sizeof(int) * b) != cudaSuccess) {
+        cudaGetLastError();
+        rc = NEGF_ERR_NOMEM;
+    }
+    const double f = -(c->kpt[2] / PI) * 2.0 * (c->Lz / Nz) * (c->Lz / Nz);  // negf.f90:230-231, :78
+    std::vector<int> info_all(n_e, 0);
+    double ms_all = 0;
+    Geo g = make_geo(c);
+    if (!rc && cudaMemsetAsync(d_out, 0, sizeof(double) * nout * n_e, c->stream) != cudaSuccess) rc = NEGF_ERR_CUDA;
+    for (int e0 = 0; e0 < n_e && !rc; e0 += b) {
+        const int nb = std::min(b, n_e - e0);
+        std::vector<RgfJob> jobs(nb);
+        for (int o = 0; o < nb; ++o) {
+            const double e = e_lo + (e_hi - e_lo) * (e0 + o) / n_e;  // negf.f90:203-204
+            RgfJob jb{};
+            jb.e_re = e; jb.e_im = c->eta; jb.e_t = e; jb.ik = 0;
+            jobs[o] = jb;
+        }
+        if (cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(RgfJob) * nb, cudaMemcpyHostToDevice, c->stream) ||
+            cudaEventRecord(c->ev0, c->stream)) { rc = NEGF_ERR_CUDA; break; }
+        if ((rc = slab_launch(c, g, d_jobs, nb, nullptr, d_slabs, sstride, WANT_D, nullptr, nullptr, d_info, c->stream)))
+            break;
+        float ms = 0.f;
+        if (cudaEventRecord(c->ev1, c->stream) ||
+            cudaMemcpyAsync(info_all.data() + e0, d_info, sizeof(int) * nb, cudaMemcpyDeviceToHost, c->stream)) {
+            rc = NEGF_ERR_CUDA;
+            break;
+        }
+        if ((rc = launch_ptor(c, d_slabs, nb * Nz, Nx, Ny, 1.0, nullptr, d_diag, c->stream, ld, (size_t)ld * N)))
+            break;
+        for (int o = 0; o < nb && !rc; ++o) {
+            const int blocks = (int)std::min<size_t>((nreal + 255) / 256, (size_t)c->num_sms * 8);
+            k_ldos_convert<<<blocks, 256, 0, c->stream>>>(d_diag + nreal * o, Nx, Ny, Nz, ldos_grid[0], ldos_grid[1],
+                                                         ldos_grid[2], dxyz[0], dxyz[1], dxyz[2], scale * f, Mx, My,
+                                                         d_out + nout * (e0 + o));
+            if (cudaGetLastError() != cudaSuccess) rc = NEGF_ERR_CUDA;
+        }
+        if (!rc && (cudaStreamSynchronize(c->stream) != cudaSuccess || cudaEventElapsedTime(&ms, c->ev0, c->ev1)))
+            rc = NEGF_ERR_CUDA;
+        ms_all += ms;
+    }
+    if (!rc && (cudaMemcpyAsync(ldos, d_out, sizeof(double) * nout * n_e, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+                cudaStreamSynchronize(c->stream) != cudaSuccess))
+        rc = NEGF_ERR_CUDA;
+    cudaFree(d_slabs); cudaFree(d_diag); cudaFree(d_out); cudaFree(d_jobs); cudaFree(d_info);
+    if (rc) return rc;
+    fill_stats(stats, info_all, ms_all);
+    return first_info(info_all);
+}
+}  // namespace
+
 extern "C" int negf_ldos(negf_ctx *c, double e_lo, double e_hi, int32_t n_e, const int32_t *ldos_grid,
                          int32_t Nx, int32_t Ny, const double *dxyz, double scale, double *ldos,
                          negf_stats *stats) {
@@ -1503,6 +1577,7 @@ extern "C" int negf_ldos(negf_ctx *c, double e_lo, double e_hi, int32_t n_e, con
     const int Nz = c->Nz, nk = c->nk;
     const int Mx = ldos_grid[0] == 0 ? Nx : 1, My = ldos_grid[1] == 0 ? Ny : 1, Mz = ldos_grid[2] == 0 ? Nz : 1;
     const size_t per = (size_t)c->N * c->N * Nz, nreal = (size_t)Nx * Ny * Nz, nout = (size_t)Mx * My * Mz;
+    if (nk == 1) return ldos_one_kpoint(c, e_lo, e_hi, n_e, ldos_grid, Nx, Ny, dxyz, scale, ldos, stats);
     // energies per chunk: LDOS matrices and their real-space diagonals resident at once
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
