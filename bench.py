@@ -31,7 +31,7 @@ sys.path.insert(0, ROOT)
 METRIC = "RGF energy-point solves/s"
 # ncu dram bytes (read + write) of k_transmission per job-slice at N = 221, measured on a
 # 296-job, 16-slice launch (same per-slice work as the full workload)
-TRAFFIC_PER_JOB_SLICE_N221 = 66.170e9 / (296 * 16)
+TRAFFIC_PER_JOB_SLICE_N221 = 67.088e9 / (296 * 16)
 UNIT = "solves/s"
 
 
@@ -326,7 +326,7 @@ def run_ours(args):
                          "peak_source": "measured in-run: cuBLAS FP64 GEMM 8192^3 (MEASURED_PEAKS.json "
                                         "has no FP64 figure)",
                          "flops_per_launch": fl,
-                         "kernel": ("k_transmission<16,1,2>" if N <= 256 else
+                         "kernel": ("k_transmission<8,1,2>" if N <= 256 else
                                     "k_transmission<16,2,1>" if N <= 512 else "k_transmission<8,4,1>"),
                          "flops_note": "executed: 8N^3 per inverse + 8 n_open N^2 per chain product "
                                        "(rows of G_{Nz,1} with gamma_L != 0); the reference's "

@@ -137,13 +137,14 @@ int negf_transmission_batch(negf_ctx *const *ctxs, int32_t nctx, const double *e
 /* Transmission kernel variants (no reference counterpart: the reference has
  * one LAPACK path, math_kernel.f90:8-42): panel width x rows per thread x
  * CTAs per SM, 0 = 16 x 1 x 2 (N <= 256), 1 = 16 x 2 x 1 (N <= 512),
- * 2 = 8 x 4 x 1 (N <= 1024).  By default the variant follows N.
+ * 2 = 8 x 4 x 1 (N <= 1024), 3 = 8 x 1 x 2 (N <= 256).  By default the
+ * variant follows N: 3 up to 256, then 1, then 2.
  * negf_set_variant forces one for this context's negf_transmission[_device]
  * and negf_transmission_batch calls (-1 = back to the default;
  * NEGF_ERR_UNSUPPORTED if it cannot hold N).  negf_autotune times every
  * variant that can hold N on negf_transmission(energies) (each run twice, the
  * second timed), keeps the fastest for this context, returns it in *chosen and
- * the rates (solves/s; 0 for variants that cannot hold N) in rates[3]
+ * the rates (solves/s; 0 for variants that cannot hold N) in rates[4]
  * (optional).  Results are identical across variants up to rounding. */
 int negf_set_variant(negf_ctx *ctx, int32_t variant);
 int negf_autotune(negf_ctx *ctx, const double *energies, int32_t nE, int32_t *chosen, double *rates);

@@ -594,7 +594,7 @@ int ensure_jobs(negf_ctx *c, int nE, int njobs) {
 
 // Kernel variants by basis size: (panel width NB, rows per thread RPT,
 // CTAs per SM).  Up to 256 plane waves two CTAs share an SM.
-enum Variant { V16x1 = 0, V16x2 = 1, V8x4 = 2, VNONE = 3 };
+enum Variant { V16x1 = 0, V16x2 = 1, V8x4 = 2, V8x1 = 3, VNONE = 4 };
 Variant pick_variant(int N) {
     if (N <= NT) return V16x1;
     if (N <= 2 * NT) return V16x2;
@@ -602,16 +602,22 @@ Variant pick_variant(int N) {
     return VNONE;
 }
 bool variant_fits(int v, int N) {
-    return (v == V16x1 && N <= NT) || (v == V16x2 && N <= 2 * NT) || (v == V8x4 && N <= 4 * NT);
+    return (v == V16x1 && N <= NT) || (v == V16x2 && N <= 2 * NT) || (v == V8x4 && N <= 4 * NT) ||
+           (v == V8x1 && N <= NT);
 }
+// Default transmission variant: up to 256 plane waves the 8-column panels in
+// fours (8 x 1 x 2; at N = 69 6836 vs 5827 solves/s for 16 x 1 x 2, equal at
+// N = 221); the slab kernels keep pick_variant.
+Variant transmission_variant(int N) { return N <= NT ? V8x1 : pick_variant(N); }
 Variant ctx_variant(const negf_ctx *c) {
-    return (c->variant >= 0 && variant_fits(c->variant, c->N)) ? (Variant)c->variant : pick_variant(c->N);
+    return (c->variant >= 0 && variant_fits(c->variant, c->N)) ? (Variant)c->variant : transmission_variant(c->N);
 }
 size_t variant_smem(Variant v, int N) {
     switch (v) {
         case V16x1: return smem_bytes<16>(N);
         case V16x2: return smem_bytes<16>(N);
         case V8x4: return smem_bytes<8>(N);
+        case V8x1: return smem_bytes<8>(N);
         default: return 0;
     }
 }
@@ -649,6 +655,7 @@ int transmission_launch(negf_ctx *c, const double *d_E, int nE, double *d_tau, d
     switch (v) {
         case V16x1: rc = prep_kernel(k_transmission<16, 1, 2>, smem, &occ); break;
         case V16x2: rc = prep_kernel(k_transmission<16, 2, 1>, smem, &occ); break;
+        case V8x1: rc = prep_kernel(k_transmission<8, 1, 2>, smem, &occ); break;
         default: rc = prep_kernel(k_transmission<8, 4, 1>, smem, &occ); break;
     }
     if (rc) return rc;
@@ -664,6 +671,9 @@ int transmission_launch(negf_ctx *c, const double *d_E, int nE, double *d_tau, d
             break;
         case V16x2:
             k_transmission<16, 2, 1><<<grid, NT, smem, st>>>(g, d_E, nE, njobs, ws, wstride, d_tau_jobs, d_info);
+            break;
+        case V8x1:
+            k_transmission<8, 1, 2><<<grid, NT, smem, st>>>(g, d_E, nE, njobs, ws, wstride, d_tau_jobs, d_info);
             break;
         default:
             k_transmission<8, 4, 1><<<grid, NT, smem, st>>>(g, d_E, nE, njobs, ws, wstride, d_tau_jobs, d_info);
@@ -947,7 +957,7 @@ int negf_transmission(negf_ctx *c, const double *energies, int32_t nE, int32_t p
 }
 
 int negf_set_variant(negf_ctx *c, int32_t variant) {
-    if (!c || variant < -1 || variant > V8x4) return NEGF_ERR_ARG;
+    if (!c || variant < -1 || variant > V8x1) return NEGF_ERR_ARG;
     if (variant >= 0 && !variant_fits(variant, c->N)) return NEGF_ERR_UNSUPPORTED;
     c->variant = variant;
     return NEGF_OK;
@@ -959,7 +969,7 @@ int negf_autotune(negf_ctx *c, const double *energies, int32_t nE, int32_t *chos
     double best = -1.0;
     int bv = -1;
     const int keep = c->variant;
-    for (int v = V16x1; v <= V8x4; ++v) {
+    for (int v = V16x1; v <= V8x1; ++v) {
         if (rates) rates[v] = 0.0;
         if (!variant_fits(v, c->N)) continue;
         c->variant = v;
@@ -1276,7 +1286,7 @@ extern "C" int negf_transmission_batch(negf_ctx *const *ctxs, int32_t nctx, cons
     std::vector<int> info_all;
     double ms_all = 0;
     int rc = 0;
-    for (int v = V16x1; v <= V8x4 && !rc; ++v) {
+    for (int v = V16x1; v <= V8x1 && !rc; ++v) {
         std::vector<int> members;
         for (int p = 0; p < nctx; ++p)
             if (ctx_variant(ctxs[p]) == v) members.push_back(p);
@@ -1307,6 +1317,7 @@ extern "C" int negf_transmission_batch(negf_ctx *const *ctxs, int32_t nctx, cons
         int occ = 1;
         switch (var) {
             case V16x1: rc = prep_kernel(k_transmission_batch<16, 1, 2>, smem, &occ); break;
+            case V8x1: rc = prep_kernel(k_transmission_batch<8, 1, 2>, smem, &occ); break;
             case V16x2: rc = prep_kernel(k_transmission_batch<16, 2, 1>, smem, &occ); break;
             default: rc = prep_kernel(k_transmission_batch<8, 4, 1>, smem, &occ); break;
         }
@@ -1343,6 +1354,9 @@ extern "C" int negf_transmission_batch(negf_ctx *const *ctxs, int32_t nctx, cons
                     break;
                 case V16x2:
                     k_transmission_batch<16, 2, 1><<<grid, NT, smem, st>>>(d_geo, d_jobs, njobs, d_E, ws, wstride, d_tj, d_info, d_counter);
+                    break;
+                case V8x1:
+                    k_transmission_batch<8, 1, 2><<<grid, NT, smem, st>>>(d_geo, d_jobs, njobs, d_E, ws, wstride, d_tj, d_info, d_counter);
                     break;
                 default:
                     k_transmission_batch<8, 4, 1><<<grid, NT, smem, st>>>(d_geo, d_jobs, njobs, d_E, ws, wstride, d_tj, d_info, d_counter);

@@ -93,15 +93,15 @@ class Engine:
         return tau, rc
 
     def set_variant(self, variant):
-        """Force the transmission kernel variant (0, 1, 2; -1 = chosen by N)."""
+        """Force the transmission kernel variant (0, 1, 2, 3; -1 = chosen by N)."""
         check("negf_set_variant", lib().negf_set_variant(self._ctx, int(variant)))
 
     def autotune(self, energies):
         """Time every variant that holds N on these energies and keep the fastest;
-        returns (variant, rates[3] in solves/s)."""
+        returns (variant, rates[4] in solves/s)."""
         e = np.ascontiguousarray(energies, np.float64)
         v = C.c_int32(-1)
-        rates = np.zeros(3)
+        rates = np.zeros(4)
         check("negf_autotune", lib().negf_autotune(self._ctx, e.ctypes.data_as(_dp), len(e), C.byref(v),
                                                    rates.ctypes.data_as(_dp)))
         return v.value, rates

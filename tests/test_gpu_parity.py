@@ -329,13 +329,13 @@ def test_every_variant_and_the_autotuner(oracle):
     E = P.transmission_energies(pr.atomic, 16)[::2]
     tau_ref, _ = oracle.transmission_jobs(oracle_problem(oracle, pr), E, nthreads=4)
     with Engine(*pr.engine_args()) as eng:
-        for v in (0, 1, 2):
+        for v in (0, 1, 2, 3):
             eng.set_variant(v)
             tau, info = eng.transmission(E)
             assert info == 0
             np.testing.assert_allclose(tau, tau_ref, rtol=RTOL, atol=1e-12)
         v, rates = eng.autotune(E)
-        assert v in (0, 1, 2) and rates[v] == rates.max() > 0
+        assert v in (0, 1, 2, 3) and rates[v] == rates.max() > 0
         tau, _ = eng.transmission(E)
         np.testing.assert_allclose(tau, tau_ref, rtol=RTOL, atol=1e-12)
         eng.set_variant(-1)
