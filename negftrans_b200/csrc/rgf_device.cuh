@@ -863,11 +863,16 @@ __device__ int gj_invert_multi(double2 *__restrict__ A, int N, int ld, const Sme
 #pragma unroll
                 for (int c = 0; c < NB; ++c) w[r][c] = (keep && c < nbp) ? A[i + (size_t)ld * (cp + c)] : zero;
                 if (i < N) {
+                    // kprev is a multiple of NB: NB loads of the row in flight per group
 #pragma unroll 1
-                    for (int kk = 0; kk < kprev; ++kk) {
-                        const double2 wa = A[i + (size_t)ld * (k0 + kk)];
+                    for (int kk0 = 0; kk0 < kprev; kk0 += NB) {
+                        double2 wa[NB];
 #pragma unroll
-                        for (int c = 0; c < NB; ++c) w[r][c] = zfma(wa, sX[kk * NB + c], w[r][c]);
+                        for (int u = 0; u < NB; ++u) wa[u] = A[i + (size_t)ld * (k0 + kk0 + u)];
+#pragma unroll
+                        for (int u = 0; u < NB; ++u)
+#pragma unroll
+                            for (int c = 0; c < NB; ++c) w[r][c] = zfma(wa[u], sX[(kk0 + u) * NB + c], w[r][c]);
                     }
                 }
             }
@@ -884,11 +889,16 @@ __device__ int gj_invert_multi(double2 *__restrict__ A, int N, int ld, const Sme
                     if (i < N) {
                         const bool keep = s.inP[i] != p + 1;
 #pragma unroll 1
-                        for (int q = 0; q < kprev; ++q) {
-                            double2 v = keep ? A[i + (size_t)ld * (k0 + q)] : zero;
+                        for (int q0 = 0; q0 < kprev; q0 += NB) {
+                            double2 v[NB];
 #pragma unroll
-                            for (int c = 0; c < NB; ++c) v = zfma(w[r][c], sY[c * kprev + q], v);
-                            A[i + (size_t)ld * (k0 + q)] = v;
+                            for (int u = 0; u < NB; ++u) v[u] = keep ? A[i + (size_t)ld * (k0 + q0 + u)] : zero;
+#pragma unroll
+                            for (int u = 0; u < NB; ++u) {
+#pragma unroll
+                                for (int c = 0; c < NB; ++c) v[u] = zfma(w[r][c], sY[c * kprev + q0 + u], v[u]);
+                                A[i + (size_t)ld * (k0 + q0 + u)] = v[u];
+                            }
                         }
                     }
                 }
