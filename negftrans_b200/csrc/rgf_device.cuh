@@ -508,14 +508,25 @@ __device__ inline void trailing_update(double2 *__restrict__ A, int N, int ld, i
     double2 *sB = s.big;               // [KMAX][BP] pivot rows of the column tile
     double2 *sW = s.big + KMAX * BP;   // [KMAX][AP] rows I0.. of the panel
     for (int J0 = 0; J0 < nrest; J0 += CN) {
-        for (int e = tid; e < KMAX * CN; e += NT) {
-            const int kk = e / CN, jt = e % CN, jr = J0 + jt;
-            double2 v = make_double2(0.0, 0.0);
-            if (kk < nbt && jr < nrest) {
-                const int j = jr < k0 ? jr : jr + nbt;
-                v = A[s.prow[k0 + kk] + (size_t)ld * j];
+        // all of a thread's gathers issued before any is stored (loads in flight)
+        {
+            constexpr int Q = (KMAX * CN) / NT;
+            double2 v[Q];
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                const int e = tid + NT * q;
+                const int kk = e / CN, jt = e % CN, jr = J0 + jt;
+                v[q] = make_double2(0.0, 0.0);
+                if (kk < nbt && jr < nrest) {
+                    const int j = jr < k0 ? jr : jr + nbt;
+                    v[q] = A[s.prow[k0 + kk] + (size_t)ld * j];
+                }
             }
-            sB[kk * BP + jt] = v;
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                const int e = tid + NT * q;
+                sB[(e / CN) * BP + e % CN] = v[q];
+            }
         }
         int col[2][2];
         bool cv[2][2];
