@@ -499,7 +499,7 @@ __device__ inline double block_sum(double v, const Smem &s) {
 // steps on the other columns, so one pass over the matrix applies KMAX
 // elimination steps.  W tiles are staged from global memory with cp.async;
 // W and the gathered pivot rows feed DMMA warp tiles.
-template <int KMAX>
+template <int KMAX, bool PREFETCH = false>
 __device__ inline void trailing_update(double2 *__restrict__ A, int N, int ld, int k0, int nbt,
                                        const Smem &s) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -547,6 +547,20 @@ __device__ inline void trailing_update(double2 *__restrict__ A, int N, int ld, i
                 cp_async16(sW + kk * AP + r, A + (v ? (i + (size_t)ld * (k0 + kk)) : 0), v);
             }
             cp_async_commit();
+            // large blocks (one CTA per SM): start the warp's C tile on its way
+            // from DRAM into L2 while W arrives (slower for the 2-CTA variants)
+            if (PREFETCH && (I0 + wm0 < N) && (J0 + wn0 < nrest)) {
+#pragma unroll
+                for (int m = 0; m < 4; ++m) {
+                    const int i = I0 + wm0 + 8 * m + (lane >> 2);
+#pragma unroll
+                    for (int n = 0; n < 2; ++n)
+#pragma unroll
+                        for (int e = 0; e < 2; ++e)
+                            if (i < N && cv[n][e])
+                                asm volatile("prefetch.global.L2 [%0];" ::"l"(A + i + (size_t)ld * col[n][e]));
+                }
+            }
             cp_async_wait<0>();
             __syncthreads();
             if ((I0 + wm0 < N) && (J0 + wn0 < nrest)) {
@@ -925,7 +939,7 @@ __device__ int gj_invert_multi(double2 *__restrict__ A, int N, int ld, const Sme
             }
             __syncthreads();
         }
-        if (nbt < N) trailing_update<P * NB>(A, N, ld, k0, nbt, s);
+        if (nbt < N) trailing_update<P * NB, (RPT >= 4)>(A, N, ld, k0, nbt, s);
         __syncthreads();
         if (tid < nbt) s.inP[s.prow[k0 + tid]] = 0;
         __syncthreads();
