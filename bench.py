@@ -31,7 +31,7 @@ sys.path.insert(0, ROOT)
 METRIC = "RGF energy-point solves/s"
 # ncu dram bytes (read + write) of k_transmission per job-slice at N = 221, measured on a
 # 296-job, 16-slice launch (same per-slice work as the full workload)
-TRAFFIC_PER_JOB_SLICE_N221 = 67.088e9 / (296 * 16)
+TRAFFIC_PER_JOB_SLICE_N221 = 66.423e9 / (296 * 16)
 UNIT = "solves/s"
 
 
