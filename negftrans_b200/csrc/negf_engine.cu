@@ -574,19 +574,34 @@ int ensure_ws(negf_ctx *c, size_t bytes) {
     return 0;
 }
 
+// Grows the per-call arrays.  The capacity is zeroed before the old arrays
+// are released, so a failed allocation leaves the context empty (the next
+// call retries) rather than holding freed pointers under a stale capacity.
 int ensure_jobs(negf_ctx *c, int nE, int njobs) {
     if (nE > c->cap_E) {
+        c->cap_E = 0;
         if (c->d_E) CK(cudaFree(c->d_E));
         if (c->d_tau) CK(cudaFree(c->d_tau));
-        CK(cudaMalloc(&c->d_E, sizeof(double) * nE));
-        CK(cudaMalloc(&c->d_tau, sizeof(double) * nE));
+        c->d_E = nullptr;
+        c->d_tau = nullptr;
+        if (cudaMalloc(&c->d_E, sizeof(double) * nE) != cudaSuccess ||
+            cudaMalloc(&c->d_tau, sizeof(double) * nE) != cudaSuccess) {
+            cudaGetLastError();
+            return NEGF_ERR_NOMEM;
+        }
         c->cap_E = nE;
     }
     if (njobs > c->cap_jobs) {
+        c->cap_jobs = 0;
         if (c->d_tau_jobs) CK(cudaFree(c->d_tau_jobs));
         if (c->d_info) CK(cudaFree(c->d_info));
-        CK(cudaMalloc(&c->d_tau_jobs, sizeof(double) * njobs));
-        CK(cudaMalloc(&c->d_info, sizeof(int) * njobs));
+        c->d_tau_jobs = nullptr;
+        c->d_info = nullptr;
+        if (cudaMalloc(&c->d_tau_jobs, sizeof(double) * njobs) != cudaSuccess ||
+            cudaMalloc(&c->d_info, sizeof(int) * njobs) != cudaSuccess) {
+            cudaGetLastError();
+            return NEGF_ERR_NOMEM;
+        }
         c->cap_jobs = njobs;
     }
     return 0;
@@ -886,7 +901,7 @@ int negf_ctx_create(const negf_problem *p, int32_t device, negf_ctx **out) {
             ay[(size_t)k * p->N + i] = (double)(2 * p->ny[i]) * PI / p->Ly + p->kpt[3 * k + 1];
         }
     }
-#define CKC(x) do { if ((x) != cudaSuccess) { negf_ctx_destroy(c); return NEGF_ERR_CUDA; } } while (0)
+#define CKC(x) do { if ((x) != cudaSuccess) { cudaGetLastError(); negf_ctx_destroy(c); return NEGF_ERR_CUDA; } } while (0)
     CKC(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     CKC(cudaEventCreate(&c->ev0));
     CKC(cudaEventCreate(&c->ev1));
@@ -1281,8 +1296,11 @@ extern "C" int negf_transmission_batch(negf_ctx *const *ctxs, int32_t nctx, cons
     cudaStream_t st = c0->stream;
     std::fill(tau, tau + (size_t)nctx * nE, 0.0);
     double *d_E = nullptr;
-    CK(cudaMalloc(&d_E, sizeof(double) * nE));
-    CK(cudaMemcpyAsync(d_E, energies, sizeof(double) * nE, cudaMemcpyHostToDevice, st));
+    if (cudaMalloc(&d_E, sizeof(double) * nE) != cudaSuccess) { cudaGetLastError(); return NEGF_ERR_NOMEM; }
+    if (cudaMemcpyAsync(d_E, energies, sizeof(double) * nE, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+        cudaFree(d_E);
+        return NEGF_ERR_CUDA;
+    }
     std::vector<int> info_all;
     double ms_all = 0;
     int rc = 0;
