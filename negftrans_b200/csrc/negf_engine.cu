@@ -620,9 +620,11 @@ bool variant_fits(int v, int N) {
     return (v == V16x1 && N <= NT) || (v == V16x2 && N <= 2 * NT) || (v == V8x4 && N <= 4 * NT) ||
            (v == V8x1 && N <= NT);
 }
-// Default transmission variant: up to 256 plane waves the 8-column panels in
-// fours (8 x 1 x 2; at N = 69 6836 vs 5827 solves/s for 16 x 1 x 2, equal at
-// N = 221); the slab kernels keep pick_variant.
+// Default variant of the transmission kernels: up to 256 plane waves the
+// 8-column panels in fours (8 x 1 x 2; at N = 69 7100 vs 5784 solves/s for
+// 16 x 1 x 2, at N = 221 194 vs 184).  The slab kernels keep pick_variant:
+// their 8 x 1 x 2 build measured slower (N = 221: density 53.9 vs 55.2,
+// LDOS 47.3 vs 53.9 jobs/s; N = 69 LDOS 953 vs 1416).
 Variant transmission_variant(int N) { return N <= NT ? V8x1 : pick_variant(N); }
 Variant ctx_variant(const negf_ctx *c) {
     return (c->variant >= 0 && variant_fits(c->variant, c->N)) ? (Variant)c->variant : transmission_variant(c->N);
@@ -1729,7 +1731,7 @@ extern "C" int negf_transmission_noalloc(int32_t N, int32_t Nz, int32_t ngx, int
     if (N < 1 || Nz < 2 || ngx < 0 || ngy < 0 || nk < 1 || nE < 1 || !d_nx || !d_ny || !d_vhat ||
         !d_kpt || !d_energies || !d_tau || !(Lx > 0) || !(Ly > 0) || !(Lz > 0))
         return NEGF_ERR_ARG;
-    const Variant v = pick_variant(N);
+    const Variant v = transmission_variant(N);
     if (v == VNONE) return NEGF_ERR_UNSUPPORTED;
     cudaStream_t st = (cudaStream_t)stream;
     int dev = 0;
@@ -1770,6 +1772,7 @@ extern "C" int negf_transmission_noalloc(int32_t N, int32_t Nz, int32_t ngx, int
     switch (v) {
         case V16x1: rc = prep_kernel(k_transmission<16, 1, 2>, smem, &occ); break;
         case V16x2: rc = prep_kernel(k_transmission<16, 2, 1>, smem, &occ); break;
+        case V8x1: rc = prep_kernel(k_transmission<8, 1, 2>, smem, &occ); break;
         default: rc = prep_kernel(k_transmission<8, 4, 1>, smem, &occ); break;
     }
     if (rc) return rc;
@@ -1794,6 +1797,9 @@ extern "C" int negf_transmission_noalloc(int32_t N, int32_t Nz, int32_t ngx, int
             break;
         case V16x2:
             k_transmission<16, 2, 1><<<grid, NT, smem, st>>>(g, d_energies, nE, (int)njobs, ws, wstride, tau_jobs, d_info);
+            break;
+        case V8x1:
+            k_transmission<8, 1, 2><<<grid, NT, smem, st>>>(g, d_energies, nE, (int)njobs, ws, wstride, tau_jobs, d_info);
             break;
         default:
             k_transmission<8, 4, 1><<<grid, NT, smem, st>>>(g, d_energies, nE, (int)njobs, ws, wstride, tau_jobs, d_info);
