@@ -99,6 +99,42 @@ def test_transmission_small(oracle, nk):
     np.testing.assert_allclose(tau, tau_ref, rtol=RTOL, atol=1e-12)
 
 
+def test_transmission_device_entry(oracle):
+    """negf_transmission_device on device buffers and the caller's stream: the
+    same tau as the host entry, the per-job tau in k-major order summing to it
+    with the k weights, the per-job info; the optional outputs may be omitted."""
+    torch = pytest.importorskip("torch")
+    pr = small_problem(nk=2)
+    E = P.transmission_energies(pr.atomic, 16)
+    nE = len(E)
+    kpt = np.asarray(pr.kpoint, np.float64).reshape(-1, 3)
+    nk = len(kpt)
+    assert nk > 1
+    dev = torch.device("cuda", 0)
+    d_E = torch.from_numpy(np.ascontiguousarray(E)).to(dev)
+    d_tau = torch.full((nE,), float("nan"), dtype=torch.float64, device=dev)
+    d_tj = torch.full((nk * nE,), float("nan"), dtype=torch.float64, device=dev)
+    d_info = torch.full((nk * nE,), -7, dtype=torch.int32, device=dev)
+    d_tau2 = torch.full((nE,), float("nan"), dtype=torch.float64, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    with Engine(*pr.engine_args()) as eng:
+        tau_host, info_host = eng.transmission(E)
+        eng.transmission_device(d_E.data_ptr(), nE, d_tau.data_ptr(), d_tj.data_ptr(), d_info.data_ptr(),
+                                stream.cuda_stream)
+        stream.synchronize()
+        eng.transmission_device(d_E.data_ptr(), nE, d_tau2.data_ptr())
+        torch.cuda.synchronize(dev)
+    assert info_host == 0
+    tau, tau2 = d_tau.cpu().numpy(), d_tau2.cpu().numpy()
+    tj = d_tj.cpu().numpy().reshape(nk, nE)
+    np.testing.assert_array_equal(tau, tau_host)
+    np.testing.assert_array_equal(tau2, tau_host)
+    assert (d_info.cpu().numpy() == 0).all()
+    np.testing.assert_allclose(kpt[:, 2] @ tj, tau, rtol=1e-14, atol=1e-15)
+    tau_ref, _ = oracle.transmission_jobs(oracle_problem(oracle, pr), E, nthreads=4)
+    np.testing.assert_allclose(tau, tau_ref, rtol=RTOL, atol=1e-12)
+
+
 def test_transmission_leads_differ(oracle):
     """V_L != V_R exercises the gamma_L-on-rows quirk of grid.f90:363-374."""
     pr = small_problem(V_L=0.067 * 0.002, V_R=0.067 * 0.005)
