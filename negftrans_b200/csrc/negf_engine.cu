@@ -73,7 +73,7 @@ __device__ int transmission_job(const Geo &g, const Smem &s, double e, int ik, d
         const int r = gj_invert<NB, RPT>(oth, N, ld, s);
         if (r && !info) info = r;
         GemmArgs ga{Pn, ld, P, ld, s.iprow, oth, ld, s.iprow, nr, N, N, nullptr};
-        cta_gemm<true>(ga, s, GEMM_STORE, g.delta);
+        cta_gemm(ga, s, GEMM_STORE, g.delta);
         __syncthreads();
         double2 *t = cur; cur = oth; oth = t;
         t = P; P = Pn; Pn = t;
@@ -85,7 +85,7 @@ __device__ int transmission_job(const Geo &g, const Smem &s, double e, int ik, d
     if (r && !info) info = r;
     // tau = sum_ij gamma_L,i gamma_R,j |2 dz^2 G_{Nz,1}(i,j)|^2   grid.f90:362-383
     GemmArgs ga{nullptr, 0, P, ld, s.iprow, oth, ld, s.iprow, nr, N, N, s.rows};
-    double t = cta_gemm<true>(ga, s, GEMM_TAU, g.delta);
+    double t = cta_gemm(ga, s, GEMM_TAU, g.delta);
     t = block_sum(t, s);
     *tau = t;
     return info;

@@ -23,7 +23,10 @@ constexpr int NWARP = NT / 32;
 // Complex FP64 GEMMs run on the FP64 tensor cores (DMMA, mma.m8n8k4.f64):
 // a CTA tile of CM x CN outputs is split into 2 x 4 warp tiles of WM x WN
 // (4 x 2 m8n8 tiles each); warps whose tile lies outside the matrix skip
-// their MMAs, so the padding waste is at 8-row granularity only.
+// their MMAs, so the padding waste is at 8-row granularity only.  Warps 0-3
+// take rows 0-31 and warps 4-7 rows 32-63: warp w runs on SM sub-partition
+// w % 4, so a tile of at most 32 rows (the open-channel rows of the chain
+// product, the last row tile of a block) still keeps all four DMMA units busy.
 constexpr int CM = 64, CN = 64;  // CTA tile
 constexpr int WM = 32, WN = 16;  // warp tile
 constexpr int KC = 16;           // k chunk staged per pipeline step
@@ -372,37 +375,7 @@ struct WarpAcc {
             }
         }
     }
-    // Split-k exchange between the two warps of a column strip: x is the
-    // strip's [32 values][32 lanes] slot in shared memory (8 KB).
-    __device__ __forceinline__ void stash(double *x, int lane) const {
-#pragma unroll
-        for (int m = 0; m < 4; ++m)
-#pragma unroll
-            for (int n = 0; n < 2; ++n)
-#pragma unroll
-                for (int e = 0; e < 2; ++e) {
-                    const int v = ((m * 2 + n) * 2 + e) * 2;
-                    x[v * 32 + lane] = re[m][n][e];
-                    x[(v + 1) * 32 + lane] = im[m][n][e];
-                }
-    }
-    __device__ __forceinline__ void merge(const double *x, int lane) {
-#pragma unroll
-        for (int m = 0; m < 4; ++m)
-#pragma unroll
-            for (int n = 0; n < 2; ++n)
-#pragma unroll
-                for (int e = 0; e < 2; ++e) {
-                    const int v = ((m * 2 + n) * 2 + e) * 2;
-                    re[m][n][e] += x[v * 32 + lane];
-                    im[m][n][e] += x[(v + 1) * 32 + lane];
-                }
-    }
 };
-// Bytes of shared memory the split-k exchange needs: 4 strips x 8 KB.
-constexpr int SPLITK_BYTES = (NWARP / 2) * 32 * 32 * (int)sizeof(double);
-static_assert(2 * KC * AP * sizeof(double2) >= SPLITK_BYTES, "split-k slots must fit in the GEMM stages");
-static_assert(KC % 8 == 0, "split-k halves must be whole k steps");
 
 // C(i,j) = sum_k A(i, acol[k]) * B(k, bcol[j]) for one CTA, complex FP64.
 // acol/bcol == nullptr means identity.  Modes of the epilogue:
@@ -424,14 +397,9 @@ struct GemmArgs {
 
 // Returns, for GEMM_TAU, this thread's partial sum of
 // gL[i] * gR[j] * |(C(i,j)*2)*delta^2|^2 (grid.f90:362-383 after negf.f90:159-165).
-// SPLITK (the chain and trace products of the transmission sweep): a row
-// tile of at most WM rows splits its k chunks between the two warps of each
-// column strip instead of leaving half the warps idle.  N = 69: 7250 vs 7103
-// solves/s; the slab kernels' products measured slower with it.
-template <bool SPLITK = false>
 __device__ inline double cta_gemm(const GemmArgs &a, const Smem &s, int mode, double delta) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int wm0 = (warp & 1) * WM, wn0 = (warp >> 1) * WN;
+    const int wm0 = (warp >> 2) * WM, wn0 = (warp & 3) * WN;
     double2 *sA = s.big;                 // [2][KC][AP]
     double2 *sB = s.big + 2 * KC * AP;   // [2][KC][BP]
     const int ntm = (a.M + CM - 1) / CM, ntn = (a.Ncol + CN - 1) / CN;
@@ -439,12 +407,7 @@ __device__ inline double cta_gemm(const GemmArgs &a, const Smem &s, int mode, do
     double tau = 0.0;
     for (int t = 0; t < ntm * ntn; ++t) {
         const int I0 = (t % ntm) * CM, J0 = (t / ntm) * CN;
-        // a row tile of at most WM rows (the open-channel rows of the chain
-        // product): the two warps of a column strip take the same rows and
-        // split every k chunk instead of the rows
-        const bool split = SPLITK && a.M - I0 <= WM;
-        const int am0 = split ? 0 : wm0, kh = split ? (warp & 1) : 0;
-        const bool active = (I0 + am0 < a.M) && (J0 + wn0 < a.Ncol);
+        const bool active = (I0 + wm0 < a.M) && (J0 + wn0 < a.Ncol);
         WarpAcc acc;
         acc.zero();
         auto load_stage = [&](int st, int k0) {
@@ -482,27 +445,15 @@ __device__ inline double cta_gemm(const GemmArgs &a, const Smem &s, int mode, do
             if (active) {
                 const double2 *cA = sA + (c & 1) * KC * AP;
                 const double2 *cB = sB + (c & 1) * KC * BP;
-                if (split) {
 #pragma unroll
-                    for (int kb = 0; kb < KC / 2; kb += 4) acc.step(cA, AP, 0, cB, BP, wn0, kh * (KC / 2) + kb, lane);
-                } else {
-#pragma unroll
-                    for (int kb = 0; kb < KC; kb += 4) acc.step(cA, AP, wm0, cB, BP, wn0, kb, lane);
-                }
+                for (int kb = 0; kb < KC; kb += 4) acc.step(cA, AP, wm0, cB, BP, wn0, kb, lane);
             }
             __syncthreads();
         }
-        if (split) {
-            // the stages are free after the last chunk's barrier
-            double *x = reinterpret_cast<double *>(s.big) + (warp >> 1) * 32 * 32;
-            if (active && kh == 1) acc.stash(x, lane);
-            __syncthreads();
-            if (active && kh == 0) acc.merge(x, lane);
-        }
-        if (active && kh == 0) {
+        if (active) {
 #pragma unroll
             for (int m = 0; m < 4; ++m) {
-                const int i = I0 + am0 + 8 * m + (lane >> 2);
+                const int i = I0 + wm0 + 8 * m + (lane >> 2);
 #pragma unroll
                 for (int n = 0; n < 2; ++n)
 #pragma unroll
@@ -525,7 +476,6 @@ __device__ inline double cta_gemm(const GemmArgs &a, const Smem &s, int mode, do
                     }
             }
         }
-        if (split) __syncthreads();  // the next tile's first stage overwrites the exchange slots
     }
     return tau;
 }
@@ -556,7 +506,7 @@ template <int KMAX, bool PREFETCH = false>
 __device__ inline void trailing_update(double2 *__restrict__ A, int N, int ld, int k0, int nbt,
                                        const Smem &s) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int wm0 = (warp & 1) * WM, wn0 = (warp >> 1) * WN;
+    const int wm0 = (warp >> 2) * WM, wn0 = (warp & 3) * WN;
     const int nrest = N - nbt;
     double2 *sB = s.big;               // [KMAX][BP] pivot rows of the column tile
     double2 *sW = s.big + KMAX * BP;   // [KMAX][AP] rows I0.. of the panel
