@@ -106,6 +106,36 @@ def oracle_problem(O, pr):
     return O.Problem(pr.nx, pr.ny, pr.vhat, a.LX, a.LY, a.LZ, a.V_L, a.V_R, a.ETA, pr.kpoint)
 
 
+def oracle_inputs(w):
+    """The inputs of workload w built by the oracle's own restatement of the
+    set-up (grid.f90:387-448 basis and k-mesh, grid.f90:12-69 + main.f90:239-249
+    V table), so that the reference arm runs no code of libnegfgpu.so.  The
+    deck's unit conversion (main.f90:184-205) is plain Python arithmetic."""
+    from negftrans_b200 import prepare as P
+    from oracle import oracle as O
+    d = w.deck
+    a = P.to_atomic(d)
+    ngx, ngy = P.ngrid(P.scaled_deck(d))
+    vh = np.asfortranarray(w.V_eV, dtype=np.float64) * P.scaled_deck_factor(d) / P.HARTREE
+    kp = O.kmesh(d.NKX, d.NKY, a.LX, a.LY)
+    nx, ny = O.basis(a.ENCUT, a.LX, a.LY)
+    vhat = O.vhat_all(vh, ngx, ngy)
+    p = O.Problem(nx, ny, vhat, a.LX, a.LY, a.LZ, a.V_L, a.V_R, a.ETA, kp)
+    return p, P.transmission_energies(a, w.n_energy)
+
+
+def cpu_rate_problem(p, energies, nthreads, reps=1):
+    """Solves/s of the oracle on problem p with `nthreads` host threads (one job each)."""
+    from oracle import oracle as O
+    E = np.asarray(energies[:nthreads], np.float64)
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        O.transmission_jobs(p, E, nthreads=nthreads)
+        times.append(time.perf_counter() - t0)
+    return len(E) / statistics.mean(times), times
+
+
 def cpu_rate(pr, energies, nthreads, reps=1):
     """Solves/s of the oracle port on `nthreads` host threads (one job each)."""
     from oracle import oracle as O
@@ -195,27 +225,26 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from negftrans_b200 import prepare as P, workloads as W
+    from negftrans_b200 import workloads as W
     w = W.config(args.workload)
-    pr = P.prepare(w.deck, w.V_eV)
-    E = P.transmission_energies(pr.atomic, w.n_energy)
-    nth = host_threads(args.cpu_threads, oracle_job_bytes(pr))
+    p, E = oracle_inputs(w)
+    nth = host_threads(args.cpu_threads, 4 * 16 * p.N * p.N * p.Nz)
     for _ in range(args.warmup):
-        cpu_rate(pr, E, nth)
+        cpu_rate_problem(p, E, nth)
     times = []
     for s in range(args.steps):
         sample = np.roll(E, -s * nth)
-        r, t = cpu_rate(pr, sample, nth)
+        r, t = cpu_rate_problem(p, sample, nth)
         times.append(t[0])
     ms = 1e3 * statistics.mean(times)
     value = nth / (ms * 1e-3)
-    sample = f"{nth} (E,k) sweeps per step, one per host thread (N={pr.N}, Nz={pr.Nz})"
+    sample = f"{nth} (E,k) sweeps per step, one per host thread (N={p.N}, Nz={p.Nz})"
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-        "config": {"workload": args.workload, "N": pr.N, "Nz": pr.Nz, "energies": w.n_energy,
-                   "kpoints": len(pr.kpoint)},
+        "config": {"workload": args.workload, "N": p.N, "Nz": p.Nz, "energies": w.n_energy,
+                   "kpoints": len(p.kpt)},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": nth, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference (Fortran+MPI+FFTW+LAPACK) cannot be built on this image; its "

@@ -170,12 +170,17 @@ int negf_transmission_device(negf_ctx *ctx, const double *d_energies, int32_t nE
  * every GPU that loads the library until the process exits; problems whose
  * per-job workspace (64 * roundup(N,8) * N bytes) does not fit return
  * NEGF_ERR_TOO_LARGE, and fewer jobs run at once when only a few fit.
- * The first call on a device looks up that array's device address; make
- * that first call before any stream capture.  The call blocks until a check
- * that every basis difference indexes inside the V table has run on
- * `stream`, then enqueues the sweep on `stream` and returns.  All calls share
- * the one array: calls whose work overlaps on the GPU (other streams, other
- * host threads) race and must be serialised by the caller. */
+ * The first call on a device looks up that array's device address in the
+ * device's primary context and keeps it for the life of the process, so the
+ * entry assumes the primary context (the CUDA runtime's default) and no
+ * cudaDeviceReset between calls.  Every call blocks: it copies a check result
+ * to the host (that every basis difference indexes inside the V table) and
+ * synchronises `stream` before it enqueues the sweep on `stream` and returns,
+ * so it cannot be called while `stream` is being captured into a CUDA graph.
+ * nE * nk above INT32_MAX returns NEGF_ERR_ARG.  All calls share the one
+ * array, which keeps the last call's contents: calls whose work overlaps on
+ * the GPU (other streams, other host threads) race and must be serialised by
+ * the caller. */
 int negf_transmission_noalloc(int32_t N, int32_t Nz, int32_t ngx, int32_t ngy, const int32_t *d_nx,
                               const int32_t *d_ny, const double *d_vhat, double Lx, double Ly,
                               double Lz, double V_L, double V_R, double eta, int32_t nk,

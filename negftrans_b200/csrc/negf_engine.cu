@@ -942,6 +942,7 @@ int negf_transmission_device(negf_ctx *c, const double *d_energies, int32_t nE, 
                              double *d_tau, double *d_tau_jobs, int32_t *d_info, void *stream) {
     if (!c || !d_energies || !d_tau || nE < 1) return NEGF_ERR_ARG;
     if (precision != NEGF_FP64) return NEGF_ERR_UNSUPPORTED;
+    if ((int64_t)nE * c->nk > INT32_MAX) return NEGF_ERR_ARG;  // jobs are indexed as int
     if (cudaSetDevice(c->device) != cudaSuccess) return NEGF_ERR_CUDA;
     const int njobs = nE * c->nk;
     int rc = ensure_jobs(c, 1, njobs);
@@ -954,6 +955,7 @@ int negf_transmission(negf_ctx *c, const double *energies, int32_t nE, int32_t p
                       negf_stats *stats) {
     if (!c || !energies || !tau || nE < 1) return NEGF_ERR_ARG;
     if (precision != NEGF_FP64) return NEGF_ERR_UNSUPPORTED;
+    if ((int64_t)nE * c->nk > INT32_MAX) return NEGF_ERR_ARG;  // jobs are indexed as int
     if (cudaSetDevice(c->device) != cudaSuccess) return NEGF_ERR_CUDA;
     const int njobs = nE * c->nk;
     int rc = ensure_jobs(c, nE, njobs);
@@ -1740,6 +1742,7 @@ extern "C" int negf_transmission_noalloc(int32_t N, int32_t Nz, int32_t ngx, int
     // scratch layout: [flag | ax | ay | kw | tau_jobs] then one workspace per CTA
     const int ld = round_up(N, 8);
     const size_t njobs = (size_t)nE * nk;
+    if (njobs > (size_t)INT32_MAX) return NEGF_ERR_ARG;  // the kernels index jobs as int
     const size_t head_doubles = 2 + 2 * (size_t)nk * N + nk + njobs;
     const size_t head_bytes = (head_doubles * sizeof(double) + 255) / 256 * 256;
     const size_t wstride = 4 * (size_t)ld * N;  // double2 per CTA
