@@ -264,6 +264,22 @@ int negf_ldos(negf_ctx *ctx, double e_lo, double e_hi, int32_t n_e, const int32_
 int negf_ptor(const double *g, const int32_t *nx, const int32_t *ny, int32_t N, int32_t Nz_s,
               int32_t Nx, int32_t Ny, double *out);
 
+/* ------------------------------------------------------------ diagnostics
+ * Checks of the tensor-core arithmetic of the mixed-precision path (no
+ * reference counterpart; device pointers, complex FP32 interleaved,
+ * column-major; block until done; NEGF_ERR_CUDA if a tensor-core wait timed
+ * out).
+ * negf_tc_product_check: C(M, ncol) = W(:, 0:K) * B(rowmap[0:K], :) with the
+ * split-fp16 tensor-core product of the trailing update (K <= 32).
+ * negf_tc_inverse_check: the inverses of nmat N x N matrices (A: nmat
+ * consecutive N*N blocks, N <= 1023) by the FP32 Gauss-Jordan inverse with
+ * tensor-core trailing updates; info[m] as LAPACK's. */
+int negf_tc_product_check(const float *d_W, int32_t ldw, const float *d_B, int32_t ldb,
+                          const int32_t *d_rowmap, float *d_C, int32_t ldc, int32_t M, int32_t ncol,
+                          int32_t K, void *stream);
+int negf_tc_inverse_check(const float *d_A, int32_t N, int32_t nmat, float *d_out, int32_t *d_info,
+                          void *stream);
+
 /* Library version string. */
 const char *negf_version(void);
 

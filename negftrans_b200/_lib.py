@@ -26,7 +26,7 @@ EXPORTS = (
     "negf_density", "negf_ldos_matrix", "negf_ptor", "negf_version", "negf_transmission_noalloc",
     "negf_density_real", "negf_ldos", "negf_basis_k", "negf_transmission_batch",
     "negf_density_neq", "negf_dm_real", "negf_set_variant", "negf_autotune", "negf_vhat_gpu",
-    "negf_density_accumulate",
+    "negf_density_accumulate", "negf_tc_product_check", "negf_tc_inverse_check",
 )
 # every symbol include/negf_mlp.h declares
 MLP_EXPORTS = (
@@ -104,6 +104,9 @@ def lib():
     L.negf_density_accumulate.argtypes = [C.c_void_p, _dp, _dp, C.c_int32, _dp, C.POINTER(Stats)]
     L.negf_vhat_gpu.argtypes = [_dp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _dp]
     L.negf_autotune.argtypes = [C.c_void_p, _dp, C.c_int32, _ip, _dp]
+    L.negf_tc_product_check.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p,
+                                        C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p]
+    L.negf_tc_inverse_check.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]
     _fp = C.POINTER(C.c_float)
     L.negf_mlp_create.argtypes = [C.c_int32, _ip, C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]
     L.negf_mlp_destroy.argtypes = [C.c_void_p]

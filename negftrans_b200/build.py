@@ -13,8 +13,11 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libnegfgpu.so")
 DRIVER = os.path.join(PKG, "negftrans")   # the main.f90-style executable
-SOURCES = ["negf_engine.cu", "negf_host.cpp", "mlp.cu"]
-HEADERS = ["rgf_device.cuh"]
+SOURCES = ["negf_engine.cu", "negf_host.cpp", "mlp.cu", "negf_mixed.cu"]
+HEADERS = ["rgf_device.cuh", "tc_umma.cuh", "mixed_device.cuh"]
+# private headers each source includes
+DEPS = {"negf_engine.cu": ("rgf_device.cuh",),
+        "negf_mixed.cu": ("rgf_device.cuh", "tc_umma.cuh", "mixed_device.cuh")}
 PUBLIC_HEADERS = ["negf_gpu.h", "negf_mlp.h"]
 OBJDIR = os.path.join(PKG, "_build")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -52,10 +55,17 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if verbose:
         base += ["-Xptxas", "-v"]
     procs, objs = [], []
+    pub_t = max(os.path.getmtime(os.path.join(ROOT, "include", h)) for h in PUBLIC_HEADERS)
     for f in SOURCES:
         obj = os.path.join(OBJDIR, os.path.splitext(f)[0] + ".o")
         objs.append(obj)
-        procs.append((f, subprocess.Popen(base + ["-c", os.path.join(CSRC, f), "-o", obj])))
+        src = os.path.join(CSRC, f)
+        dep_t = max([os.path.getmtime(src), pub_t] + [os.path.getmtime(os.path.join(CSRC, h))
+                                                      for h in DEPS.get(f, ())])
+        # an object newer than its source and the headers it includes is reused
+        if not force and os.path.exists(obj) and os.path.getmtime(obj) >= dep_t:
+            continue
+        procs.append((f, subprocess.Popen(base + ["-c", src, "-o", obj])))
     bad = [f for f, p in procs if p.wait() != 0]
     if bad:
         raise RuntimeError("nvcc failed on " + ", ".join(bad))
