@@ -37,7 +37,9 @@ extern "C" {
 #define NEGF_ERR_UNSUPPORTED (-4)
 #define NEGF_ERR_TOO_LARGE (-5) /* problem needs more than the fixed scratch */
 
-#define NEGF_FP64 0 /* complex128 throughout */
+#define NEGF_FP64 0  /* complex128 throughout */
+#define NEGF_MIXED 1 /* split-fp16 tensor-core factorization, FP64 residual refinement,
+                      * FP64 re-run of the jobs the check rejects (see negf_mixed_policy) */
 
 typedef struct negf_ctx negf_ctx;
 
@@ -61,6 +63,34 @@ typedef struct negf_problem {
                            * function of the discretised flat lead (the fixed point
                            * of Sancho-Rubio decimation, no reference counterpart)  */
 } negf_problem;
+
+/* Policy of the NEGF_MIXED path (no reference counterpart: the reference runs
+ * LAPACK in complex*16 only, math_kernel.f90:8-42).  Every energy point is
+ * either refined from the mixed-precision factorization and accepted, or
+ * solved by the FP64 path; none is reported from low precision alone. */
+typedef struct negf_mixed_policy {
+    double threshold_window; /* Hartree.  Jobs whose energy lies within this distance of
+                              * a subband threshold V + |k+G|^2/2 of either lead run in
+                              * FP64.  0 = off (the default).                           */
+    double eta_fp64_below;   /* Hartree.  If the context's eta is below this, every job
+                              * runs in FP64.  0 = off (the default).                   */
+    double tau_tolerance;    /* A refined job is accepted when its estimated remaining
+                              * error 2 max(tau, 1) (|d| / |x|)^2 is below this (d: the
+                              * refinement correction of G_{Nz,1} on the open channels,
+                              * x the refined value).  Default 1e-7.                    */
+} negf_mixed_policy;
+
+typedef struct negf_mixed_stats {
+    int32_t n_jobs;          /* (E,k) jobs of the last NEGF_MIXED call                  */
+    int32_t n_mixed;         /* accepted from the mixed path                            */
+    int32_t n_fp64_policy;   /* sent to FP64 by the policy                              */
+    int32_t n_fp64_rejected; /* refined, rejected by the check and re-run in FP64       */
+    int32_t jobs_per_wave;   /* mixed jobs resident at once (device memory bound)       */
+    int32_t pad;
+    double max_correction;   /* largest |d| / |x| among accepted jobs                   */
+    double mixed_ms;         /* device time of the mixed part (CUDA events)             */
+    double fp64_ms;          /* device time of the FP64 re-runs                         */
+} negf_mixed_stats;
 
 typedef struct negf_stats {
     int32_t n_jobs;        /* (E,k) RGF sweeps run                                */
@@ -123,6 +153,24 @@ int negf_tri_solve(negf_ctx *ctx, const double *D, int32_t N, int32_t Nz, const 
  * tau[e] = sum_k weight_k * tau(E_e, k), the reduced Transmission(:)%tau. */
 int negf_transmission(negf_ctx *ctx, const double *energies, int32_t nE, int32_t precision,
                       double *tau, negf_stats *stats);
+
+/* The NEGF_MIXED path of negf_transmission / negf_transmission_device.
+ * Per job: the Schur complements D_k - gR(k) are formed in FP64 and rounded
+ * to complex FP32; their inverses use FP32 Gauss-Jordan panels with partial
+ * pivoting and rank-32 trailing updates on the tcgen05 tensor cores in split
+ * fp16 (FP32 accumulation); every generator is kept in device memory.  Then
+ * one refinement step on the open channels of the right lead: x0 = first
+ * block column of G from the stored factors, the residual of the whole
+ * block-tridiagonal system in FP64, the correction d from the stored
+ * factors, and tau (grid.f90:362-383) from x0 + d in FP64.  Jobs rejected by
+ * the check of negf_mixed_policy, and jobs the policy sends to FP64, are
+ * re-run by the FP64 path; tau and stats then cover all jobs.  Jobs are
+ * processed in waves sized to the free device memory (about 8 N^2 N_z bytes
+ * per job).  negf_transmission_device with NEGF_MIXED synchronises `stream`
+ * once per wave (to schedule the re-runs).  N <= 1023. */
+int negf_set_mixed_policy(negf_ctx *ctx, const negf_mixed_policy *policy);
+int negf_get_mixed_policy(const negf_ctx *ctx, negf_mixed_policy *policy);
+int negf_get_mixed_stats(const negf_ctx *ctx, negf_mixed_stats *stats);
 
 /* negf_transmission for nctx problems at once -- e.g. one per k-point with a
  * per-k basis, or several devices of different length -- on the device of

@@ -18,6 +18,7 @@ NEGF_ERR_NOMEM = -3
 NEGF_ERR_UNSUPPORTED = -4
 NEGF_ERR_TOO_LARGE = -5
 NEGF_FP64 = 0
+NEGF_MIXED = 1
 
 # every symbol include/negf_gpu.h declares
 EXPORTS = (
@@ -27,6 +28,7 @@ EXPORTS = (
     "negf_density_real", "negf_ldos", "negf_basis_k", "negf_transmission_batch",
     "negf_density_neq", "negf_dm_real", "negf_set_variant", "negf_autotune", "negf_vhat_gpu",
     "negf_density_accumulate", "negf_tc_product_check", "negf_tc_inverse_check",
+    "negf_set_mixed_policy", "negf_get_mixed_policy", "negf_get_mixed_stats",
 )
 # every symbol include/negf_mlp.h declares
 MLP_EXPORTS = (
@@ -43,6 +45,19 @@ class Problem(C.Structure):
                 ("nx", _ip), ("ny", _ip), ("vhat", _dp), ("Lx", C.c_double), ("Ly", C.c_double),
                 ("Lz", C.c_double), ("V_L", C.c_double), ("V_R", C.c_double), ("eta", C.c_double),
                 ("nk", C.c_int32), ("kpt", _dp), ("lead_model", C.c_int32)]
+
+
+class MixedPolicy(C.Structure):
+    _fields_ = [("threshold_window", C.c_double), ("eta_fp64_below", C.c_double), ("tau_tolerance", C.c_double)]
+
+
+class MixedStats(C.Structure):
+    _fields_ = [("n_jobs", C.c_int32), ("n_mixed", C.c_int32), ("n_fp64_policy", C.c_int32),
+                ("n_fp64_rejected", C.c_int32), ("jobs_per_wave", C.c_int32), ("pad", C.c_int32),
+                ("max_correction", C.c_double), ("mixed_ms", C.c_double), ("fp64_ms", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
 
 
 class Stats(C.Structure):
@@ -107,6 +122,9 @@ def lib():
     L.negf_tc_product_check.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p,
                                         C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p]
     L.negf_tc_inverse_check.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.negf_set_mixed_policy.argtypes = [C.c_void_p, C.POINTER(MixedPolicy)]
+    L.negf_get_mixed_policy.argtypes = [C.c_void_p, C.POINTER(MixedPolicy)]
+    L.negf_get_mixed_stats.argtypes = [C.c_void_p, C.POINTER(MixedStats)]
     _fp = C.POINTER(C.c_float)
     L.negf_mlp_create.argtypes = [C.c_int32, _ip, C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]
     L.negf_mlp_destroy.argtypes = [C.c_void_p]

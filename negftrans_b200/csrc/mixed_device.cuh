@@ -67,7 +67,7 @@ struct TileSmem {
     uint64_t *bar;
     uint32_t *tslot;
 };
-constexpr size_t tile_smem_bytes() {
+__host__ __device__ constexpr size_t tile_smem_bytes() {
     return 4 * (size_t)TM * KB * 2 + 4 * (size_t)TN * KB * 2 + TM * 4 + TN * 4 + 16 + 16;
 }
 // base must be 128-byte aligned

@@ -18,6 +18,7 @@
 #include <mutex>
 #include <vector>
 
+#include "engine_internal.h"
 #include "negf_gpu.h"
 #include "rgf_device.cuh"
 
@@ -517,27 +518,7 @@ __global__ void k_ldos_convert(const double2 *__restrict__ diag, int Nx, int Ny,
 }  // namespace
 
 // ======================================================================= host
-struct negf_ctx {
-    int device = 0;
-    int num_sms = 0;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    int N = 0, Nz = 0, ld = 0, ngx = 0, ngy = 0, nk = 0;
-    double Lx = 0, Ly = 0, Lz = 0, V_L = 0, V_R = 0, eta = 0;
-    int lead_model = 0;
-    int variant = -1;         // transmission kernel variant forced by negf_set_variant /
-                              // negf_autotune; -1 = chosen by N
-    std::vector<double> kpt;  // nk x 3
-    double2 *d_vhat = nullptr;
-    int *d_nx = nullptr, *d_ny = nullptr;
-    double *d_ax = nullptr, *d_ay = nullptr, *d_kw = nullptr;
-    // scratch grown on demand
-    void *d_ws = nullptr;
-    size_t ws_bytes = 0;
-    double *d_E = nullptr, *d_tau = nullptr, *d_tau_jobs = nullptr;
-    int *d_info = nullptr;
-    int cap_E = 0, cap_jobs = 0;
-};
+// struct negf_ctx: engine_internal.h
 
 namespace {
 
@@ -893,6 +874,8 @@ int negf_ctx_create(const negf_problem *p, int32_t device, negf_ctx **out) {
     c->V_L = p->V_L; c->V_R = p->V_R; c->eta = p->eta;
     c->lead_model = p->lead_model;
     c->kpt.assign(p->kpt, p->kpt + 3 * (size_t)p->nk);
+    c->nx.assign(p->nx, p->nx + p->N);
+    c->ny.assign(p->ny, p->ny + p->N);
     const size_t nv = (size_t)(2 * p->ngx + 1) * (2 * p->ngy + 1) * p->Nz;
     std::vector<double> ax((size_t)p->nk * p->N), ay((size_t)p->nk * p->N), kw(p->nk);
     for (int k = 0; k < p->nk; ++k) {
@@ -931,6 +914,7 @@ int negf_ctx_destroy(negf_ctx *c) {
     cudaFree(c->d_vhat); cudaFree(c->d_nx); cudaFree(c->d_ny);
     cudaFree(c->d_ax); cudaFree(c->d_ay); cudaFree(c->d_kw);
     cudaFree(c->d_ws); cudaFree(c->d_E); cudaFree(c->d_tau); cudaFree(c->d_tau_jobs); cudaFree(c->d_info);
+    cudaFree(c->d_mixed);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -941,10 +925,29 @@ int negf_ctx_destroy(negf_ctx *c) {
 int negf_transmission_device(negf_ctx *c, const double *d_energies, int32_t nE, int32_t precision,
                              double *d_tau, double *d_tau_jobs, int32_t *d_info, void *stream) {
     if (!c || !d_energies || !d_tau || nE < 1) return NEGF_ERR_ARG;
-    if (precision != NEGF_FP64) return NEGF_ERR_UNSUPPORTED;
+    if (precision != NEGF_FP64 && precision != NEGF_MIXED) return NEGF_ERR_UNSUPPORTED;
     if ((int64_t)nE * c->nk > INT32_MAX) return NEGF_ERR_ARG;  // jobs are indexed as int
     if (cudaSetDevice(c->device) != cudaSuccess) return NEGF_ERR_CUDA;
     const int njobs = nE * c->nk;
+    if (precision == NEGF_MIXED) {
+        // the mixed path schedules FP64 re-runs on the host: wait for the
+        // caller's stream, run on the context's, hand the results back
+        cudaStream_t cs = (cudaStream_t)stream;
+        CK(cudaStreamSynchronize(cs));
+        std::vector<double> E(nE), tj(njobs), tau(nE, 0.0);
+        std::vector<int> info(njobs);
+        CK(cudaMemcpy(E.data(), d_energies, sizeof(double) * nE, cudaMemcpyDeviceToHost));
+        double ms = 0;
+        int rc = negf_internal_mixed(c, E.data(), d_energies, nE, tj.data(), info.data(), &ms);
+        if (rc < 0) return rc;
+        for (int ik = 0; ik < c->nk; ++ik)
+            for (int ie = 0; ie < nE; ++ie) tau[ie] += tj[(size_t)ik * nE + ie] * c->kpt[3 * ik + 2];
+        CK(cudaMemcpyAsync(d_tau, tau.data(), sizeof(double) * nE, cudaMemcpyHostToDevice, cs));
+        if (d_tau_jobs) CK(cudaMemcpyAsync(d_tau_jobs, tj.data(), sizeof(double) * njobs, cudaMemcpyHostToDevice, cs));
+        if (d_info) CK(cudaMemcpyAsync(d_info, info.data(), sizeof(int) * njobs, cudaMemcpyHostToDevice, cs));
+        CK(cudaStreamSynchronize(cs));
+        return NEGF_OK;
+    }
     int rc = ensure_jobs(c, 1, njobs);
     if (rc) return rc;
     double *tj = d_tau_jobs ? d_tau_jobs : c->d_tau_jobs;
@@ -954,12 +957,26 @@ int negf_transmission_device(negf_ctx *c, const double *d_energies, int32_t nE, 
 int negf_transmission(negf_ctx *c, const double *energies, int32_t nE, int32_t precision, double *tau,
                       negf_stats *stats) {
     if (!c || !energies || !tau || nE < 1) return NEGF_ERR_ARG;
-    if (precision != NEGF_FP64) return NEGF_ERR_UNSUPPORTED;
+    if (precision != NEGF_FP64 && precision != NEGF_MIXED) return NEGF_ERR_UNSUPPORTED;
     if ((int64_t)nE * c->nk > INT32_MAX) return NEGF_ERR_ARG;  // jobs are indexed as int
     if (cudaSetDevice(c->device) != cudaSuccess) return NEGF_ERR_CUDA;
     const int njobs = nE * c->nk;
     int rc = ensure_jobs(c, nE, njobs);
     if (rc) return rc;
+    if (precision == NEGF_MIXED) {
+        CK(cudaMemcpyAsync(c->d_E, energies, sizeof(double) * nE, cudaMemcpyHostToDevice, c->stream));
+        std::vector<double> tj(njobs);
+        std::vector<int> info(njobs);
+        double ms = 0;
+        rc = negf_internal_mixed(c, energies, c->d_E, nE, tj.data(), info.data(), &ms);
+        if (rc < 0) return rc;
+        // tau(E) = sum_k w_k tau(E,k) in k order (negf.f90:172)
+        for (int ie = 0; ie < nE; ++ie) tau[ie] = 0.0;
+        for (int ik = 0; ik < c->nk; ++ik)
+            for (int ie = 0; ie < nE; ++ie) tau[ie] += tj[(size_t)ik * nE + ie] * c->kpt[3 * ik + 2];
+        fill_stats(stats, info, (float)ms);
+        return first_info(info);
+    }
     CK(cudaMemcpyAsync(c->d_E, energies, sizeof(double) * nE, cudaMemcpyHostToDevice, c->stream));
     CK(cudaEventRecord(c->ev0, c->stream));
     rc = transmission_launch(c, c->d_E, nE, c->d_tau, c->d_tau_jobs, c->d_info, c->stream);
@@ -1288,6 +1305,87 @@ done:
 }
 
 }  // extern "C"
+
+// FP64 re-runs for the mixed path: the listed (energy, k-point) jobs of one
+// context through the batch kernel.
+int negf_internal_fp64_jobs(negf_ctx *c, const double *d_E, const int *ie, const int *ik, int njobs,
+                            double *h_tau, int *h_info, float *ms) {
+    *ms = 0.f;
+    if (njobs <= 0) return 0;
+    cudaStream_t st = c->stream;
+    const Variant var = ctx_variant(c);
+    if (var == VNONE) return NEGF_ERR_UNSUPPORTED;
+    std::vector<BatchJob> jobs(njobs);
+    for (int q = 0; q < njobs; ++q) jobs[q] = BatchJob{0, ie[q], ik[q], 0};
+    const size_t smem = variant_smem(var, c->N);
+    int occ = 1, rc = 0;
+    switch (var) {
+        case V16x1: rc = prep_kernel(k_transmission_batch<16, 1, 2>, smem, &occ); break;
+        case V8x1: rc = prep_kernel(k_transmission_batch<8, 1, 2>, smem, &occ); break;
+        case V16x2: rc = prep_kernel(k_transmission_batch<16, 2, 1>, smem, &occ); break;
+        default: rc = prep_kernel(k_transmission_batch<8, 4, 1>, smem, &occ); break;
+    }
+    if (rc) return rc;
+    const int grid = std::min(njobs, c->num_sms * occ);
+    const size_t wstride = 4 * (size_t)c->ld * c->N;
+    if ((rc = ensure_ws(c, sizeof(double2) * wstride * grid))) return rc;
+    Geo g = make_geo(c);
+    Geo *d_geo = nullptr;
+    BatchJob *d_jobs = nullptr;
+    double *d_tj = nullptr;
+    int *d_info = nullptr, *d_counter = nullptr;
+    if (cudaMalloc(&d_geo, sizeof(Geo)) != cudaSuccess || cudaMalloc(&d_jobs, sizeof(BatchJob) * njobs) != cudaSuccess ||
+        cudaMalloc(&d_tj, sizeof(double) * njobs) != cudaSuccess || cudaMalloc(&d_info, sizeof(int) * njobs) != cudaSuccess ||
+        cudaMalloc(&d_counter, sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        rc = NEGF_ERR_NOMEM;
+    }
+    if (!rc && (cudaMemcpyAsync(d_geo, &g, sizeof(Geo), cudaMemcpyHostToDevice, st) ||
+                cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(BatchJob) * njobs, cudaMemcpyHostToDevice, st) ||
+                cudaMemsetAsync(d_counter, 0, sizeof(int), st) || cudaEventRecord(c->ev0, st)))
+        rc = NEGF_ERR_CUDA;
+    if (!rc) {
+        double2 *ws = (double2 *)c->d_ws;
+        switch (var) {
+            case V16x1:
+                k_transmission_batch<16, 1, 2><<<grid, NT, smem, st>>>(d_geo, d_jobs, njobs, d_E, ws, wstride, d_tj, d_info, d_counter);
+                break;
+            case V16x2:
+                k_transmission_batch<16, 2, 1><<<grid, NT, smem, st>>>(d_geo, d_jobs, njobs, d_E, ws, wstride, d_tj, d_info, d_counter);
+                break;
+            case V8x1:
+                k_transmission_batch<8, 1, 2><<<grid, NT, smem, st>>>(d_geo, d_jobs, njobs, d_E, ws, wstride, d_tj, d_info, d_counter);
+                break;
+            default:
+                k_transmission_batch<8, 4, 1><<<grid, NT, smem, st>>>(d_geo, d_jobs, njobs, d_E, ws, wstride, d_tj, d_info, d_counter);
+                break;
+        }
+        if (cudaGetLastError() || cudaEventRecord(c->ev1, st) ||
+            cudaMemcpyAsync(h_tau, d_tj, sizeof(double) * njobs, cudaMemcpyDeviceToHost, st) ||
+            cudaMemcpyAsync(h_info, d_info, sizeof(int) * njobs, cudaMemcpyDeviceToHost, st) ||
+            cudaStreamSynchronize(st) || cudaEventElapsedTime(ms, c->ev0, c->ev1))
+            rc = NEGF_ERR_CUDA;
+    }
+    cudaFree(d_geo); cudaFree(d_jobs); cudaFree(d_tj); cudaFree(d_info); cudaFree(d_counter);
+    return rc;
+}
+
+extern "C" int negf_set_mixed_policy(negf_ctx *c, const negf_mixed_policy *p) {
+    if (!c || !p || !(p->threshold_window >= 0) || !(p->eta_fp64_below >= 0) || !(p->tau_tolerance > 0))
+        return NEGF_ERR_ARG;
+    c->mixed_policy = *p;
+    return NEGF_OK;
+}
+extern "C" int negf_get_mixed_policy(const negf_ctx *c, negf_mixed_policy *p) {
+    if (!c || !p) return NEGF_ERR_ARG;
+    *p = c->mixed_policy;
+    return NEGF_OK;
+}
+extern "C" int negf_get_mixed_stats(const negf_ctx *c, negf_mixed_stats *s) {
+    if (!c || !s) return NEGF_ERR_ARG;
+    *s = c->mixed_stats;
+    return NEGF_OK;
+}
 
 // ------------------------------------------------------ batches of problems
 extern "C" int negf_transmission_batch(negf_ctx *const *ctxs, int32_t nctx, const double *energies, int32_t nE,

@@ -27,11 +27,13 @@
 #include <cstdio>
 #include <vector>
 
+#include "engine_internal.h"
 #include "mixed_device.cuh"
 #include "negf_gpu.h"
+#include "rgf_device.cuh"
 
-using namespace negf;
 using namespace negf::mx;
+namespace tc = negf::tc;
 
 namespace {
 
@@ -287,8 +289,8 @@ __device__ inline bool trailing_update_tc(float2 *__restrict__ A, int N, int ld,
                 }
             }
             tc::fence_before_sync();
-            __syncthreads();
-            if (err) return false;
+            // a timed-out wait ends the update in every thread together
+            if (__syncthreads_or(err)) return false;
         }
     }
     return true;
@@ -491,6 +493,641 @@ __global__ void __launch_bounds__(NT, 1)
     tile_teardown(t, tbase);
 }
 
+// =================================================== mixed-precision sweep
+// Storage of one job of a wave (offsets from MixedLayout, the same for every
+// job):
+//   tiles  Nz matrices in split-fp16 tile form: slot b = gR(b) of the sweep
+//          (b = 1 .. Nz-1, 0-based slices), slot 0 = G_11.  Each matrix is
+//          the raw Gauss-Jordan result R (inv(S)(r, c) = R(prow[r], iprow[c]))
+//          cut into tiles of TM rows x KB columns; tile (rt, kc) is 32 KB at
+//          (rt * nkc + kc) * 32 KB: four planes (re hi, re lo, im hi, im lo)
+//          of fp16 in the K-major core-matrix layout, R(t, k) scaled by
+//          2^-rexp[t] (one exponent per row over all columns)
+//   prow   [Nz][N] the pivot rows of each slot, rexp [Nz][N] the row exponents
+//   x      [Nz][ncap][N] x0: column j = G(:, 1) times the open channel oc[j]
+//   rc     [Nz][ncap][N] the FP64 residual r, then the correction stage c
+//   d      [2][ncap][N] the correction, two slices at a time
+//   oc     [ncap] open channels of the right lead, then n_open
+// complex FP32 everywhere (column j of a slice at j * N).
+struct MixedLayout {
+    int N, Nz, ld, ntr, nkc, ncap;
+    size_t mat_bytes;  // one matrix in split tiles
+    size_t off_tiles, off_prow, off_rexp, off_x, off_rc, off_d, off_oc, job_bytes;
+    size_t scratch_bytes;  // per CTA
+};
+constexpr size_t TILE_BYTES = 4 * (size_t)TM * KB * 2;  // 32 KB
+inline size_t align256(size_t x) { return (x + 255) / 256 * 256; }
+MixedLayout make_layout(int N, int Nz, int ld, int ncap) {
+    MixedLayout L;
+    L.N = N; L.Nz = Nz; L.ld = ld; L.ncap = ncap;
+    L.ntr = (N + TM - 1) / TM;
+    L.nkc = (N + KB - 1) / KB;
+    L.mat_bytes = (size_t)L.ntr * L.nkc * TILE_BYTES;
+    size_t o = 0;
+    L.off_tiles = o; o = align256(o + (size_t)Nz * L.mat_bytes);
+    L.off_prow = o; o = align256(o + (size_t)Nz * N * 4);
+    L.off_rexp = o; o = align256(o + (size_t)Nz * N * 4);
+    L.off_x = o; o = align256(o + (size_t)Nz * ncap * N * 8);
+    L.off_rc = o; o = align256(o + (size_t)Nz * ncap * N * 8);
+    L.off_d = o; o = align256(o + (size_t)2 * ncap * N * 8);
+    L.off_oc = o; o = align256(o + (size_t)(ncap + 4) * 4);
+    L.job_bytes = o;
+    // sweep: two working matrices; passes: the B operand of one product in split tiles
+    L.scratch_bytes = align256(std::max((size_t)2 * N * ld * 8, (size_t)L.nkc * ncap * 256));
+    return L;
+}
+
+struct MixedArgs {
+    negf::Geo g;
+    MixedLayout L;
+    const double *E;       // energies
+    const int2 *jobs;      // per wave slot: (energy index, k-point)
+    int njobs;
+    unsigned char *jobmem; // njobs job regions
+    unsigned char *scratch;
+    double *tau, *dnorm, *xnorm;
+    int *status;           // 0 ok; > 0 zero pivot (info); -1 too many open channels; -2 tensor wait timed out
+};
+
+// The job's N-sized vectors used by negf::job_vectors / d_element / open_cols.
+__host__ __device__ inline size_t job_smem_bytes(int N) {
+    const int n4 = rup(N, 4), n2 = rup(N, 2);
+    size_t b = 3 * (size_t)n4 * 4 + 16;
+    b = (b + 15) / 16 * 16;
+    b += 2 * (size_t)n2 * 16 + 2 * (size_t)n2 * 8;
+    return (b + 127) / 128 * 128;
+}
+__device__ inline negf::Smem carve_job(unsigned char *base, int N) {
+    negf::Smem s{};
+    const int n4 = rup(N, 4), n2 = rup(N, 2);
+    s.nx = (int *)base;
+    s.ny = s.nx + n4;
+    s.rows = s.ny + n4;
+    s.nrows = s.rows + n4;
+    size_t off = ((size_t)3 * n4 * 4 + 16 + 15) / 16 * 16;
+    s.sigL = (double2 *)(base + off);
+    s.sigR = s.sigL + n2;
+    s.gL = (double *)(s.sigR + n2);
+    s.gR = s.gL + n2;
+    return s;
+}
+
+// M = round32(D_k - inv(prev)) with D_k generated in FP64 from the V table
+// (negf::d_element, grid.f90:236-333) and inv(prev)(i, j) = R(prow[t] ...)
+// read through the previous inverse's permutations: thread t reads row t of
+// R (coalesced) and writes row iprow[t] of M.
+__device__ inline void form_mixed(float2 *__restrict__ M, const negf::Geo &g, const negf::Smem &js,
+                                  const GjSmem &s, int k, double2 E, int ik, const float2 *__restrict__ R) {
+    const int N = g.N, ld = g.ld;
+    const double2 *vs = g.vhat + (size_t)g.W * g.H * k;
+    for (int j0 = 0; j0 < N; j0 += 4) {
+        for (int t = threadIdx.x; t < N; t += NT) {
+            const int i = R ? s.iprow[t] : t;
+            double2 d[4];
+            float2 r[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int j = j0 + q;
+                d[q] = make_double2(0.0, 0.0);
+                r[q] = make_float2(0.f, 0.f);
+                if (j < N) {
+                    d[q] = negf::d_element(g, js, vs, k, E, ik, i, j, js.nx[j], js.ny[j]);
+                    if (R) r[q] = R[t + (size_t)ld * s.iprow[j]];
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (j0 + q < N) M[i + (size_t)ld * (j0 + q)] = make_float2((float)(d[q].x - (double)r[q].x),
+                                                                           (float)(d[q].y - (double)r[q].y));
+        }
+    }
+}
+
+// Stores the raw inverse R (working layout) as the split tiles of slot b,
+// with its pivot rows and row exponents.
+__device__ inline void store_factor(const float2 *__restrict__ R, const MixedLayout &L, const GjSmem &s,
+                                    int *rexpN, unsigned char *jm, int b) {
+    const int N = L.N, ld = L.ld, tid = threadIdx.x;
+    int *prow_g = (int *)(jm + L.off_prow) + (size_t)b * N;
+    int *rexp_g = (int *)(jm + L.off_rexp) + (size_t)b * N;
+    unsigned char *tiles = jm + L.off_tiles + (size_t)b * L.mat_bytes;
+    for (int t = tid; t < N; t += NT) {
+        float m = 0.0f;
+        for (int j = 0; j < N; ++j) {
+            const float2 v = R[t + (size_t)ld * j];
+            m = fmaxf(m, fmaxf(fabsf(v.x), fabsf(v.y)));
+        }
+        const int e = tc::scale_exponent(m);
+        rexpN[t] = e;
+        rexp_g[t] = e;
+        prow_g[t] = s.prow[t];
+    }
+    __syncthreads();
+    const int r = tid % TM, h = tid / TM;
+    for (int rt = 0; rt < L.ntr; ++rt) {
+        const int row = rt * TM + r;
+        const float sc = tc::exp2i(row < N ? -rexpN[row] : 0);
+        for (int kc = 0; kc < L.nkc; ++kc) {
+            unsigned char *tile = tiles + ((size_t)rt * L.nkc + kc) * TILE_BYTES;
+#pragma unroll
+            for (int g2 = 0; g2 < 2; ++g2) {
+                const int kg = 2 * h + g2;
+                float2 v[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const int col = kc * KB + 8 * kg + q;
+                    float2 x = (row < N && col < N) ? R[row + (size_t)ld * col] : make_float2(0.f, 0.f);
+                    v[q] = make_float2(x.x * sc, x.y * sc);
+                }
+                __align__(16) __half rh[8], rl[8], ih[8], il[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const tc::Split2 a = tc::split_fp16(v[q].x), bb = tc::split_fp16(v[q].y);
+                    rh[q] = a.hi; rl[q] = a.lo; ih[q] = bb.hi; il[q] = bb.lo;
+                }
+                const uint32_t off = tc::kmajor_offset(r, 8 * kg, KB);
+                *(uint4 *)(tile + 0 * (TM * KB * 2) + off) = *(const uint4 *)rh;
+                *(uint4 *)(tile + 1 * (TM * KB * 2) + off) = *(const uint4 *)rl;
+                *(uint4 *)(tile + 2 * (TM * KB * 2) + off) = *(const uint4 *)ih;
+                *(uint4 *)(tile + 3 * (TM * KB * 2) + off) = *(const uint4 *)il;
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// One CTA per job (persistent over the wave): the right-connected sweep
+// gR(b) = inv(D_b - gR(b+1)), b = Nz-1 .. 1, then G_11 = inv(D_0 - gR(1))
+// (math_kernel.f90:81-118), every inverse stored as a split-tile factor, and
+// x0(:, j) = G_11(:, oc[j]) for the open channels oc of the right lead.
+template <int RPT>
+__global__ void __launch_bounds__(NT, 1) k_mixed_sweep(MixedArgs a) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const MixedLayout &L = a.L;
+    const negf::Geo &g = a.g;
+    const int N = L.N, Nz = L.Nz, ld = L.ld, tid = threadIdx.x;
+    GjSmem s = carve_gj(smem, N);
+    size_t off = gj_smem_bytes(N);
+    TileSmem t = carve_tile(smem + off);
+    off += (tile_smem_bytes() + 127) / 128 * 128;
+    negf::Smem js = carve_job(smem + off, N);
+    off += job_smem_bytes(N);
+    int *rexpN = (int *)(smem + off);
+    for (int i = tid; i < N; i += NT) { js.nx[i] = g.nx[i]; js.ny[i] = g.ny[i]; }
+    const uint32_t tbase = tile_setup(t);
+    uint32_t ph = 0;
+    float2 *W0 = (float2 *)(a.scratch + (size_t)blockIdx.x * L.scratch_bytes);
+    float2 *W1 = W0 + (size_t)N * ld;
+    for (int w = blockIdx.x; w < a.njobs; w += gridDim.x) {
+        const int2 jb = a.jobs[w];
+        const double e = a.E[jb.x];
+        const double2 E = make_double2(e, g.eta);
+        unsigned char *jm = a.jobmem + (size_t)w * L.job_bytes;
+        negf::job_vectors(g, js, E, e, jb.y);
+        __syncthreads();
+        negf::open_cols(N, js, js.gR);
+        __syncthreads();
+        const int nopen = *js.nrows;
+        int *oc = (int *)(jm + L.off_oc);
+        if (nopen > L.ncap) {
+            if (tid == 0) a.status[w] = -1;
+            __syncthreads();
+            continue;
+        }
+        for (int j = tid; j < nopen; j += NT) oc[j] = js.rows[j];
+        if (tid == 0) oc[L.ncap] = nopen;
+        float2 *cur = W0, *oth = W1;
+        int info = 0, err = 0;
+        for (int b = Nz - 1; b >= 0; --b) {
+            form_mixed(oth, g, js, s, b, E, jb.y, b < Nz - 1 ? cur : nullptr);
+            __syncthreads();
+            float2 *tt = cur; cur = oth; oth = tt;
+            const int r = gj_invert_mixed<RPT>(cur, N, ld, s, t, tbase, ph, &err);
+            if (r && !info) info = r;
+            if (err) break;  // uniform: set from __syncthreads_or
+            store_factor(cur, L, s, rexpN, jm, b);
+        }
+        if (!err) {
+            float2 *x0 = (float2 *)(jm + L.off_x);  // slice 0
+            for (int j = 0; j < L.ncap; ++j) {
+                const int jc = j < nopen ? s.iprow[oc[j]] : -1;
+                for (int r = tid; r < N; r += NT)
+                    x0[r + (size_t)N * j] = jc >= 0 ? cur[s.prow[r] + (size_t)ld * jc] : make_float2(0.f, 0.f);
+            }
+        }
+        if (tid == 0) a.status[w] = err ? -2 : info;
+        __syncthreads();
+        if (err) break;
+    }
+    tile_teardown(t, tbase);
+}
+
+// ======================================================= refinement passes
+// y = alpha * (gR(slot) v) + wadd with gR(slot) applied from its split-tile
+// factor: gR(r, c) = R(prow[r], iprow[c]), so with v_p(k) = v(prow[k]) and
+// z = R v_p, y(iprow[t]) = alpha z(t) + wadd(iprow[t]).  v = v1 - v2 (v2 may be
+// null).  The B operand v_p is converted once per product into split tiles
+// (one exponent per column over all N rows) in the CTA's scratch; then for
+// each 128-row tile of R the K chunks stream through a 3-stage pipeline of
+// bulk copies (A: one 32 KB tile, B: one chunk) into tcgen05 MMAs.
+enum PassMode { PASS_X0 = 0, PASS_BACK = 1, PASS_CORR = 2 };
+constexpr int PSTAGES = 3;
+
+struct PassSmem {
+    unsigned char *stA[PSTAGES];
+    unsigned char *stB[PSTAGES];
+    int *prow, *iprow, *rexp, *cexp;
+    uint64_t *full, *empty, *accf;
+    uint32_t *tslot;
+    double *red;
+};
+__host__ __device__ inline size_t pass_smem_bytes(int N, int ncap) {
+    size_t b = PSTAGES * (TILE_BYTES + (size_t)ncap * 256);
+    b += 3 * (size_t)rup(N, 4) * 4 + (size_t)ncap * 4;
+    b += (2 * PSTAGES + 1) * 8 + 16 + NWARP * 8 * 2;
+    b += job_smem_bytes(N);
+    return (b + 127) / 128 * 128;
+}
+__device__ inline PassSmem carve_pass(unsigned char *base, int N, int ncap) {
+    PassSmem p;
+    unsigned char *q = base;
+    for (int s = 0; s < PSTAGES; ++s) { p.stA[s] = q; q += TILE_BYTES; }
+    for (int s = 0; s < PSTAGES; ++s) { p.stB[s] = q; q += (size_t)ncap * 256; }
+    p.prow = (int *)q; q += (size_t)rup(N, 4) * 4;
+    p.iprow = (int *)q; q += (size_t)rup(N, 4) * 4;
+    p.rexp = (int *)q; q += (size_t)rup(N, 4) * 4;
+    p.cexp = (int *)q; q += (size_t)ncap * 4;
+    q = (unsigned char *)(((uintptr_t)q + 15) & ~(uintptr_t)15);
+    p.full = (uint64_t *)q; q += PSTAGES * 8;
+    p.empty = (uint64_t *)q; q += PSTAGES * 8;
+    p.accf = (uint64_t *)q; q += 8;
+    p.tslot = (uint32_t *)q; q += 8;
+    p.red = (double *)q;
+    return p;
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(tc::smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     tc::smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(tc::smem_u32(bar))
+                 : "memory");
+}
+
+// MMAs of one staged K chunk with N = npad output columns (thread 0).
+__device__ inline void issue_pass_chunk(const unsigned char *sA, const unsigned char *sB, int npad,
+                                        uint32_t tbase, bool first) {
+    constexpr uint32_t SBO = (KB / 8) * 128, LBO = 128;
+    const uint32_t id = tc::idesc_f16(TM, npad, false), idn = tc::idesc_f16(TM, npad, true);
+    const uint32_t dre = tbase, dim = tbase + npad;
+    const uint32_t a0 = tc::smem_u32(sA), b0 = tc::smem_u32(sB);
+    const uint32_t aplane = TM * KB * 2, bplane = npad * KB * 2;
+    const int pa[3] = {0, 0, 1}, pb[3] = {0, 1, 0};
+#pragma unroll
+    for (int ks = 0; ks < KB / 16; ++ks) {
+        const uint32_t koff = ks * 256;
+#pragma unroll
+        for (int sp = 0; sp < 3; ++sp) {
+            const uint64_t are = tc::sdesc(a0 + (0 + pa[sp]) * aplane + koff, LBO, SBO);
+            const uint64_t aim = tc::sdesc(a0 + (2 + pa[sp]) * aplane + koff, LBO, SBO);
+            const uint64_t bre = tc::sdesc(b0 + (0 + pb[sp]) * bplane + koff, LBO, SBO);
+            const uint64_t bim = tc::sdesc(b0 + (2 + pb[sp]) * bplane + koff, LBO, SBO);
+            const uint32_t acc = (first && ks == 0 && sp == 0) ? 0u : 1u;
+            tc::mma_f16(dre, are, bre, id, acc);
+            tc::mma_f16(dre, aim, bim, idn, 1u);
+            tc::mma_f16(dim, are, bim, id, acc);
+            tc::mma_f16(dim, aim, bre, id, 1u);
+        }
+    }
+}
+
+// One product of a pass (see above).  Returns false on a tensor wait timeout
+// (uniform over the CTA).  phases: bit s = full[s], bit 8+s = empty[s], bit
+// 16 = accf (thread 0 tracks full/empty, every thread accf).
+__device__ bool pass_product(const MixedLayout &L, const PassSmem &p, unsigned char *jm, unsigned char *bscr,
+                             int slot, const float2 *__restrict__ v1, const float2 *__restrict__ v2,
+                             float2 *__restrict__ out, float alpha, const float2 *__restrict__ wadd, int nopen,
+                             int npad, uint32_t tbase, uint32_t &phases) {
+    const int N = L.N, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int *prow_g = (const int *)(jm + L.off_prow) + (size_t)slot * N;
+    const int *rexp_g = (const int *)(jm + L.off_rexp) + (size_t)slot * N;
+    const unsigned char *tiles = jm + L.off_tiles + (size_t)slot * L.mat_bytes;
+    for (int k = tid; k < N; k += NT) {
+        const int pr = prow_g[k];
+        p.prow[k] = pr;
+        p.iprow[pr] = k;
+        p.rexp[k] = rexp_g[k];
+    }
+    __syncthreads();
+    // column exponents of v_p (= of v: a row permutation)
+    for (int j = warp; j < npad; j += NWARP) {
+        float m = 0.0f;
+        if (j < nopen)
+            for (int k = lane; k < N; k += 32) {
+                float2 x = v1[k + (size_t)N * j];
+                if (v2) { const float2 y = v2[k + (size_t)N * j]; x.x -= y.x; x.y -= y.y; }
+                m = fmaxf(m, fmaxf(fabsf(x.x), fabsf(x.y)));
+            }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (lane == 0) p.cexp[j] = tc::scale_exponent(m);
+    }
+    __syncthreads();
+    // B operand split tiles: chunk kc at kc * npad * 256 B, planes of npad * KB fp16
+    const uint32_t bplane = npad * KB * 2;
+    for (int item = tid; item < L.nkc * npad * 4; item += NT) {
+        const int g4 = item & 3, j = (item >> 2) % npad, kc = (item >> 2) / npad;
+        const float sc = tc::exp2i(-p.cexp[j]);
+        float2 v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int k = kc * KB + 8 * g4 + q;
+            float2 x = make_float2(0.f, 0.f);
+            if (k < N && j < nopen) {
+                const int pr = p.prow[k];
+                x = v1[pr + (size_t)N * j];
+                if (v2) { const float2 y = v2[pr + (size_t)N * j]; x.x -= y.x; x.y -= y.y; }
+            }
+            v[q] = make_float2(x.x * sc, x.y * sc);
+        }
+        __align__(16) __half rh[8], rl[8], ih[8], il[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const tc::Split2 a = tc::split_fp16(v[q].x), b = tc::split_fp16(v[q].y);
+            rh[q] = a.hi; rl[q] = a.lo; ih[q] = b.hi; il[q] = b.lo;
+        }
+        unsigned char *dst = bscr + (size_t)kc * npad * 256 + tc::kmajor_offset(j, 8 * g4, KB);
+        *(uint4 *)(dst + 0 * bplane) = *(const uint4 *)rh;
+        *(uint4 *)(dst + 1 * bplane) = *(const uint4 *)rl;
+        *(uint4 *)(dst + 2 * bplane) = *(const uint4 *)ih;
+        *(uint4 *)(dst + 3 * bplane) = *(const uint4 *)il;
+    }
+    // the bulk copies (async proxy) read what these generic stores wrote
+    asm volatile("fence.proxy.async.global;\n" ::: "memory");
+    __syncthreads();
+    const uint32_t bbytes = (uint32_t)npad * 256;
+    int err = 0;
+    for (int rt = 0; rt < L.ntr; ++rt) {
+        if (tid == 0) {
+            tc::fence_after_sync();
+            const unsigned char *arow = tiles + (size_t)rt * L.nkc * TILE_BYTES;
+            auto produce = [&](int kc) {
+                const int st = kc % PSTAGES;
+                mbar_expect_tx(&p.full[st], (uint32_t)TILE_BYTES + bbytes);
+                bulk_g2s(p.stA[st], arow + (size_t)kc * TILE_BYTES, (uint32_t)TILE_BYTES, &p.full[st]);
+                bulk_g2s(p.stB[st], bscr + (size_t)kc * bbytes, bbytes, &p.full[st]);
+            };
+            const int nk = L.nkc;
+            for (int kc = 0; kc < nk && kc < PSTAGES; ++kc) produce(kc);
+            for (int kc = 0; kc < nk && !err; ++kc) {
+                const int st = kc % PSTAGES;
+                if (!tc::mbar_wait(&p.full[st], (phases >> st) & 1u, WAIT_LIMIT)) { err = 1; break; }
+                phases ^= 1u << st;
+                tc::fence_after_sync();
+                issue_pass_chunk(p.stA[st], p.stB[st], npad, tbase, kc == 0);
+                tc::mma_commit(&p.empty[st]);
+                // refill the stage of chunk kc-1 (its MMAs ran ahead of chunk kc's)
+                if (kc >= 1 && kc - 1 + PSTAGES < nk) {
+                    const int s1 = (kc - 1) % PSTAGES;
+                    if (!tc::mbar_wait(&p.empty[s1], (phases >> (8 + s1)) & 1u, WAIT_LIMIT)) { err = 1; break; }
+                    phases ^= 1u << (8 + s1);
+                    produce(kc - 1 + PSTAGES);
+                }
+            }
+            // empty barriers of the chunks whose refill wait was skipped
+            for (int kc = max(0, nk - PSTAGES); kc < nk && !err; ++kc) {
+                if (kc == 0 && nk > PSTAGES) continue;
+                const int st = kc % PSTAGES;
+                if (!tc::mbar_wait(&p.empty[st], (phases >> (8 + st)) & 1u, WAIT_LIMIT)) { err = 1; break; }
+                phases ^= 1u << (8 + st);
+            }
+            tc::mma_commit(p.accf);
+        }
+        if (!tc::mbar_wait(p.accf, (phases >> 16) & 1u, WAIT_LIMIT)) err = 1;
+        phases ^= 1u << 16;
+        tc::fence_after_sync();
+        // epilogue: tile row r -> matrix row t of R -> output row iprow[t]
+        const int r = 32 * (warp & 3) + lane, t = rt * TM + r;
+        const bool rv = t < N;
+        const int i = rv ? p.iprow[t] : 0;
+        const int er = rv ? p.rexp[t] : 0;
+        for (int c16 = warp >> 2; c16 < npad / 16; c16 += 2) {
+            float re[16], im[16];
+            {
+                const uint32_t lb = (uint32_t)(32 * (warp & 3)) << 16;
+                tc::tmem_ld16(tbase + lb + c16 * 16, re);
+                tc::tmem_ld16(tbase + lb + npad + c16 * 16, im);
+                tc::tmem_wait_ld();
+            }
+            if (rv) {
+#pragma unroll
+                for (int q = 0; q < 16; ++q) {
+                    const int j = c16 * 16 + q;
+                    float2 y = make_float2(0.f, 0.f);
+                    if (j < nopen) {
+                        const int ex = er + p.cexp[j];
+                        y = make_float2(alpha * ldexpf(re[q], ex), alpha * ldexpf(im[q], ex));
+                        if (wadd) { const float2 wv = wadd[i + (size_t)N * j]; y.x += wv.x; y.y += wv.y; }
+                    }
+                    if (j < L.ncap) out[i + (size_t)N * j] = y;
+                }
+            }
+        }
+        tc::fence_before_sync();
+        if (__syncthreads_or(err)) return false;
+    }
+    return true;
+}
+
+// One CTA per job: PASS_X0 x0(b) = -gR(b) x0(b-1), b = 1..Nz-1 (x0(0) from the
+// sweep); PASS_BACK c(Nz-1) = r(Nz-1), c(b) = r(b) - gR(b+1) c(b+1) in place
+// of r; PASS_CORR d(0) = G_11 c(0), d(b) = gR(b) (c(b) - d(b-1)), then
+// tau = sum_ij gamma_L,i gamma_R,oc_j |2 dz^2 (x0 + d)(Nz-1)(i, j)|^2 in FP64
+// (grid.f90:362-383) and the norms of d and x0 + d on the rows that enter it.
+__global__ void __launch_bounds__(NT, 1) k_mixed_pass(MixedArgs a, int mode) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const MixedLayout &L = a.L;
+    const int N = L.N, Nz = L.Nz, tid = threadIdx.x;
+    PassSmem p = carve_pass(smem, N, L.ncap);
+    negf::Smem js = carve_job(smem + pass_smem_bytes(N, L.ncap) - job_smem_bytes(N), N);
+    uint32_t ncols = 32;
+    while (ncols < 2u * L.ncap) ncols <<= 1;
+    if (tid < 32) tc::tmem_alloc(p.tslot, ncols);
+    if (tid == 0) {
+        for (int s = 0; s < PSTAGES; ++s) { tc::mbar_init(&p.full[s], 1); tc::mbar_init(&p.empty[s], 1); }
+        tc::mbar_init(p.accf, 1);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tbase = *p.tslot;
+    uint32_t phases = 0;
+    unsigned char *bscr = a.scratch + (size_t)blockIdx.x * L.scratch_bytes;
+    const size_t sl = (size_t)L.ncap * N;  // float2 per slice of a vector array
+    bool ok = true;
+    for (int w = blockIdx.x; w < a.njobs && ok; w += gridDim.x) {
+        if (a.status[w] != 0) continue;
+        unsigned char *jm = a.jobmem + (size_t)w * L.job_bytes;
+        const int nopen = ((const int *)(jm + L.off_oc))[L.ncap];
+        const int npad = max(16, rup(nopen, 16));
+        float2 *x = (float2 *)(jm + L.off_x), *rc = (float2 *)(jm + L.off_rc), *d = (float2 *)(jm + L.off_d);
+        if (mode == PASS_X0) {
+            for (int b = 1; b < Nz && ok; ++b)
+                ok = pass_product(L, p, jm, bscr, b, x + (b - 1) * sl, nullptr, x + b * sl, -1.f, nullptr, nopen,
+                                  npad, tbase, phases);
+        } else if (mode == PASS_BACK) {
+            for (int b = Nz - 2; b >= 0 && ok; --b)
+                ok = pass_product(L, p, jm, bscr, b + 1, rc + (b + 1) * sl, nullptr, rc + b * sl, -1.f, rc + b * sl,
+                                  nopen, npad, tbase, phases);
+        } else {
+            ok = pass_product(L, p, jm, bscr, 0, rc, nullptr, d, 1.f, nullptr, nopen, npad, tbase, phases);
+            for (int b = 1; b < Nz && ok; ++b)
+                ok = pass_product(L, p, jm, bscr, b, rc + b * sl, d + ((b - 1) & 1) * sl, d + (b & 1) * sl, 1.f,
+                                  nullptr, nopen, npad, tbase, phases);
+            if (ok) {
+                // tau of x0 + d at the last slice, FP64
+                const negf::Geo &g = a.g;
+                const int2 jb = a.jobs[w];
+                const double e = a.E[jb.x];
+                for (int i = tid; i < N; i += NT) { js.nx[i] = g.nx[i]; js.ny[i] = g.ny[i]; }
+                __syncthreads();
+                negf::job_vectors(g, js, make_double2(e, g.eta), e, jb.y);
+                __syncthreads();
+                const int *oc = (const int *)(jm + L.off_oc);
+                const float2 *xl = x + (size_t)(Nz - 1) * sl, *dl = d + ((Nz - 1) & 1) * sl;
+                const double c2 = g.c2;
+                double tau = 0.0, dn = 0.0, xn = 0.0;
+                for (int e2 = tid; e2 < N * nopen; e2 += NT) {
+                    const int i = e2 % N, j = e2 / N;
+                    const double gl = js.gL[i];
+                    if (gl == 0.0) continue;
+                    const float2 a0 = xl[i + (size_t)N * j], a1 = dl[i + (size_t)N * j];
+                    const double gx = ((double)a0.x + (double)a1.x) * c2, gy = ((double)a0.y + (double)a1.y) * c2;
+                    tau += gl * js.gR[oc[j]] * (gx * gx + gy * gy);
+                    dn += (double)a1.x * a1.x + (double)a1.y * a1.y;
+                    xn += ((double)a0.x + a1.x) * ((double)a0.x + a1.x) + ((double)a0.y + a1.y) * ((double)a0.y + a1.y);
+                }
+                // fixed-order block reduction (bitwise repeatable)
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    tau += __shfl_xor_sync(0xffffffffu, tau, o);
+                    dn += __shfl_xor_sync(0xffffffffu, dn, o);
+                    xn += __shfl_xor_sync(0xffffffffu, xn, o);
+                }
+                if ((tid & 31) == 0) {
+                    p.red[(tid >> 5)] = tau;
+                    p.red[NWARP + (tid >> 5)] = dn;
+                }
+                __syncthreads();
+                if (tid == 0) {
+                    double T = 0, D = 0;
+                    for (int q = 0; q < NWARP; ++q) { T += p.red[q]; D += p.red[NWARP + q]; }
+                    a.tau[w] = T;
+                    a.dnorm[w] = sqrt(D);
+                }
+                __syncthreads();
+                if ((tid & 31) == 0) p.red[tid >> 5] = xn;
+                __syncthreads();
+                if (tid == 0) {
+                    double X = 0;
+                    for (int q = 0; q < NWARP; ++q) X += p.red[q];
+                    a.xnorm[w] = sqrt(X);
+                }
+                __syncthreads();
+            }
+        }
+        if (!ok && tid == 0) a.status[w] = -2;
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (tid < 32) tc::tmem_dealloc(tbase, ncols);
+}
+
+// FP64 residual of the block-tridiagonal system for x0, one CTA per (slice b,
+// job): r(b) = E_1 delta_b0 - x0(b-1) - D_b x0(b) - x0(b+1), D_b generated in
+// FP64 (negf::d_element) and the product on the FP64 tensor cores (DMMA
+// warp tiles of negf::WarpAcc), 64 x 64 output tiles, K in chunks of 16.
+__global__ void __launch_bounds__(NT, 2) k_mixed_residual(MixedArgs a) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const MixedLayout &L = a.L;
+    const negf::Geo &g = a.g;
+    const int N = L.N, Nz = L.Nz, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int b = blockIdx.x, w = blockIdx.y;
+    if (a.status[w] != 0) return;
+    constexpr int KC = negf::KC, AP = negf::AP, BP = negf::BP;
+    double2 *sA = (double2 *)smem;           // [KC][AP]
+    double2 *sB = sA + KC * AP;              // [KC][BP]
+    negf::Smem js = carve_job(smem + (size_t)KC * (AP + BP) * 16, N);
+    unsigned char *jm = a.jobmem + (size_t)w * L.job_bytes;
+    const int *oc = (const int *)(jm + L.off_oc);
+    const int nopen = oc[L.ncap];
+    const int npad = max(16, rup(nopen, 16));
+    const int2 jb = a.jobs[w];
+    const double e = a.E[jb.x];
+    const double2 E = make_double2(e, g.eta);
+    for (int i = tid; i < N; i += NT) { js.nx[i] = g.nx[i]; js.ny[i] = g.ny[i]; }
+    __syncthreads();
+    negf::job_vectors(g, js, E, e, jb.y);
+    __syncthreads();
+    const size_t sl = (size_t)L.ncap * N;
+    const float2 *x = (const float2 *)(jm + L.off_x);
+    const float2 *xb = x + b * sl;
+    float2 *out = (float2 *)(jm + L.off_rc) + b * sl;
+    const double2 *vs = g.vhat + (size_t)g.W * g.H * b;
+    const int wm0 = (warp >> 2) * negf::WM, wn0 = (warp & 3) * negf::WN;
+    for (int I0 = 0; I0 < N; I0 += negf::CM) {
+        for (int J0 = 0; J0 < npad; J0 += negf::CN) {
+            const bool active = (I0 + wm0 < N) && (J0 + wn0 < npad);
+            negf::WarpAcc acc;
+            acc.zero();
+            for (int k0 = 0; k0 < N; k0 += KC) {
+                for (int e2 = tid; e2 < KC * negf::CM; e2 += NT) {
+                    const int kk = e2 / negf::CM, ii = e2 % negf::CM, i = I0 + ii, k = k0 + kk;
+                    sA[kk * AP + ii] = (i < N && k < N) ? negf::d_element(g, js, vs, b, E, jb.y, i, k, js.nx[k], js.ny[k])
+                                                        : make_double2(0.0, 0.0);
+                }
+                for (int e2 = tid; e2 < KC * negf::CN; e2 += NT) {
+                    const int jj = e2 / KC, kk = e2 % KC, j = J0 + jj, k = k0 + kk;
+                    float2 v = (j < nopen && k < N) ? xb[k + (size_t)N * j] : make_float2(0.f, 0.f);
+                    sB[kk * BP + jj] = make_double2(v.x, v.y);
+                }
+                __syncthreads();
+                if (active) {
+#pragma unroll
+                    for (int kb = 0; kb < KC; kb += 4) acc.step(sA, AP, wm0, sB, BP, wn0, kb, lane);
+                }
+                __syncthreads();
+            }
+            if (active) {
+#pragma unroll
+                for (int m = 0; m < 4; ++m) {
+                    const int i = I0 + wm0 + 8 * m + (lane >> 2);
+#pragma unroll
+                    for (int n = 0; n < 2; ++n)
+#pragma unroll
+                        for (int e3 = 0; e3 < 2; ++e3) {
+                            const int j = J0 + wn0 + 8 * n + 2 * (lane & 3) + e3;
+                            if (i < N && j < L.ncap) {
+                                double rx = 0.0, ry = 0.0;
+                                if (j < nopen) {
+                                    rx = -acc.re[m][n][e3];
+                                    ry = -acc.im[m][n][e3];
+                                    if (b > 0) { const float2 v = x[(b - 1) * sl + i + (size_t)N * j]; rx -= v.x; ry -= v.y; }
+                                    if (b + 1 < Nz) { const float2 v = x[(b + 1) * sl + i + (size_t)N * j]; rx -= v.x; ry -= v.y; }
+                                    if (b == 0 && i == oc[j]) rx += 1.0;
+                                }
+                                out[i + (size_t)N * j] = make_float2((float)rx, (float)ry);
+                            }
+                        }
+                }
+            }
+        }
+    }
+}
+
 #define CKM(x)                                                                             \
     do {                                                                                   \
         cudaError_t e_ = (x);                                                              \
@@ -552,4 +1189,204 @@ extern "C" int negf_tc_inverse_check(const float *d_A, int32_t N, int32_t nmat, 
     cudaFree(work);
     cudaFree(d_status);
     return h ? NEGF_ERR_CUDA : NEGF_OK;
+}
+
+// ======================================================================= host
+namespace {
+
+negf::Geo mixed_geo(const negf_ctx *c) {
+    negf::Geo g;
+    g.N = c->N; g.Nz = c->Nz; g.ld = c->ld;
+    g.ngx = c->ngx; g.ngy = c->ngy; g.W = 2 * c->ngx + 1; g.H = 2 * c->ngy + 1;
+    g.nk = c->nk;
+    g.vhat = c->d_vhat; g.nx = c->d_nx; g.ny = c->d_ny;
+    g.ax = c->d_ax; g.ay = c->d_ay; g.kw = c->d_kw;
+    g.delta = c->Lz / c->Nz;
+    g.c2 = 2 * (g.delta * g.delta);
+    g.V_L = c->V_L; g.V_R = c->V_R; g.eta = c->eta;
+    g.lead_model = c->lead_model;
+    return g;
+}
+
+constexpr double PI_M = 3.141592653589793;  // global.f90:28
+
+// |k+G_i|^2 / 2 for mode i at k-point ik (grid.f90:258)
+double kinetic(const negf_ctx *c, int ik, int i) {
+    const double ax = (double)(2 * c->nx[i]) * PI_M / c->Lx + c->kpt[3 * ik];
+    const double ay = (double)(2 * c->ny[i]) * PI_M / c->Ly + c->kpt[3 * ik + 1];
+    return (ax * ax + ay * ay) / 2;
+}
+
+template <typename K>
+int set_smem(K kern, size_t bytes) {
+    CKM(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    return 0;
+}
+
+}  // namespace
+
+int negf_internal_mixed(negf_ctx *c, const double *h_E, const double *d_E, int nE, double *h_tau_jobs,
+                        int *h_info, double *device_ms) {
+    const int nk = c->nk, njobs = nE * nk, N = c->N, Nz = c->Nz;
+    negf_mixed_stats stats{};
+    stats.n_jobs = njobs;
+    *device_ms = 0;
+    if (N > 1023) return NEGF_ERR_UNSUPPORTED;
+    const negf_mixed_policy pol = c->mixed_policy;
+    cudaStream_t st = c->stream;
+
+    // ---- policy: which jobs run in FP64 from the start
+    std::vector<int> f_ie, f_ik, m_jobs;
+    std::vector<int> nopen_est(njobs, 0);
+    int nmax = 0;
+    for (int ik = 0; ik < nk; ++ik) {
+        std::vector<double> kin(N);
+        for (int i = 0; i < N; ++i) kin[i] = kinetic(c, ik, i);
+        for (int ie = 0; ie < nE; ++ie) {
+            const int q = ik * nE + ie;
+            const double E = h_E[ie];
+            bool fp64 = c->eta < pol.eta_fp64_below;
+            int n = 0;
+            for (int i = 0; i < N; ++i) {
+                if (pol.threshold_window > 0 &&
+                    (std::fabs(E - (c->V_L + kin[i])) < pol.threshold_window ||
+                     std::fabs(E - (c->V_R + kin[i])) < pol.threshold_window))
+                    fp64 = true;
+                // open channel of the right lead (gamma_R != 0, grid.f90:355-360), with a
+                // margin for rounding at the threshold
+                if (2 * (E - c->V_R) - 2 * kin[i] > -1e-12 * (std::fabs(E) + 2 * kin[i])) ++n;
+            }
+            if (n > 127) fp64 = true;
+            nopen_est[q] = n;
+            if (fp64) {
+                f_ie.push_back(ie);
+                f_ik.push_back(ik);
+                stats.n_fp64_policy++;
+            } else {
+                m_jobs.push_back(q);
+                nmax = std::max(nmax, n);
+            }
+        }
+    }
+    int rc = 0;
+    double mixed_ms = 0;
+    if (!m_jobs.empty()) {
+        const int ncap = std::max(16, rup(nmax, 16));
+        const MixedLayout L = make_layout(N, Nz, c->ld, ncap);
+        const size_t per_job = L.job_bytes + L.scratch_bytes;
+        const size_t small_per_job = sizeof(int2) + 3 * sizeof(double) + sizeof(int);
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        // the FP64 re-runs keep their own workspace (4 blocks per CTA)
+        const size_t fp64_ws = (size_t)c->num_sms * 4 * c->ld * N * 16;
+        const size_t avail = free_b + c->mixed_bytes;
+        const size_t budget = avail > fp64_ws + ((size_t)4 << 30) ? (size_t)(0.92 * (avail - fp64_ws)) - ((size_t)2 << 30) : 0;
+        int W = (int)std::min<size_t>({(size_t)m_jobs.size(), (size_t)c->num_sms, budget / (per_job + small_per_job)});
+        if (W < 1) {
+            // not enough device memory for one job: everything in FP64
+            for (int q : m_jobs) { f_ie.push_back(q % nE); f_ik.push_back(q / nE); }
+            stats.n_fp64_policy += (int)m_jobs.size();
+            m_jobs.clear();
+        } else {
+            const size_t need = (size_t)W * (per_job + small_per_job) + 4096;
+            if (need > c->mixed_bytes) {
+                if (c->d_mixed) cudaFree(c->d_mixed);
+                c->d_mixed = nullptr;
+                c->mixed_bytes = 0;
+                if (cudaMalloc(&c->d_mixed, need) != cudaSuccess) { cudaGetLastError(); return NEGF_ERR_NOMEM; }
+                c->mixed_bytes = need;
+            }
+            stats.jobs_per_wave = W;
+            unsigned char *base = (unsigned char *)c->d_mixed;
+            MixedArgs a;
+            a.g = mixed_geo(c);
+            a.L = L;
+            a.E = d_E;
+            a.jobmem = base;
+            a.scratch = base + (size_t)W * L.job_bytes;
+            unsigned char *smallp = a.scratch + (size_t)W * L.scratch_bytes;
+            int2 *d_jobs = (int2 *)smallp;
+            a.jobs = d_jobs;
+            a.tau = (double *)align256((size_t)(d_jobs + W));
+            a.dnorm = a.tau + W;
+            a.xnorm = a.dnorm + W;
+            a.status = (int *)(a.xnorm + W);
+            const size_t sm_sweep = gj_smem_bytes(N) + (tile_smem_bytes() + 127) / 128 * 128 + job_smem_bytes(N) +
+                                    (size_t)rup(N, 4) * 4;
+            const size_t sm_pass = pass_smem_bytes(N, ncap);
+            const size_t sm_res = (size_t)negf::KC * (negf::AP + negf::BP) * 16 + job_smem_bytes(N);
+            if (N <= NT) rc = set_smem(k_mixed_sweep<1>, sm_sweep);
+            else if (N <= 2 * NT) rc = set_smem(k_mixed_sweep<2>, sm_sweep);
+            else rc = set_smem(k_mixed_sweep<4>, sm_sweep);
+            if (!rc) rc = set_smem(k_mixed_pass, sm_pass);
+            if (!rc) rc = set_smem(k_mixed_residual, sm_res);
+            if (rc) return rc;
+            std::vector<int2> wj(W);
+            std::vector<double> tau(W), dn(W), xn(W);
+            std::vector<int> status(W);
+            for (size_t w0 = 0; w0 < m_jobs.size(); w0 += W) {
+                const int nw = (int)std::min<size_t>(W, m_jobs.size() - w0);
+                for (int w = 0; w < nw; ++w) wj[w] = make_int2(m_jobs[w0 + w] % nE, m_jobs[w0 + w] / nE);
+                a.njobs = nw;
+                CKM(cudaMemcpyAsync(d_jobs, wj.data(), sizeof(int2) * nw, cudaMemcpyHostToDevice, st));
+                CKM(cudaEventRecord(c->ev0, st));
+                if (N <= NT) k_mixed_sweep<1><<<nw, NT, sm_sweep, st>>>(a);
+                else if (N <= 2 * NT) k_mixed_sweep<2><<<nw, NT, sm_sweep, st>>>(a);
+                else k_mixed_sweep<4><<<nw, NT, sm_sweep, st>>>(a);
+                CKM(cudaGetLastError());
+                k_mixed_pass<<<nw, NT, sm_pass, st>>>(a, PASS_X0);
+                CKM(cudaGetLastError());
+                k_mixed_residual<<<dim3(Nz, nw), NT, sm_res, st>>>(a);
+                CKM(cudaGetLastError());
+                k_mixed_pass<<<nw, NT, sm_pass, st>>>(a, PASS_BACK);
+                CKM(cudaGetLastError());
+                k_mixed_pass<<<nw, NT, sm_pass, st>>>(a, PASS_CORR);
+                CKM(cudaGetLastError());
+                CKM(cudaEventRecord(c->ev1, st));
+                CKM(cudaMemcpyAsync(tau.data(), a.tau, sizeof(double) * nw, cudaMemcpyDeviceToHost, st));
+                CKM(cudaMemcpyAsync(dn.data(), a.dnorm, sizeof(double) * nw, cudaMemcpyDeviceToHost, st));
+                CKM(cudaMemcpyAsync(xn.data(), a.xnorm, sizeof(double) * nw, cudaMemcpyDeviceToHost, st));
+                CKM(cudaMemcpyAsync(status.data(), a.status, sizeof(int) * nw, cudaMemcpyDeviceToHost, st));
+                CKM(cudaStreamSynchronize(st));
+                float ms = 0.f;
+                CKM(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+                mixed_ms += ms;
+                for (int w = 0; w < nw; ++w) {
+                    const int q = m_jobs[w0 + w];
+                    const double corr = xn[w] > 0 ? dn[w] / xn[w] : INFINITY;
+                    const double est = 2.0 * std::max(tau[w], 1.0) * corr * corr;
+                    if (status[w] == 0 && std::isfinite(tau[w]) && est < pol.tau_tolerance) {
+                        h_tau_jobs[q] = tau[w];
+                        h_info[q] = 0;
+                        stats.n_mixed++;
+                        stats.max_correction = std::max(stats.max_correction, corr);
+                    } else {
+                        if (status[w] == -2) return NEGF_ERR_CUDA;  // a tensor-core wait timed out
+                        f_ie.push_back(q % nE);
+                        f_ik.push_back(q / nE);
+                        stats.n_fp64_rejected++;
+                    }
+                }
+            }
+        }
+    }
+    // ---- FP64 re-runs
+    float ms64 = 0.f;
+    if (!f_ie.empty()) {
+        std::vector<double> t64(f_ie.size());
+        std::vector<int> i64(f_ie.size());
+        rc = negf_internal_fp64_jobs(c, d_E, f_ie.data(), f_ik.data(), (int)f_ie.size(), t64.data(), i64.data(),
+                                     &ms64);
+        if (rc) return rc;
+        for (size_t q = 0; q < f_ie.size(); ++q) {
+            const int job = f_ik[q] * nE + f_ie[q];
+            h_tau_jobs[job] = t64[q];
+            h_info[job] = i64[q];
+        }
+    }
+    stats.mixed_ms = mixed_ms;
+    stats.fp64_ms = ms64;
+    c->mixed_stats = stats;
+    *device_ms = mixed_ms + ms64;
+    return NEGF_OK;
 }

@@ -20,7 +20,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import NEGF_FP64, Problem, Stats, _dp, _ip, check, lib
+from ._lib import NEGF_FP64, NEGF_MIXED, MixedPolicy, MixedStats, Problem, Stats, _dp, _ip, check, lib
 
 
 class Engine:
@@ -91,6 +91,27 @@ class Engine:
             self._ctx, e.ctypes.data_as(_dp), len(e), precision, tau.ctypes.data_as(_dp), C.byref(st)))
         self.last_stats = st
         return tau, rc
+
+    def set_mixed_policy(self, threshold_window=None, eta_fp64_below=None, tau_tolerance=None):
+        """Policy of the NEGF_MIXED path (Hartree): energies within threshold_window of a
+        lead subband threshold run in FP64; eta below eta_fp64_below sends every job to
+        FP64; a refined job is accepted when 2 max(tau,1) (|d|/|x|)^2 < tau_tolerance.
+        Unset arguments keep their current values."""
+        p = MixedPolicy()
+        check("negf_get_mixed_policy", lib().negf_get_mixed_policy(self._ctx, C.byref(p)))
+        if threshold_window is not None:
+            p.threshold_window = float(threshold_window)
+        if eta_fp64_below is not None:
+            p.eta_fp64_below = float(eta_fp64_below)
+        if tau_tolerance is not None:
+            p.tau_tolerance = float(tau_tolerance)
+        check("negf_set_mixed_policy", lib().negf_set_mixed_policy(self._ctx, C.byref(p)))
+
+    def mixed_stats(self):
+        """Counts and device times of the last NEGF_MIXED call (dict)."""
+        s = MixedStats()
+        check("negf_get_mixed_stats", lib().negf_get_mixed_stats(self._ctx, C.byref(s)))
+        return s.as_dict()
 
     def set_variant(self, variant):
         """Force the transmission kernel variant (0, 1, 2, 3; -1 = chosen by N)."""

@@ -78,3 +78,87 @@ def test_fp32_gauss_jordan_inverse(N):
         assert res < 1e-6, (m, res)
         Xr = np.linalg.inv(Am)
         assert np.linalg.norm(X - Xr) / np.linalg.norm(Xr) < 1e-5
+
+
+# ------------------------------------------------------ mixed transmission
+# NEGF_MIXED: split-fp16 tensor-core factorization + FP64 residual refinement
+# + FP64 re-run of rejected jobs.  The bar of the headline metric: every
+# energy within max|dT| <= 1e-6 of the FP64 oracle.
+TOL_MIXED = 1e-6
+
+
+def _oracle(pr, E, nthreads=8):
+    from oracle import oracle as O
+    a = pr.atomic
+    p = O.Problem(pr.nx, pr.ny, pr.vhat, a.LX, a.LY, a.LZ, a.V_L, a.V_R, a.ETA, pr.kpoint)
+    tau, info = O.transmission_jobs(p, E, nthreads=nthreads)
+    assert info == 0
+    return tau
+
+
+def _prepared(name, nz=None):
+    from negftrans_b200 import prepare as P, workloads as W
+    w = W.config(name, nz=nz)
+    return w, P.prepare(w.deck, w.V_eV)
+
+
+@pytest.mark.parametrize("name,ne,nk", [("small:1.2:16", 16, 1), ("qpc_n69", 48, 1)])
+def test_mixed_transmission_matches_oracle(name, ne, nk):
+    from negftrans_b200 import prepare as P
+    from negftrans_b200._lib import NEGF_MIXED
+    from negftrans_b200.negf import Engine
+    w, pr = _prepared(name)
+    grid = P.transmission_energies(pr.atomic, w.n_energy)
+    E = np.ascontiguousarray(grid[:: max(1, len(grid) // ne)][:ne])
+    ref = _oracle(pr, E)
+    with Engine(*pr.engine_args()) as eng:
+        tau, info = eng.transmission(E, precision=NEGF_MIXED)
+        st = eng.mixed_stats()
+    assert info == 0
+    assert st["n_jobs"] == len(E) * nk
+    assert st["n_mixed"] + st["n_fp64_policy"] + st["n_fp64_rejected"] == st["n_jobs"]
+    assert st["n_mixed"] >= 0.8 * st["n_jobs"], st
+    assert np.max(np.abs(tau - ref)) <= TOL_MIXED, np.max(np.abs(tau - ref))
+
+
+@pytest.mark.parametrize("name", ["qpc_disorder_n221", "qpc_disorder_n797"])
+def test_mixed_transmission_matches_full_size_fixture(name):
+    import os
+    from negftrans_b200 import prepare as P
+    from negftrans_b200._lib import NEGF_MIXED
+    from negftrans_b200.negf import Engine
+    ref = np.load(os.path.join(os.path.dirname(__file__), "golden", f"oracle_{name}.npz"))
+    w, pr = _prepared(name)
+    E = P.transmission_energies(pr.atomic, int(ref["grid_size"]))[ref["idx"]]
+    with Engine(*pr.engine_args()) as eng:
+        tau, info = eng.transmission(E, precision=NEGF_MIXED)
+        st = eng.mixed_stats()
+    assert info == 0
+    assert np.max(np.abs(tau - ref["tau"])) <= TOL_MIXED, (np.abs(tau - ref["tau"]), st)
+
+
+def test_mixed_policy_routes_jobs_to_fp64():
+    from negftrans_b200 import prepare as P
+    from negftrans_b200._lib import NEGF_FP64, NEGF_MIXED
+    from negftrans_b200.negf import Engine
+    w, pr = _prepared("qpc_n69", nz=40)
+    E = P.transmission_energies(pr.atomic, w.n_energy)[::16]
+    a = pr.atomic
+    with Engine(*pr.engine_args()) as eng:
+        t64, _ = eng.transmission(E, precision=NEGF_FP64)
+        # eta below the bound: every job runs the FP64 path, bit for bit
+        eng.set_mixed_policy(eta_fp64_below=2 * a.ETA)
+        tm, _ = eng.transmission(E, precision=NEGF_MIXED)
+        st = eng.mixed_stats()
+        assert st["n_fp64_policy"] == len(E) and st["n_mixed"] == 0
+        np.testing.assert_array_equal(tm, t64)
+        # threshold window: exactly the energies near a lead threshold go to FP64
+        eng.set_mixed_policy(eta_fp64_below=0.0, threshold_window=1e-3 * 0.067 / 27.211386245988)
+        tm, _ = eng.transmission(E, precision=NEGF_MIXED)
+        st = eng.mixed_stats()
+    kx = 2.0 * pr.nx * np.pi / a.LX
+    ky = 2.0 * pr.ny * np.pi / a.LY
+    th = 0.5 * (kx ** 2 + ky ** 2)
+    near = sum(bool(np.any(np.abs(e - th) < 1e-3 * 0.067 / 27.211386245988)) for e in E)
+    assert st["n_fp64_policy"] == near
+    assert np.max(np.abs(tm - t64)) <= TOL_MIXED
