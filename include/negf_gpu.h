@@ -75,9 +75,14 @@ typedef struct negf_mixed_policy {
     double eta_fp64_below;   /* Hartree.  If the context's eta is below this, every job
                               * runs in FP64.  0 = off (the default).                   */
     double tau_tolerance;    /* A refined job is accepted when its estimated remaining
-                              * error 2 max(tau, 1) (|d| / |x|)^2 is below this (d: the
-                              * refinement correction of G_{Nz,1} on the open channels,
-                              * x the refined value).  Default 1e-7.                    */
+                              * error 2 max(tau, 1) (|d_k| / |x|) rho_k is below this:
+                              * d_k the k-th refinement correction of G_{Nz,1} on the
+                              * open channels, x the refined value, rho_k the measured
+                              * contraction (|d_1| / |x| after one step, |d_k| / |d_k-1|
+                              * after more).  Default 1e-7.                             */
+    int32_t max_refinements; /* refinement steps before a job that has not met the
+                              * tolerance is re-run in FP64 (1..8, default 5)           */
+    int32_t pad;
 } negf_mixed_policy;
 
 typedef struct negf_mixed_stats {

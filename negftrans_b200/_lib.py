@@ -48,7 +48,8 @@ class Problem(C.Structure):
 
 
 class MixedPolicy(C.Structure):
-    _fields_ = [("threshold_window", C.c_double), ("eta_fp64_below", C.c_double), ("tau_tolerance", C.c_double)]
+    _fields_ = [("threshold_window", C.c_double), ("eta_fp64_below", C.c_double), ("tau_tolerance", C.c_double),
+                ("max_refinements", C.c_int32), ("pad", C.c_int32)]
 
 
 class MixedStats(C.Structure):

@@ -1371,7 +1371,8 @@ int negf_internal_fp64_jobs(negf_ctx *c, const double *d_E, const int *ie, const
 }
 
 extern "C" int negf_set_mixed_policy(negf_ctx *c, const negf_mixed_policy *p) {
-    if (!c || !p || !(p->threshold_window >= 0) || !(p->eta_fp64_below >= 0) || !(p->tau_tolerance > 0))
+    if (!c || !p || !(p->threshold_window >= 0) || !(p->eta_fp64_below >= 0) || !(p->tau_tolerance > 0) ||
+        p->max_refinements < 1 || p->max_refinements > 8)
         return NEGF_ERR_ARG;
     c->mixed_policy = *p;
     return NEGF_OK;

@@ -218,81 +218,366 @@ __device__ inline void stage_w(const TileSmem &t, const GjSmem &s, const float2 
     }
 }
 
-// B tile of the trailing update: column j < TN of the tile is matrix column
-// col(J0 + j) (the columns outside the panel), its K values the pivot rows
-// prow[k0 .. k0+nbt) of that column; one exponent per column.  Thread
-// (column j = tid / 4, K group g = tid % 4).
-__device__ inline void stage_b_pivot_rows(const TileSmem &t, const GjSmem &s, const float2 *__restrict__ A,
-                                          int ld, int N, int k0, int nbt, int J0) {
-    const int tid = threadIdx.x, j = tid >> 2, g = tid & 3;
-    const int nrest = N - nbt, jr = J0 + j;
-    const bool cv = jr < nrest;
-    const int col = jr < k0 ? jr : jr + nbt;
-    float2 v[8];
-    float m = 0.0f;
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        const int kk = 8 * g + q;
-        v[q] = (cv && kk < nbt) ? A[s.prow[k0 + kk] + (size_t)ld * col] : make_float2(0.f, 0.f);
-        m = fmaxf(m, fmaxf(fabsf(v[q].x), fabsf(v[q].y)));
+// ---------------------------------------------- pipelined trailing update
+// The panel's W (N x nbt) and its pivot rows of the other columns
+// (nbt x (N - nbt)) are converted once per panel into split-fp16 tiles in the
+// CTA's global scratch (W: TM-row tiles of 32 KB with one exponent per row; B:
+// PTN-column tiles of 8 KB with one exponent per column).  The TM x PTN output
+// tiles then run through a warp-specialised pipeline whose roles synchronise
+// only through mbarriers:
+//   warp 0 (producer)   bulk copies of the W tile of each row tile (one
+//                       buffer), the B tile (three buffers) and the old C
+//                       values (one bulk copy per column, three buffers) of
+//                       tile t+3 as soon as tile t's C has been stored, and
+//                       the bulk stores of finished C tiles;
+//   warp 1, lane 0      the tcgen05 MMAs of each tile into one of two
+//                       tensor-memory accumulators;
+//   warps 4-7           the epilogue: accumulator (tcgen05.ld, one lane
+//                       quadrant per warp) times 2^(row + column exponent)
+//                       added to the old C in shared memory.
+// The leading dimension must be a multiple of 8 (16-byte bulk copies of whole
+// columns; rows N..ld-1 travel unchanged).
+constexpr int PTN = 32;                         // columns of an output tile
+constexpr int NCB = 3;                          // C buffers
+constexpr int NBB = 3;                          // B buffers
+constexpr uint32_t WTILE = 4u * TM * KB * 2;     // 32 KB
+constexpr uint32_t BTILE = 4u * PTN * KB * 2;    // 8 KB
+constexpr uint32_t CTILE = (uint32_t)TM * PTN * 8;  // 32 KB: PTN columns of TM float2
+struct Pipe {
+    unsigned char *sW;
+    unsigned char *sB[NBB];
+    unsigned char *sC[NCB];
+    uint64_t *fullW, *emptyW;        // [1], [1]
+    uint64_t *fullB, *emptyB;        // [NBB]
+    uint64_t *fullC, *doneC;         // [NCB]: C loaded / C updated by the epilogue
+    uint64_t *accFull, *accEmpty;    // [2]
+    uint64_t *drain;                 // [1] completion of every MMA before tensor memory is freed
+    int *rexpW;                      // [ntr * TM] row exponents of W
+    int *cexpB;                      // [ntc * PTN] column exponents of the pivot rows
+    uint32_t *tslot;
+    unsigned char *wt, *bt;          // global: W tiles, B tiles
+    uint32_t tbase;
+    uint32_t nW, nB, nT;             // W tiles, B tiles and output tiles so far (phase counters)
+};
+constexpr int PIPE_BARS = 2 + 2 * NBB + 2 * NCB + 4 + 1;
+__host__ __device__ inline size_t pipe_smem_bytes(int N) {
+    const int ntr = (N + TM - 1) / TM, ntc = (N + PTN - 1) / PTN;
+    return (size_t)WTILE + NBB * (size_t)BTILE + NCB * (size_t)CTILE + PIPE_BARS * 8 + 8 + 4 * (size_t)ntr * TM +
+           4 * (size_t)ntc * PTN + 16;
+}
+// global scratch of one CTA for the panel tiles
+__host__ __device__ inline size_t pipe_scratch_bytes(int N) {
+    const int ntr = (N + TM - 1) / TM, ntc = (N + PTN - 1) / PTN;
+    return (size_t)ntr * WTILE + (size_t)ntc * BTILE;
+}
+__device__ inline Pipe carve_pipe(unsigned char *base, int N, unsigned char *gscratch) {
+    Pipe P;
+    const int ntr = (N + TM - 1) / TM, ntc = (N + PTN - 1) / PTN;
+    unsigned char *q = base;
+    P.sW = q; q += WTILE;
+    for (int i = 0; i < NCB; ++i) { P.sC[i] = q; q += CTILE; }
+    for (int i = 0; i < NBB; ++i) { P.sB[i] = q; q += BTILE; }
+    uint64_t *bar = (uint64_t *)q;
+    P.fullW = bar; P.emptyW = bar + 1;
+    P.fullB = bar + 2; P.emptyB = P.fullB + NBB;
+    P.fullC = P.emptyB + NBB; P.doneC = P.fullC + NCB;
+    P.accFull = P.doneC + NCB; P.accEmpty = P.accFull + 2;
+    P.drain = P.accEmpty + 2;
+    q += PIPE_BARS * 8 + 8;
+    P.rexpW = (int *)q; q += 4 * (size_t)ntr * TM;
+    P.cexpB = (int *)q; q += 4 * (size_t)ntc * PTN;
+    P.tslot = (uint32_t *)q;
+    P.wt = gscratch;
+    P.bt = gscratch + (size_t)ntr * WTILE;
+    P.nW = P.nB = P.nT = 0;
+    return P;
+}
+// 128 tensor-memory columns: two accumulators of PTN complex columns (re, im)
+__device__ inline void pipe_setup(Pipe &P) {
+    if (threadIdx.x < 32) tc::tmem_alloc(P.tslot, 4 * PTN);
+    if (threadIdx.x == 0) {
+        tc::mbar_init(P.fullW, 1);
+        tc::mbar_init(P.emptyW, 1);
+        for (int i = 0; i < NBB; ++i) { tc::mbar_init(&P.fullB[i], 1); tc::mbar_init(&P.emptyB[i], 1); }
+        for (int i = 0; i < NCB; ++i) { tc::mbar_init(&P.fullC[i], 1); tc::mbar_init(&P.doneC[i], 4); }
+        for (int i = 0; i < 2; ++i) { tc::mbar_init(&P.accFull[i], 1); tc::mbar_init(&P.accEmpty[i], 4); }
+        tc::mbar_init(P.drain, 1);
     }
-    m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 1));
-    m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 2));
-    const int e = tc::scale_exponent(m);
-    const float sc = tc::exp2i(-e);
-    if (g == 0) t.cexp[j] = e;
-#pragma unroll
-    for (int q = 0; q < 8; ++q) v[q] = make_float2(v[q].x * sc, v[q].y * sc);
-    store_split8(t.sb, j, g, v);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    P.tbase = *P.tslot;
+}
+__device__ inline void pipe_teardown(const Pipe &P) {
+    // the MMA issuer's last commit: every MMA it issued has completed (bounded;
+    // on the normal path they have long finished)
+    if (threadIdx.x == 32) {
+        tc::mma_commit(P.drain);
+        tc::mbar_wait(P.drain, 0, WAIT_LIMIT);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (threadIdx.x < 32) tc::tmem_dealloc(P.tbase, 4 * PTN);
 }
 
-// A(:, rest) = mask(A(:, rest)) + W * A_old(prow[k0:k0+nbt], rest) with
-// W = A(:, k0:k0+nbt): the combined effect of the panel's Gauss-Jordan steps
-// on every other column (mask zeroes the panel's pivot rows), on the tensor
-// cores.  Returns false if an MMA wait timed out.
-__device__ inline bool trailing_update_tc(float2 *__restrict__ A, int N, int ld, int k0, int nbt, const GjSmem &s,
-                                          const TileSmem &t, uint32_t tbase, uint32_t &ph) {
-    const int tid = threadIdx.x, warp = tid >> 5;
-    const int nrest = N - nbt;
-    int err = 0;
-    for (int J0 = 0; J0 < nrest; J0 += TN) {
-        stage_b_pivot_rows(t, s, A, ld, N, k0, nbt, J0);
-        for (int I0 = 0; I0 < N; I0 += TM) {
-            stage_w(t, s, A, ld, N, I0, k0, nbt);  // contains a barrier
-            tc::fence_async_smem();
-            __syncthreads();
-            if (tid == 0) {
-                tc::fence_after_sync();
-                issue_chunk(t, tbase, true);
-                tc::mma_commit(t.bar);
-            }
-            wait_mma(t, ph, &err);
-            // epilogue: warps 0-3 columns 0-31, warps 4-7 columns 32-63
-            const int r = 32 * (warp & 3) + (tid & 31), i = I0 + r;
-            const bool rv = i < N;
-            const bool keep = rv && !s.inP[i];
-            const int er = t.rexp[r];
-#pragma unroll 1
-            for (int c16 = 2 * (warp >> 2); c16 < 2 * (warp >> 2) + 2; ++c16) {
-                float re[16], im[16];
-                load_acc16(tbase, c16, re, im);
+__device__ __forceinline__ void expect_bytes(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(tc::smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(tc::smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void bulk_copy(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     tc::smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(tc::smem_u32(bar))
+                 : "memory");
+}
+// shared -> global bulk store in the issuing thread's bulk group
+__device__ __forceinline__ void bulk_store(void *dst, const void *src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(dst), "r"(tc::smem_u32(src)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
+// this thread's committed bulk stores have finished reading shared memory
+__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+// ... and have completed
+__device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+
+// MMAs of one K chunk: A (TM x KB, plane stride TM*KB*2), B (n x KB, plane
+// stride n*KB*2), D re at d0, im at d0 + n.  first = overwrite.
+__device__ inline void issue_split_mma(uint32_t a0, uint32_t b0, int n, uint32_t d0, bool first) {
+    constexpr uint32_t SBO = (KB / 8) * 128, LBO = 128;
+    const uint32_t id = tc::idesc_f16(TM, n, false), idn = tc::idesc_f16(TM, n, true);
+    const uint32_t aplane = TM * KB * 2, bplane = n * KB * 2;
+    const int pa[3] = {0, 0, 1}, pb[3] = {0, 1, 0};
 #pragma unroll
-                for (int q = 0; q < 16; ++q) {
-                    const int j = c16 * 16 + q, jr = J0 + j;
-                    if (rv && jr < nrest) {
-                        const int col = jr < k0 ? jr : jr + nbt;
-                        float2 *cp = A + i + (size_t)ld * col;
-                        const float2 c = keep ? *cp : make_float2(0.f, 0.f);
-                        const int ex = er + t.cexp[j];
-                        *cp = make_float2(c.x + ldexpf(re[q], ex), c.y + ldexpf(im[q], ex));
+    for (int ks = 0; ks < KB / 16; ++ks) {
+        const uint32_t koff = ks * 256;
+#pragma unroll
+        for (int sp = 0; sp < 3; ++sp) {
+            const uint64_t are = tc::sdesc(a0 + (0 + pa[sp]) * aplane + koff, LBO, SBO);
+            const uint64_t aim = tc::sdesc(a0 + (2 + pa[sp]) * aplane + koff, LBO, SBO);
+            const uint64_t bre = tc::sdesc(b0 + (0 + pb[sp]) * bplane + koff, LBO, SBO);
+            const uint64_t bim = tc::sdesc(b0 + (2 + pb[sp]) * bplane + koff, LBO, SBO);
+            const uint32_t acc = (first && ks == 0 && sp == 0) ? 0u : 1u;
+            tc::mma_f16(d0, are, bre, id, acc);
+            tc::mma_f16(d0, aim, bim, idn, 1u);
+            tc::mma_f16(d0 + n, are, bim, id, acc);
+            tc::mma_f16(d0 + n, aim, bre, id, 1u);
+        }
+    }
+}
+
+// W tiles: row r of the panel [k0, k0+nbt) of A, two threads per row (lanes
+// l and l+16 of a warp, 16 K values each).
+__device__ inline void convert_w(const Pipe &P, const float2 *__restrict__ A, int ld, int N, int k0, int nbt) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, h = lane >> 4;
+    const int ntr = (N + TM - 1) / TM;
+    for (int r0 = warp * 16; r0 < ntr * TM; r0 += NWARP * 16) {
+        const int row = r0 + (lane & 15);
+        float2 v[16];
+        float m = 0.0f;
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            const int kk = 16 * h + q;
+            v[q] = (row < N && kk < nbt) ? A[row + (size_t)ld * (k0 + kk)] : make_float2(0.f, 0.f);
+            m = fmaxf(m, fmaxf(fabsf(v[q].x), fabsf(v[q].y)));
+        }
+        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 16));
+        const int e = tc::scale_exponent(m);
+        const float sc = tc::exp2i(-e);
+        if (h == 0) P.rexpW[row] = e;
+        unsigned char *tile = P.wt + (size_t)(row / TM) * WTILE;
+#pragma unroll
+        for (int g = 0; g < 2; ++g) {
+            __align__(16) __half rh[8], rl[8], ih[8], il[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const tc::Split2 a = tc::split_fp16(v[8 * g + q].x * sc), b = tc::split_fp16(v[8 * g + q].y * sc);
+                rh[q] = a.hi; rl[q] = a.lo; ih[q] = b.hi; il[q] = b.lo;
+            }
+            const uint32_t off = tc::kmajor_offset(row % TM, 8 * (2 * h + g), KB);
+            *(uint4 *)(tile + 0 * (TM * KB * 2) + off) = *(const uint4 *)rh;
+            *(uint4 *)(tile + 1 * (TM * KB * 2) + off) = *(const uint4 *)rl;
+            *(uint4 *)(tile + 2 * (TM * KB * 2) + off) = *(const uint4 *)ih;
+            *(uint4 *)(tile + 3 * (TM * KB * 2) + off) = *(const uint4 *)il;
+        }
+    }
+}
+// B tiles: rest column jr (the columns outside the panel, in order) with the
+// K values A(prow[k0 + kk], col(jr)); four threads per column.
+__device__ inline void convert_b(const Pipe &P, const GjSmem &s, const float2 *__restrict__ A, int ld, int N,
+                                 int k0, int nbt) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane & 3;
+    const int nrest = N - nbt, ntc = (nrest + PTN - 1) / PTN;
+    for (int c0 = warp * 8; c0 < ntc * PTN; c0 += NWARP * 8) {
+        const int jr = c0 + (lane >> 2);
+        const bool cv = jr < nrest;
+        const int col = jr < k0 ? jr : jr + nbt;
+        float2 v[8];
+        float m = 0.0f;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int kk = 8 * g + q;
+            v[q] = (cv && kk < nbt) ? A[s.prow[k0 + kk] + (size_t)ld * col] : make_float2(0.f, 0.f);
+            m = fmaxf(m, fmaxf(fabsf(v[q].x), fabsf(v[q].y)));
+        }
+        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 1));
+        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 2));
+        const int e = tc::scale_exponent(m);
+        const float sc = tc::exp2i(-e);
+        if (g == 0) P.cexpB[jr] = e;
+        __align__(16) __half rh[8], rl[8], ih[8], il[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const tc::Split2 a = tc::split_fp16(v[q].x * sc), b = tc::split_fp16(v[q].y * sc);
+            rh[q] = a.hi; rl[q] = a.lo; ih[q] = b.hi; il[q] = b.lo;
+        }
+        unsigned char *tile = P.bt + (size_t)(jr / PTN) * BTILE;
+        const uint32_t off = tc::kmajor_offset(jr % PTN, 8 * g, KB);
+        *(uint4 *)(tile + 0 * (PTN * KB * 2) + off) = *(const uint4 *)rh;
+        *(uint4 *)(tile + 1 * (PTN * KB * 2) + off) = *(const uint4 *)rl;
+        *(uint4 *)(tile + 2 * (PTN * KB * 2) + off) = *(const uint4 *)ih;
+        *(uint4 *)(tile + 3 * (PTN * KB * 2) + off) = *(const uint4 *)il;
+    }
+}
+
+// A(:, rest) = mask(A(:, rest)) + W * A_old(prow[k0:k0+nbt], rest), pipelined
+// (see above).  ld % 8 == 0.  Returns false if a wait timed out (uniform).
+__device__ inline bool trailing_pipe(Pipe &P, float2 *__restrict__ A, int N, int ld, int k0, int nbt,
+                                     const GjSmem &s) {
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nrest = N - nbt, ntr = (N + TM - 1) / TM, ntc = (nrest + PTN - 1) / PTN, T = ntr * ntc;
+    convert_w(P, A, ld, N, k0, nbt);
+    convert_b(P, s, A, ld, N, k0, nbt);
+    asm volatile("fence.proxy.async.global;\n" ::: "memory");  // generic stores -> bulk-copy reads
+    __syncthreads();
+    const uint32_t bW = P.nW, bB = P.nB, bT = P.nT;
+    int err = 0;
+    // matrix column of output column c of tile t (-1 outside the rest columns)
+    auto tile_col = [&](int t, int c) -> int {
+        const int jr = (t % ntc) * PTN + c;
+        return jr < nrest ? (jr < k0 ? jr : jr + nbt) : -1;
+    };
+    auto tile_rows = [&](int t) -> int { return min(TM, ld - (t / ntc) * TM); };
+    if (warp == 0) {
+        // ------------------------------------------------------ producer
+        auto load = [&](int u) -> bool {
+            if (u % ntc == 0) {
+                const uint32_t iw = bW + u / ntc;
+                bool ok = true;
+                if (lane == 0) {
+                    if (iw >= 1) ok = tc::mbar_wait(P.emptyW, (iw - 1) & 1u, WAIT_LIMIT);
+                    if (ok) {
+                        expect_bytes(P.fullW, WTILE);
+                        bulk_copy(P.sW, P.wt + (size_t)(u / ntc) * WTILE, WTILE, P.fullW);
+                    }
+                }
+                if (!__shfl_sync(0xffffffffu, (int)ok, 0)) return false;
+            }
+            const uint32_t ib = bB + u, ic = bT + u;
+            bool ok = true;
+            if (lane == 0) {
+                if (ib >= NBB) ok = tc::mbar_wait(&P.emptyB[ib % NBB], ((ib - NBB) / NBB) & 1u, WAIT_LIMIT);
+                if (ok) {
+                    expect_bytes(&P.fullB[ib % NBB], BTILE);
+                    bulk_copy(P.sB[ib % NBB], P.bt + (size_t)(u % ntc) * BTILE, BTILE, &P.fullB[ib % NBB]);
+                }
+            }
+            if (!__shfl_sync(0xffffffffu, (int)ok, 0)) return false;
+            // the C buffer last held tile u - NCB, whose store this warp issued before
+            bulk_wait_read0();
+            const int rows = tile_rows(u), ncol = min(PTN, nrest - (u % ntc) * PTN);
+            if (lane == 0) expect_bytes(&P.fullC[ic % NCB], (uint32_t)(rows * 8 * ncol));
+            __syncwarp();
+            const int col = tile_col(u, lane);
+            if (col >= 0)
+                bulk_copy(P.sC[ic % NCB] + lane * (TM * 8), A + (size_t)(u / ntc) * TM + (size_t)ld * col, rows * 8,
+                          &P.fullC[ic % NCB]);
+            return true;
+        };
+        for (int u = 0; u < NCB && u < T && !err; ++u)
+            if (!load(u)) err = 1;
+        for (int v = 0; v < T && !err; ++v) {
+            const uint32_t ic = bT + v;
+            if (!tc::mbar_wait(&P.doneC[ic % NCB], (ic / NCB) & 1u, WAIT_LIMIT)) { err = 1; break; }
+            const int col = tile_col(v, lane);
+            if (col >= 0)
+                bulk_store(A + (size_t)(v / ntc) * TM + (size_t)ld * col, P.sC[ic % NCB] + lane * (TM * 8),
+                           tile_rows(v) * 8);
+            bulk_commit();
+            if (v + NCB < T && !load(v + NCB)) err = 1;
+        }
+        bulk_wait0();
+        asm volatile("fence.proxy.async.global;\n" ::: "memory");
+    } else if (warp == 1) {
+        // --------------------------------------------------- MMA issuer
+        if (lane == 0) {
+            for (int t = 0; t < T; ++t) {
+                const uint32_t ic = bT + t, ib = bB + t, a = ic & 1u;
+                if (ic >= 2 && !tc::mbar_wait(&P.accEmpty[a], ((ic >> 1) & 1u) ^ 1u, WAIT_LIMIT)) { err = 1; break; }
+                if (t % ntc == 0 && !tc::mbar_wait(P.fullW, (bW + t / ntc) & 1u, WAIT_LIMIT)) { err = 1; break; }
+                if (!tc::mbar_wait(&P.fullB[ib % NBB], (ib / NBB) & 1u, WAIT_LIMIT)) { err = 1; break; }
+                tc::fence_after_sync();
+                issue_split_mma(tc::smem_u32(P.sW), tc::smem_u32(P.sB[ib % NBB]), PTN, P.tbase + a * (2 * PTN), true);
+                tc::mma_commit(&P.accFull[a]);
+                tc::mma_commit(&P.emptyB[ib % NBB]);
+                if (t % ntc == ntc - 1) tc::mma_commit(P.emptyW);
+            }
+        }
+        __syncwarp();
+    } else if (warp >= 4) {
+        // ------------------------------------------------------ epilogue
+        const int q4 = warp & 3, r = 32 * q4 + lane;
+        const uint32_t lb = (uint32_t)(32 * q4) << 16;
+        for (int t = 0; t < T && !err; ++t) {
+            const uint32_t ic = bT + t, a = ic & 1u, cb = ic % NCB;
+            if (!tc::mbar_wait(&P.accFull[a], (ic >> 1) & 1u, WAIT_LIMIT)) err = 1;
+            if (!tc::mbar_wait(&P.fullC[cb], (ic / NCB) & 1u, WAIT_LIMIT)) err = 1;
+            if (__any_sync(0xffffffffu, err)) { err = 1; break; }
+            tc::fence_after_sync();
+            const int it = t / ntc, jt = t % ntc, i = it * TM + r;
+            const bool rv = i < N, keep = rv && !s.inP[i];
+            const int er = rv ? P.rexpW[i] : 0;
+            float2 *cs = (float2 *)P.sC[cb];
+            const uint32_t dacc = P.tbase + lb + a * (2 * PTN);
+#pragma unroll
+            for (int g = 0; g < PTN / 16; ++g) {
+                float re[16], im[16];
+                tc::tmem_ld16(dacc + g * 16, re);
+                tc::tmem_ld16(dacc + PTN + g * 16, im);
+                float2 old[16];
+#pragma unroll
+                for (int q = 0; q < 16; ++q) old[q] = cs[(g * 16 + q) * TM + r];
+                tc::tmem_wait_ld();
+                if (rv) {
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) {
+                        const int jr = jt * PTN + g * 16 + q;
+                        if (jr < nrest) {
+                            const float f = tc::exp2i(er + P.cexpB[jr]);
+                            const float2 o = keep ? old[q] : make_float2(0.f, 0.f);
+                            cs[(g * 16 + q) * TM + r] = make_float2(fmaf(re[q], f, o.x), fmaf(im[q], f, o.y));
+                        }
                     }
                 }
             }
+            // tensor memory read: the accumulator may take the next tile's MMAs
             tc::fence_before_sync();
-            // a timed-out wait ends the update in every thread together
-            if (__syncthreads_or(err)) return false;
+            tc::fence_async_smem();  // the bulk stores (async proxy) read these values
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive(&P.accEmpty[a]);
+                mbar_arrive(&P.doneC[cb]);
+            }
         }
     }
+    if (__syncthreads_or(err)) return false;
+    P.nW += ntr;
+    P.nB += T;
+    P.nT += T;
     return true;
 }
 
@@ -306,8 +591,7 @@ __device__ inline bool trailing_update_tc(float2 *__restrict__ A, int N, int ld,
 // LAPACK-style info (1-based column of the first zero pivot, 0 if none);
 // *err = 1 if a tensor-core wait timed out.
 template <int RPT>
-__device__ int gj_invert_mixed(float2 *__restrict__ A, int N, int ld, const GjSmem &s, const TileSmem &t,
-                               uint32_t tbase, uint32_t &ph, int *err) {
+__device__ int gj_invert_mixed(float2 *__restrict__ A, int N, int ld, const GjSmem &s, Pipe &P, int *err) {
     const int tid = threadIdx.x;
     const float2 zero = make_float2(0.f, 0.f);
     int info = 0;
@@ -387,7 +671,7 @@ __device__ int gj_invert_mixed(float2 *__restrict__ A, int N, int ld, const GjSm
             }
             __syncthreads();
         }
-        if (nbt < N && !trailing_update_tc(A, N, ld, k0, nbt, s, t, tbase, ph)) {
+        if (nbt < N && !trailing_pipe(P, A, N, ld, k0, nbt, s)) {
             *err = 1;
             return info;
         }
@@ -455,8 +739,8 @@ __global__ void __launch_bounds__(NT, 1)
             for (int q = 0; q < 16; ++q) {
                 const int jc = J0 + c16 * 16 + q;
                 if (i < M && jc < ncol) {
-                    const int ex = t.rexp[r] + t.cexp[c16 * 16 + q];
-                    C[i + (size_t)ldc * jc] = make_float2(ldexpf(re[q], ex), ldexpf(im[q], ex));
+                    const float f = tc::exp2i(t.rexp[r] + t.cexp[c16 * 16 + q]);
+                    C[i + (size_t)ldc * jc] = make_float2(re[q] * f, im[q] * f);
                 }
             }
         }
@@ -469,28 +753,27 @@ __global__ void __launch_bounds__(NT, 1)
 // work holds the matrices (overwritten), out receives the inverses.
 template <int RPT>
 __global__ void __launch_bounds__(NT, 1)
-    k_tc_inverse_check(float2 *__restrict__ work, int N, float2 *__restrict__ out, int *__restrict__ info,
-                       int *status) {
+    k_tc_inverse_check(float2 *__restrict__ work, int N, int ld, float2 *__restrict__ out, int *__restrict__ info,
+                       int *status, unsigned char *pscratch) {
     extern __shared__ __align__(128) unsigned char smem[];
     GjSmem s = carve_gj(smem, N);
-    TileSmem t = carve_tile(smem + gj_smem_bytes(N));
-    const uint32_t tbase = tile_setup(t);
-    uint32_t ph = 0;
+    Pipe P = carve_pipe(smem + gj_smem_bytes(N), N, pscratch + (size_t)blockIdx.x * pipe_scratch_bytes(N));
+    pipe_setup(P);
     int err = 0;
-    float2 *A = work + (size_t)blockIdx.x * N * N;
-    const int inf = gj_invert_mixed<RPT>(A, N, N, s, t, tbase, ph, &err);
+    float2 *A = work + (size_t)blockIdx.x * ld * N;
+    const int inf = gj_invert_mixed<RPT>(A, N, ld, s, P, &err);
     if (!err) {
         float2 *o = out + (size_t)blockIdx.x * N * N;
         for (int j = 0; j < N; ++j) {
             const int jc = s.iprow[j];
-            for (int r = threadIdx.x; r < N; r += NT) o[s.iprow[r] + (size_t)N * j] = A[r + (size_t)N * jc];
+            for (int r = threadIdx.x; r < N; r += NT) o[s.iprow[r] + (size_t)N * j] = A[r + (size_t)ld * jc];
         }
     }
     if (threadIdx.x == 0) {
         info[blockIdx.x] = inf;
         if (err) atomicExch(status, 1);
     }
-    tile_teardown(t, tbase);
+    pipe_teardown(P);
 }
 
 // =================================================== mixed-precision sweep
@@ -533,7 +816,7 @@ MixedLayout make_layout(int N, int Nz, int ld, int ncap) {
     L.off_oc = o; o = align256(o + (size_t)(ncap + 4) * 4);
     L.job_bytes = o;
     // sweep: two working matrices; passes: the B operand of one product in split tiles
-    L.scratch_bytes = align256(std::max((size_t)2 * N * ld * 8, (size_t)L.nkc * ncap * 256));
+    L.scratch_bytes = align256(std::max((size_t)2 * N * ld * 8 + pipe_scratch_bytes(N), (size_t)L.nkc * ncap * 256));
     return L;
 }
 
@@ -545,9 +828,12 @@ struct MixedArgs {
     int njobs;
     unsigned char *jobmem; // njobs job regions
     unsigned char *scratch;
-    double *tau, *dnorm, *xnorm;
-    int *status;           // 0 ok; > 0 zero pivot (info); -1 too many open channels; -2 tensor wait timed out
+    double *tau, *dnorm, *xnorm, *dprev;
+    int *status;           // 0 in progress; > 0 zero pivot (info); MIX_DONE converged;
+                           // -1 too many open channels; -2 tensor wait timed out
+    double tol;            // acceptance bound on the estimated remaining |dtau|
 };
+constexpr int MIX_DONE = 0x40000000;
 
 // The job's N-sized vectors used by negf::job_vectors / d_element / open_cols.
 __host__ __device__ inline size_t job_smem_bytes(int N) {
@@ -556,6 +842,30 @@ __host__ __device__ inline size_t job_smem_bytes(int N) {
     b = (b + 15) / 16 * 16;
     b += 2 * (size_t)n2 * 16 + 2 * (size_t)n2 * 8;
     return (b + 127) / 128 * 128;
+}
+// The sweep's variant: only nx, ny, the open-channel list and the lead
+// self-energies in its own space; gamma_L / gamma_R (needed only while the
+// open channels are listed at the start of a job) at gscr.
+__host__ __device__ inline size_t job_smem_bytes_slim(int N) {
+    const int n4 = rup(N, 4), n2 = rup(N, 2);
+    size_t b = 3 * (size_t)n4 * 4 + 16;
+    b = (b + 15) / 16 * 16;
+    b += 2 * (size_t)n2 * 16;
+    return (b + 127) / 128 * 128;
+}
+__device__ inline negf::Smem carve_job_slim(unsigned char *base, int N, unsigned char *gscr) {
+    negf::Smem s{};
+    const int n4 = rup(N, 4), n2 = rup(N, 2);
+    s.nx = (int *)base;
+    s.ny = s.nx + n4;
+    s.rows = s.ny + n4;
+    s.nrows = s.rows + n4;
+    size_t off = ((size_t)3 * n4 * 4 + 16 + 15) / 16 * 16;
+    s.sigL = (double2 *)(base + off);
+    s.sigR = s.sigL + n2;
+    s.gL = (double *)gscr;
+    s.gR = s.gL + n2;
+    return s;
 }
 __device__ inline negf::Smem carve_job(unsigned char *base, int N) {
     negf::Smem s{};
@@ -613,6 +923,7 @@ __device__ inline void store_factor(const float2 *__restrict__ R, const MixedLay
     unsigned char *tiles = jm + L.off_tiles + (size_t)b * L.mat_bytes;
     for (int t = tid; t < N; t += NT) {
         float m = 0.0f;
+#pragma unroll 8
         for (int j = 0; j < N; ++j) {
             const float2 v = R[t + (size_t)ld * j];
             m = fmaxf(m, fmaxf(fabsf(v.x), fabsf(v.y)));
@@ -668,16 +979,16 @@ __global__ void __launch_bounds__(NT, 1) k_mixed_sweep(MixedArgs a) {
     const int N = L.N, Nz = L.Nz, ld = L.ld, tid = threadIdx.x;
     GjSmem s = carve_gj(smem, N);
     size_t off = gj_smem_bytes(N);
-    TileSmem t = carve_tile(smem + off);
-    off += (tile_smem_bytes() + 127) / 128 * 128;
-    negf::Smem js = carve_job(smem + off, N);
-    off += job_smem_bytes(N);
-    int *rexpN = (int *)(smem + off);
-    for (int i = tid; i < N; i += NT) { js.nx[i] = g.nx[i]; js.ny[i] = g.ny[i]; }
-    const uint32_t tbase = tile_setup(t);
-    uint32_t ph = 0;
+    unsigned char *pipe_smem = smem + off;
+    off += (pipe_smem_bytes(N) + 127) / 128 * 128;
     float2 *W0 = (float2 *)(a.scratch + (size_t)blockIdx.x * L.scratch_bytes);
     float2 *W1 = W0 + (size_t)N * ld;
+    Pipe P = carve_pipe(pipe_smem, N, (unsigned char *)(W1 + (size_t)N * ld));
+    negf::Smem js = carve_job_slim(smem + off, N, P.sC[0]);
+    off += job_smem_bytes_slim(N);
+    int *rexpN = (int *)(smem + off);
+    for (int i = tid; i < N; i += NT) { js.nx[i] = g.nx[i]; js.ny[i] = g.ny[i]; }
+    pipe_setup(P);
     for (int w = blockIdx.x; w < a.njobs; w += gridDim.x) {
         const int2 jb = a.jobs[w];
         const double e = a.E[jb.x];
@@ -702,7 +1013,7 @@ __global__ void __launch_bounds__(NT, 1) k_mixed_sweep(MixedArgs a) {
             form_mixed(oth, g, js, s, b, E, jb.y, b < Nz - 1 ? cur : nullptr);
             __syncthreads();
             float2 *tt = cur; cur = oth; oth = tt;
-            const int r = gj_invert_mixed<RPT>(cur, N, ld, s, t, tbase, ph, &err);
+            const int r = gj_invert_mixed<RPT>(cur, N, ld, s, P, &err);
             if (r && !info) info = r;
             if (err) break;  // uniform: set from __syncthreads_or
             store_factor(cur, L, s, rexpN, jm, b);
@@ -719,7 +1030,7 @@ __global__ void __launch_bounds__(NT, 1) k_mixed_sweep(MixedArgs a) {
         __syncthreads();
         if (err) break;
     }
-    tile_teardown(t, tbase);
+    pipe_teardown(P);
 }
 
 // ======================================================= refinement passes
@@ -810,7 +1121,7 @@ __device__ inline void issue_pass_chunk(const unsigned char *sA, const unsigned 
 __device__ bool pass_product(const MixedLayout &L, const PassSmem &p, unsigned char *jm, unsigned char *bscr,
                              int slot, const float2 *__restrict__ v1, const float2 *__restrict__ v2,
                              float2 *__restrict__ out, float alpha, const float2 *__restrict__ wadd, int nopen,
-                             int npad, uint32_t tbase, uint32_t &phases) {
+                             int npad, uint32_t tbase, uint32_t &phases, float2 *__restrict__ xacc = nullptr) {
     const int N = L.N, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int *prow_g = (const int *)(jm + L.off_prow) + (size_t)slot * N;
     const int *rexp_g = (const int *)(jm + L.off_rexp) + (size_t)slot * N;
@@ -923,16 +1234,26 @@ __device__ bool pass_product(const MixedLayout &L, const PassSmem &p, unsigned c
                 tc::tmem_wait_ld();
             }
             if (rv) {
+                float2 wv[16], xv[16];
+#pragma unroll
+                for (int q = 0; q < 16; ++q) {
+                    const int j = c16 * 16 + q;
+                    wv[q] = (wadd && j < nopen) ? wadd[i + (size_t)N * j] : make_float2(0.f, 0.f);
+                    xv[q] = (xacc && j < nopen) ? xacc[i + (size_t)N * j] : make_float2(0.f, 0.f);
+                }
 #pragma unroll
                 for (int q = 0; q < 16; ++q) {
                     const int j = c16 * 16 + q;
                     float2 y = make_float2(0.f, 0.f);
                     if (j < nopen) {
-                        const int ex = er + p.cexp[j];
-                        y = make_float2(alpha * ldexpf(re[q], ex), alpha * ldexpf(im[q], ex));
-                        if (wadd) { const float2 wv = wadd[i + (size_t)N * j]; y.x += wv.x; y.y += wv.y; }
+                        const float f = alpha * tc::exp2i(er + p.cexp[j]);
+                        y = make_float2(fmaf(re[q], f, wv[q].x), fmaf(im[q], f, wv[q].y));
                     }
-                    if (j < L.ncap) out[i + (size_t)N * j] = y;
+                    if (j < L.ncap) {
+                        out[i + (size_t)N * j] = y;
+                        // the refined solution of the next iteration, x += d
+                        if (xacc && j < nopen) xacc[i + (size_t)N * j] = make_float2(xv[q].x + y.x, xv[q].y + y.y);
+                    }
                 }
             }
         }
@@ -947,7 +1268,7 @@ __device__ bool pass_product(const MixedLayout &L, const PassSmem &p, unsigned c
 // of r; PASS_CORR d(0) = G_11 c(0), d(b) = gR(b) (c(b) - d(b-1)), then
 // tau = sum_ij gamma_L,i gamma_R,oc_j |2 dz^2 (x0 + d)(Nz-1)(i, j)|^2 in FP64
 // (grid.f90:362-383) and the norms of d and x0 + d on the rows that enter it.
-__global__ void __launch_bounds__(NT, 1) k_mixed_pass(MixedArgs a, int mode) {
+__global__ void __launch_bounds__(NT, 1) k_mixed_pass(MixedArgs a, int mode, int iter, int last) {
     extern __shared__ __align__(128) unsigned char smem[];
     const MixedLayout &L = a.L;
     const int N = L.N, Nz = L.Nz, tid = threadIdx.x;
@@ -983,10 +1304,14 @@ __global__ void __launch_bounds__(NT, 1) k_mixed_pass(MixedArgs a, int mode) {
                 ok = pass_product(L, p, jm, bscr, b + 1, rc + (b + 1) * sl, nullptr, rc + b * sl, -1.f, rc + b * sl,
                                   nopen, npad, tbase, phases);
         } else {
-            ok = pass_product(L, p, jm, bscr, 0, rc, nullptr, d, 1.f, nullptr, nopen, npad, tbase, phases);
+            // unless this is the last iteration, x(b) += d(b) for b < Nz-1 on the way
+            // (the last slice is kept so that tau is formed from x + d in FP64)
+            float2 *xa = last ? nullptr : x;
+            ok = pass_product(L, p, jm, bscr, 0, rc, nullptr, d, 1.f, nullptr, nopen, npad, tbase, phases,
+                              (Nz > 1 && xa) ? xa : nullptr);
             for (int b = 1; b < Nz && ok; ++b)
                 ok = pass_product(L, p, jm, bscr, b, rc + b * sl, d + ((b - 1) & 1) * sl, d + (b & 1) * sl, 1.f,
-                                  nullptr, nopen, npad, tbase, phases);
+                                  nullptr, nopen, npad, tbase, phases, (b < Nz - 1 && xa) ? xa + b * sl : nullptr);
             if (ok) {
                 // tau of x0 + d at the last slice, FP64
                 const negf::Geo &g = a.g;
@@ -1035,7 +1360,23 @@ __global__ void __launch_bounds__(NT, 1) k_mixed_pass(MixedArgs a, int mode) {
                     double X = 0;
                     for (int q = 0; q < NWARP; ++q) X += p.red[q];
                     a.xnorm[w] = sqrt(X);
+                    // remaining error after this correction: |d_k| times the contraction,
+                    // estimated as |d_1| / |x| after the first step and |d_k| / |d_k-1| later
+                    const double dn = a.dnorm[w], xnv = sqrt(X);
+                    const double corr = xnv > 0 ? dn / xnv : INFINITY;
+                    const double rho = iter == 1 ? corr : (a.dprev[w] > 0 ? dn / a.dprev[w] : INFINITY);
+                    const double est = 2.0 * fmax(a.tau[w], 1.0) * corr * rho;
+                    a.dprev[w] = dn;
+                    if (est < a.tol && isfinite(a.tau[w])) a.status[w] = MIX_DONE;
                 }
+                __syncthreads();
+                // not converged and another iteration follows: fold d into the last slice
+                if (!last && a.status[w] == 0)
+                    for (int e2 = tid; e2 < N * nopen; e2 += NT) {
+                        float2 *xv = (float2 *)xl + e2;
+                        const float2 dv = dl[e2];
+                        *xv = make_float2(xv->x + dv.x, xv->y + dv.y);
+                    }
                 __syncthreads();
             }
         }
@@ -1165,22 +1506,26 @@ extern "C" int negf_tc_inverse_check(const float *d_A, int32_t N, int32_t nmat, 
                                      void *stream) {
     if (!d_A || !d_out || !d_info || N < 1 || N > 1023 || nmat < 1) return NEGF_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
-    const size_t smem = gj_smem_bytes(N) + tile_smem_bytes();
+    const size_t smem = gj_smem_bytes(N) + pipe_smem_bytes(N);
     float2 *work = nullptr;
     int *d_status = nullptr;
-    CKM(cudaMalloc(&work, sizeof(float2) * (size_t)N * N * nmat));
+    unsigned char *pscr = nullptr;
+    const int ld = rup(N, 8);  // whole-column bulk copies of the trailing update need ld % 8 == 0
+    CKM(cudaMalloc(&pscr, pipe_scratch_bytes(N) * nmat));
+    CKM(cudaMalloc(&work, sizeof(float2) * (size_t)ld * N * nmat));
     CKM(cudaMalloc(&d_status, sizeof(int)));
-    CKM(cudaMemcpyAsync(work, d_A, sizeof(float2) * (size_t)N * N * nmat, cudaMemcpyDeviceToDevice, st));
+    CKM(cudaMemcpy2DAsync(work, sizeof(float2) * ld, d_A, sizeof(float2) * N, sizeof(float2) * N, (size_t)N * nmat,
+                          cudaMemcpyDeviceToDevice, st));
     CKM(cudaMemsetAsync(d_status, 0, sizeof(int), st));
     if (N <= NT) {
         CKM(cudaFuncSetAttribute(k_tc_inverse_check<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_tc_inverse_check<1><<<nmat, NT, smem, st>>>(work, N, (float2 *)d_out, d_info, d_status);
+        k_tc_inverse_check<1><<<nmat, NT, smem, st>>>(work, N, ld, (float2 *)d_out, d_info, d_status, pscr);
     } else if (N <= 2 * NT) {
         CKM(cudaFuncSetAttribute(k_tc_inverse_check<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_tc_inverse_check<2><<<nmat, NT, smem, st>>>(work, N, (float2 *)d_out, d_info, d_status);
+        k_tc_inverse_check<2><<<nmat, NT, smem, st>>>(work, N, ld, (float2 *)d_out, d_info, d_status, pscr);
     } else {
         CKM(cudaFuncSetAttribute(k_tc_inverse_check<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_tc_inverse_check<4><<<nmat, NT, smem, st>>>(work, N, (float2 *)d_out, d_info, d_status);
+        k_tc_inverse_check<4><<<nmat, NT, smem, st>>>(work, N, ld, (float2 *)d_out, d_info, d_status, pscr);
     }
     CKM(cudaGetLastError());
     int h = 0;
@@ -1188,6 +1533,7 @@ extern "C" int negf_tc_inverse_check(const float *d_A, int32_t N, int32_t nmat, 
     CKM(cudaStreamSynchronize(st));
     cudaFree(work);
     cudaFree(d_status);
+    cudaFree(pscr);
     return h ? NEGF_ERR_CUDA : NEGF_OK;
 }
 
@@ -1274,7 +1620,7 @@ int negf_internal_mixed(negf_ctx *c, const double *h_E, const double *d_E, int n
         const int ncap = std::max(16, rup(nmax, 16));
         const MixedLayout L = make_layout(N, Nz, c->ld, ncap);
         const size_t per_job = L.job_bytes + L.scratch_bytes;
-        const size_t small_per_job = sizeof(int2) + 3 * sizeof(double) + sizeof(int);
+        const size_t small_per_job = sizeof(int2) + 4 * sizeof(double) + sizeof(int);
         size_t free_b = 0, total_b = 0;
         cudaMemGetInfo(&free_b, &total_b);
         // the FP64 re-runs keep their own workspace (4 blocks per CTA)
@@ -1310,9 +1656,11 @@ int negf_internal_mixed(negf_ctx *c, const double *h_E, const double *d_E, int n
             a.tau = (double *)align256((size_t)(d_jobs + W));
             a.dnorm = a.tau + W;
             a.xnorm = a.dnorm + W;
-            a.status = (int *)(a.xnorm + W);
-            const size_t sm_sweep = gj_smem_bytes(N) + (tile_smem_bytes() + 127) / 128 * 128 + job_smem_bytes(N) +
-                                    (size_t)rup(N, 4) * 4;
+            a.dprev = a.xnorm + W;
+            a.status = (int *)(a.dprev + W);
+            a.tol = pol.tau_tolerance;
+            const size_t sm_sweep = gj_smem_bytes(N) + (pipe_smem_bytes(N) + 127) / 128 * 128 +
+                                    job_smem_bytes_slim(N) + (size_t)rup(N, 4) * 4;
             const size_t sm_pass = pass_smem_bytes(N, ncap);
             const size_t sm_res = (size_t)negf::KC * (negf::AP + negf::BP) * 16 + job_smem_bytes(N);
             if (N <= NT) rc = set_smem(k_mixed_sweep<1>, sm_sweep);
@@ -1334,14 +1682,18 @@ int negf_internal_mixed(negf_ctx *c, const double *h_E, const double *d_E, int n
                 else if (N <= 2 * NT) k_mixed_sweep<2><<<nw, NT, sm_sweep, st>>>(a);
                 else k_mixed_sweep<4><<<nw, NT, sm_sweep, st>>>(a);
                 CKM(cudaGetLastError());
-                k_mixed_pass<<<nw, NT, sm_pass, st>>>(a, PASS_X0);
+                k_mixed_pass<<<nw, NT, sm_pass, st>>>(a, PASS_X0, 0, 0);
                 CKM(cudaGetLastError());
-                k_mixed_residual<<<dim3(Nz, nw), NT, sm_res, st>>>(a);
-                CKM(cudaGetLastError());
-                k_mixed_pass<<<nw, NT, sm_pass, st>>>(a, PASS_BACK);
-                CKM(cudaGetLastError());
-                k_mixed_pass<<<nw, NT, sm_pass, st>>>(a, PASS_CORR);
-                CKM(cudaGetLastError());
+                // refinement steps; converged jobs (MIX_DONE) are skipped by the next ones
+                for (int it = 1; it <= pol.max_refinements; ++it) {
+                    const int last = it == pol.max_refinements;
+                    k_mixed_residual<<<dim3(Nz, nw), NT, sm_res, st>>>(a);
+                    CKM(cudaGetLastError());
+                    k_mixed_pass<<<nw, NT, sm_pass, st>>>(a, PASS_BACK, it, last);
+                    CKM(cudaGetLastError());
+                    k_mixed_pass<<<nw, NT, sm_pass, st>>>(a, PASS_CORR, it, last);
+                    CKM(cudaGetLastError());
+                }
                 CKM(cudaEventRecord(c->ev1, st));
                 CKM(cudaMemcpyAsync(tau.data(), a.tau, sizeof(double) * nw, cudaMemcpyDeviceToHost, st));
                 CKM(cudaMemcpyAsync(dn.data(), a.dnorm, sizeof(double) * nw, cudaMemcpyDeviceToHost, st));
@@ -1354,8 +1706,7 @@ int negf_internal_mixed(negf_ctx *c, const double *h_E, const double *d_E, int n
                 for (int w = 0; w < nw; ++w) {
                     const int q = m_jobs[w0 + w];
                     const double corr = xn[w] > 0 ? dn[w] / xn[w] : INFINITY;
-                    const double est = 2.0 * std::max(tau[w], 1.0) * corr * corr;
-                    if (status[w] == 0 && std::isfinite(tau[w]) && est < pol.tau_tolerance) {
+                    if (status[w] == MIX_DONE) {
                         h_tau_jobs[q] = tau[w];
                         h_info[q] = 0;
                         stats.n_mixed++;

@@ -132,12 +132,15 @@ __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.
 // x = 2^e (hi + lo) with hi = fp16(x 2^-e), lo = fp16(x 2^-e - hi): 22
 // significant bits.  The exponent e is chosen per row of A and per column of
 // B so that the largest magnitude maps into [2^14, 2^15) (fp16 overflows at
-// 65520); e is clamped to [-100, 100] so that 2^-e stays a normal float.
+// 65520).  e is clamped to [-60, 60], so that a row exponent plus a column
+// exponent is a normal float's exponent and an epilogue rescales with one
+// multiply (rows above 2^74 or below 2^-46 lie far outside the range of these
+// Green's functions; for them the clamp only costs fp16 range).
 __device__ __forceinline__ int scale_exponent(float maxabs) {
     if (!(maxabs > 0.0f)) return 0;
     const int ex = (int)((__float_as_uint(maxabs) >> 23) & 0xFF) - 127;  // floor(log2) for normals
     const int e = ex - 14;
-    return e < -100 ? -100 : (e > 100 ? 100 : e);
+    return e < -60 ? -60 : (e > 60 ? 60 : e);
 }
 __device__ __forceinline__ float exp2i(int e) { return __uint_as_float((uint32_t)(e + 127) << 23); }
 

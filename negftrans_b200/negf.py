@@ -92,10 +92,12 @@ class Engine:
         self.last_stats = st
         return tau, rc
 
-    def set_mixed_policy(self, threshold_window=None, eta_fp64_below=None, tau_tolerance=None):
+    def set_mixed_policy(self, threshold_window=None, eta_fp64_below=None, tau_tolerance=None,
+                         max_refinements=None):
         """Policy of the NEGF_MIXED path (Hartree): energies within threshold_window of a
         lead subband threshold run in FP64; eta below eta_fp64_below sends every job to
-        FP64; a refined job is accepted when 2 max(tau,1) (|d|/|x|)^2 < tau_tolerance.
+        FP64; a refined job is accepted when its estimated remaining |dtau| is below
+        tau_tolerance after at most max_refinements steps (else it is re-run in FP64).
         Unset arguments keep their current values."""
         p = MixedPolicy()
         check("negf_get_mixed_policy", lib().negf_get_mixed_policy(self._ctx, C.byref(p)))
@@ -105,6 +107,8 @@ class Engine:
             p.eta_fp64_below = float(eta_fp64_below)
         if tau_tolerance is not None:
             p.tau_tolerance = float(tau_tolerance)
+        if max_refinements is not None:
+            p.max_refinements = int(max_refinements)
         check("negf_set_mixed_policy", lib().negf_set_mixed_policy(self._ctx, C.byref(p)))
 
     def mixed_stats(self):
