@@ -1,16 +1,25 @@
 #!/usr/bin/env python
-"""Benchmark of the RGF hot path: (E,k) energy-point solves per second.
+"""Benchmark of the RGF hot path: (E,k) energy-point solves per second,
+mixed precision against FP64 on one B200.
 
 Workload (default): qpc_disorder_n221 -- N = 221 plane waves, N_z = 800
 slices, Gamma point, a QPC with 2 meV / 10 nm disorder, energies from the
-2048-point grid on [0, 40) meV, complex128 throughout.  One step = one
-transmission batch of `--batch` energies (a full sweep per energy: N_z block
-inverses + N_z-1 block products + the transmission trace).
+2048-point grid on [0, 40) meV.  `--workload qpc_disorder_n797` is the large
+block case (N = 797, N_z = 400, 1024 energies; a step there takes ~10-20 s).
 
-Output: one JSON line (rank 0).  `value` is device-timed with inputs resident
-in HBM; `e2e` goes through the C ABI with host buffers (copies included).
-`--impl reference` times the CPU restatement of the reference's algorithm
-(LAPACK zgetrf/zgetri + zgemm per block, one job per host thread) instead.
+--precision mixed (default): one step = negf_transmission(NEGF_MIXED) on
+`--batch` energies (default one mixed wave, one job per SM): split-fp16
+tensor-core factorization, FP64 residual refinement, FP64 re-run of rejected
+jobs -- every job of the step, whatever path it takes.  `value` = jobs / the
+device time of the call (CUDA events on the context's stream); `e2e` = jobs /
+the wall time of the same host-buffer call.  Outside the timed region the
+FP64 path runs every timed energy (at its best batch, two CTAs per SM):
+`fp64_value`, `mixed_over_fp64` and `max_abs_dT` over all of them.
+--precision fp64: the FP64 path alone (device-resident inputs, L2 flushed).
+
+Output: one JSON line (rank 0).  `--impl reference` times the CPU
+restatement of the reference's algorithm (LAPACK zgetrf/zgetri + zgemm per
+block, one job per host thread) instead.
 """
 from __future__ import annotations
 
@@ -28,7 +37,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "RGF energy-point solves/s"
+METRIC = "RGF energy-point solves/s, mixed vs FP64 on 1 B200 at max|ΔT|≤1e-6"  # the headline metric, verbatim
 # ncu dram bytes (read + write) of k_transmission per job-slice at N = 221, measured on a
 # 296-job, 16-slice launch (same per-slice work as the full workload)
 TRAFFIC_PER_JOB_SLICE_N221 = 66.423e9 / (296 * 16)
@@ -42,7 +51,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="qpc_disorder_n221")
-    ap.add_argument("--batch", type=int, default=296, help="energies per step and GPU")
+    ap.add_argument("--batch", type=int, default=0,
+                    help="energies per step and GPU (0: one mixed wave = the SM count, or 2x for fp64)")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
+                    help="mixed: NEGF_MIXED headline with the FP64 rate and max|dT| beside it")
     ap.add_argument("--nz", type=int, default=0,
                     help="profiling only: rebuild the workload with this many slices (same dz)")
     ap.add_argument("--cpu-threads", type=int, default=0, help="0 = all host cores (as many as host memory holds)")
@@ -243,8 +255,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-        "config": {"workload": args.workload, "N": p.N, "Nz": p.Nz, "energies": w.n_energy,
-                   "kpoints": len(p.kpt)},
+        "config": workload_config(args.workload, p.N, p.Nz, w.n_energy, len(p.kpt)),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": nth, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference (Fortran+MPI+FFTW+LAPACK) cannot be built on this image; its "
@@ -253,7 +264,7 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def run_ours(args):
+def run_ours_fp64(args):
     import torch
     import torch.distributed as dist
 
@@ -274,7 +285,7 @@ def run_ours(args):
     w = W.config(args.workload, nz=args.nz or None)
     pr = P.prepare(w.deck, w.V_eV)
     E_all = P.transmission_energies(pr.atomic, w.n_energy)
-    B = args.batch
+    B = args.batch or 2 * torch.cuda.get_device_properties(dev).multi_processor_count
     nk = len(pr.kpoint)
     eng = Engine(*pr.engine_args(), device=local)
 
@@ -341,10 +352,10 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-            "config": {"workload": args.workload, "N": N, "Nz": Nz, "energies_per_step_per_gpu": B,
-                       "kpoints": nk, "precision": "fp64", "parallelism": f"energy-sharded x{world}",
-                       "l2": "256 MB buffer written between timed steps; per-job workspace "
-                             f"{4 * ((N + 7) // 8 * 8) * N * 16 * min(B * nk, 148) / 1e6:.0f} MB > L2"},
+            "config": workload_config(args.workload, N, Nz, w.n_energy, nk),
+            "step": {"energies_per_gpu": B, "precision": "fp64", "parallelism": f"energy-sharded x{world}",
+                     "l2": "256 MB buffer written between timed steps; per-job workspace "
+                           f"{4 * ((N + 7) // 8 * 8) * N * 16 * min(B * nk, 148) / 1e6:.0f} MB > L2"},
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak,
                          # ncu dram read+write of this kernel per job-slice at N = 221 (a 296-job,
@@ -437,6 +448,190 @@ def run_ours(args):
         if rank == 0:
             line["ldos"] = {"jobs": B * nk, "seconds": el, "jobs_per_s": B * nk / el,
                             "device_ms": eng.last_stats.device_ms, "info": info_l}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if distributed:
+        dist.destroy_process_group()
+
+
+def workload_config(name, N, Nz, n_energy, nk):
+    """The workload identity, the same dict for this implementation and the reference arm."""
+    return {"workload": name, "N": N, "Nz": Nz, "energies": n_energy, "kpoints": nk}
+
+
+def mixed_mma_flops(N, Nz):
+    """Tensor-core flops (fp16 MMAs) the mixed sweep executes per solve: per
+    Gauss-Jordan panel of 32 columns, 24 MMAs (3 split products x 4 real
+    products x 2 K-steps of 16) per 128 x 32 output tile of the rows x the
+    columns outside the panel."""
+    ntr = -(-N // 128)
+    f = 0.0
+    for k0 in range(0, N, 32):
+        nbt = min(32, N - k0)
+        nrest = N - nbt
+        if nrest <= 0:
+            continue
+        f += ntr * (-(-nrest // 32)) * 24 * 2.0 * 128 * 32 * 16
+    return f * Nz
+
+
+def run_ours(args):
+    if args.precision == "fp64":
+        return run_ours_fp64(args)
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    distributed = "RANK" in os.environ and "MASTER_ADDR" in os.environ
+    if distributed:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+
+    from negftrans_b200 import prepare as P, workloads as W
+    from negftrans_b200._lib import NEGF_FP64, NEGF_MIXED
+    from negftrans_b200.negf import Engine
+
+    w = W.config(args.workload, nz=args.nz or None)
+    pr = P.prepare(w.deck, w.V_eV)
+    E_all = P.transmission_energies(pr.atomic, w.n_energy)
+    nk = len(pr.kpoint)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    eng = Engine(*pr.engine_args(), device=local)
+    # one mixed wave holds at most one job per SM (fewer when device memory is short)
+    eng.transmission(E_all[:8], precision=NEGF_MIXED)  # set-up call (allocations)
+    B = args.batch or sms
+    n_steps = args.warmup + args.steps
+    perm = np.random.default_rng(2024).permutation(len(E_all))
+    # a step is B energies per GPU: every rank holds the step's whole batch and the
+    # product multi-GPU layer splits it (contiguous slices, all-gather of tau)
+    idx = [perm[(s * world * B + np.arange(world * B)) % len(E_all)] for s in range(n_steps)]
+    E_host = [np.ascontiguousarray(E_all[i]) for i in idx]
+    if distributed:
+        from negftrans_b200.multigpu import ShardedEngine
+        solver = ShardedEngine(eng, pr.Nz, device=dev)
+    else:
+        solver = eng
+
+    def step(s):
+        t0 = time.perf_counter()
+        tau, info = solver.transmission(E_host[s], precision=NEGF_MIXED)
+        wall = time.perf_counter() - t0
+        return tau, info, wall, eng.last_stats.device_ms, eng.mixed_stats()
+
+    for s in range(args.warmup):
+        step(s)
+    torch.cuda.synchronize(dev)
+    if distributed:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    dev_ms, walls, taus, infos, stats = [], [], [], [], []
+    with ClockSampler(local) as clk:
+        for s in range(args.steps):
+            tau, info, wall, ms, st = step(args.warmup + s)
+            dev_ms.append(ms)
+            walls.append(wall)
+            taus.append(tau)
+            infos.append(info)
+            stats.append(st)
+    torch.cuda.synchronize(dev)
+    if distributed:
+        dist.barrier()
+    ms = statistics.mean(dev_ms)
+    wall = statistics.mean(walls)
+    if distributed:
+        t = torch.tensor([ms, wall], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, wall = float(t[0]), float(t[1])
+    jobs_per_step = B * nk * world
+    value = jobs_per_step / (ms * 1e-3)
+
+    # the FP64 path on the same energies, outside the timed region: its rate at
+    # its best batch (two CTAs per SM) and max|dT| of every timed mixed energy
+    timed_E = np.concatenate([E_host[args.warmup + s] for s in range(args.steps)])
+    timed_tau = np.concatenate(taus)
+    if world > 1:
+        # each rank checks its own share of the timed energies
+        from negftrans_b200.shard import energy_shard
+        lo, hi = energy_shard(len(timed_E), rank, world)
+        timed_E, timed_tau = timed_E[lo:hi], timed_tau[lo:hi]
+    F = 2 * sms
+    fp_ms, fp_jobs, tau64 = [], [], np.zeros_like(timed_tau)
+    eng.transmission(timed_E[:F], precision=NEGF_FP64)  # warm-up
+    for c0 in range(0, len(timed_E), F):
+        chunk = timed_E[c0:c0 + F]
+        t64, _ = eng.transmission(chunk, precision=NEGF_FP64)
+        tau64[c0:c0 + len(chunk)] = t64
+        if len(chunk) == F:
+            fp_ms.append(eng.last_stats.device_ms)
+            fp_jobs.append(len(chunk) * nk)
+    fp64_value = (sum(fp_jobs) / (sum(fp_ms) * 1e-3)) if fp_ms else None
+    dT = np.abs(timed_tau - tau64)
+    if distributed:
+        t = torch.tensor([fp64_value or 0.0, float(dT.max()) if len(dT) else 0.0], dtype=torch.float64, device=dev)
+        fv = t[:1].clone()
+        dist.all_reduce(fv, op=dist.ReduceOp.SUM)   # whole-job FP64 rate
+        dm_ = t[1:].clone()
+        dist.all_reduce(dm_, op=dist.ReduceOp.MAX)
+        fp64_value, dmax = float(fv.item()), float(dm_.item())
+    else:
+        dmax = float(dT.max()) if len(dT) else 0.0
+
+    line = None
+    if rank == 0:
+        N, Nz = pr.N, pr.Nz
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        except Exception:
+            pass
+        tc_peak = peaks.get("bf16_tflops", 1590.0)
+        fp64_peak = fp64_peak_tflops(torch, dev)
+        n_mixed = sum(s_["n_mixed"] for s_ in stats)
+        n_rej = sum(s_["n_fp64_rejected"] for s_ in stats)
+        n_pol = sum(s_["n_fp64_policy"] for s_ in stats)
+        waves = sum(-(-(s_["n_jobs"] - s_["n_fp64_policy"]) // max(1, s_["jobs_per_wave"])) for s_ in stats)
+        pol = eng.mixed_policy()["max_refinements"]
+        mma = mixed_mma_flops(N, Nz) * n_mixed / args.steps
+        mixed_ms = statistics.mean(s_["mixed_ms"] for s_ in stats)
+        cs = clk.summary()
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64 (split-fp16 tensor products, f32 accumulate) + f64 refinement",
+            "data": "synthetic",
+            "config": workload_config(args.workload, N, Nz, w.n_energy, nk),
+            "step": {"energies_per_gpu": B, "precision": "mixed (NEGF_MIXED)",
+                     "parallelism": f"energy-sharded x{world}",
+                     "l2": f"per-job factor storage ~{8 * N * N * Nz / 1e6:.0f} MB > L2 (inputs larger than L2)"},
+            "fp64_value": fp64_value,
+            "mixed_over_fp64": (value / fp64_value) if fp64_value else None,
+            "max_abs_dT": dmax, "dT_energies": int(len(dT)) * world,
+            "energies_covered": int(len(np.unique(timed_E))),
+            "accepted_mixed": n_mixed, "fp64_rejected": n_rej, "fp64_policy": n_pol,
+            "roofline": {"bound": "tensor", "kernel": "k_mixed_sweep (tcgen05 kind::f16 trailing updates)",
+                         "achieved": mma / (mixed_ms * 1e-3) / 1e12, "peak": tc_peak, "unit": "TFLOP/s",
+                         "frac": mma / (mixed_ms * 1e-3) / 1e12 / tc_peak, "traffic": None,
+                         "peak_source": "MEASURED_PEAKS.json bf16_tflops (dense fp16 runs at the bf16 rate)",
+                         "flops_note": "executed fp16 MMA flops of the sweep's trailing updates per step "
+                                       "(3 split products x 4 real products) over the mixed device time",
+                         "reference_equiv_tflops": flops_per_solve(N, Nz) * jobs_per_step / (ms * 1e-3) / 1e12,
+                         "fp64_peak_tflops": fp64_peak},
+            "gpu_launches": waves * (2 + 3 * pol) + (args.steps if n_rej else 0),
+            "clocks": cs,
+            "e2e": {"value": jobs_per_step / wall, "unit": UNIT, "h2d_bytes_per_step": 8 * B,
+                    "d2h_bytes_per_step": 8 * B, "api": "negf_transmission(NEGF_MIXED) with host buffers"},
+            "singular_jobs": int(sum(1 for i in infos if i)),
+        }
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        nth = host_threads(args.cpu_threads, oracle_job_bytes(pr))
+        r, t = cpu_rate(pr, E_all[::7], nth)
+        line["cpu_baseline"] = {"value": r, "unit": UNIT, "cores": nth, "kind": "port",
+                                "sample": f"{nth} sweeps of this workload, one per thread, {t[0]:.1f} s"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     eng.close()

@@ -281,6 +281,12 @@ int negf_density_neq(negf_ctx *ctx, int32_t n_circle, int32_t n_window, double m
  * (main.f90:306-351): density (Nx,Ny,Nz) = Im(diag of PtoR(dm slice)) * scale. */
 int negf_dm_real(negf_ctx *ctx, const double *dm, int32_t Nx, int32_t Ny, double scale,
                  double *density);
+/* negf_dm_real for a slab of nslices consecutive z-slices (any slab of the
+ * device, the basis of ctx): dm (N,N,nslices) complex -> density
+ * (Nx,Ny,nslices).  The per-rank step after the z reduce-scatter of a
+ * multi-GPU density (main.f90:306-340 on each rank's slices). */
+int negf_dm_real_slab(negf_ctx *ctx, const double *dm, int32_t nslices, int32_t Nx, int32_t Ny,
+                      double scale, double *density);
 
 /* Local_Density_Of_State, negf.f90:176-236, summed over k-points for the
  * energies i_e0 .. i_e0+n_chunk-1 (0-based) of the grid

@@ -28,7 +28,7 @@ EXPORTS = (
     "negf_density_real", "negf_ldos", "negf_basis_k", "negf_transmission_batch",
     "negf_density_neq", "negf_dm_real", "negf_set_variant", "negf_autotune", "negf_vhat_gpu",
     "negf_density_accumulate", "negf_tc_product_check", "negf_tc_inverse_check",
-    "negf_set_mixed_policy", "negf_get_mixed_policy", "negf_get_mixed_stats",
+    "negf_set_mixed_policy", "negf_get_mixed_policy", "negf_get_mixed_stats", "negf_dm_real_slab",
 )
 # every symbol include/negf_mlp.h declares
 MLP_EXPORTS = (
@@ -116,6 +116,7 @@ def lib():
     L.negf_density_neq.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
                                    C.c_double, C.c_double, _dp, C.POINTER(Stats)]
     L.negf_dm_real.argtypes = [C.c_void_p, _dp, C.c_int32, C.c_int32, C.c_double, _dp]
+    L.negf_dm_real_slab.argtypes = [C.c_void_p, _dp, C.c_int32, C.c_int32, C.c_int32, C.c_double, _dp]
     L.negf_set_variant.argtypes = [C.c_void_p, C.c_int32]
     L.negf_density_accumulate.argtypes = [C.c_void_p, _dp, _dp, C.c_int32, _dp, C.POINTER(Stats)]
     L.negf_vhat_gpu.argtypes = [_dp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _dp]

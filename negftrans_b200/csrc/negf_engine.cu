@@ -1611,16 +1611,22 @@ extern "C" int negf_vhat_gpu(const double *vreal, int32_t Nx, int32_t Ny, int32_
 
 extern "C" int negf_dm_real(negf_ctx *c, const double *dm, int32_t Nx, int32_t Ny, double scale,
                             double *density) {
-    if (!c || !dm || !density || Nx < 1 || Ny < 1) return NEGF_ERR_ARG;
+    if (!c) return NEGF_ERR_ARG;
+    return negf_dm_real_slab(c, dm, c->Nz, Nx, Ny, scale, density);
+}
+
+extern "C" int negf_dm_real_slab(negf_ctx *c, const double *dm, int32_t nslices, int32_t Nx, int32_t Ny,
+                                 double scale, double *density) {
+    if (!c || !dm || !density || Nx < 1 || Ny < 1 || nslices < 1) return NEGF_ERR_ARG;
     if (cudaSetDevice(c->device) != cudaSuccess) return NEGF_ERR_CUDA;
-    const size_t per = (size_t)c->N * c->N * c->Nz, nd = (size_t)Nx * Ny * c->Nz;
+    const size_t per = (size_t)c->N * c->N * nslices, nd = (size_t)Nx * Ny * nslices;
     double2 *d_G = nullptr;
     double *d_dens = nullptr;
     if (cudaMalloc(&d_G, sizeof(double2) * per) != cudaSuccess) { cudaGetLastError(); return NEGF_ERR_NOMEM; }
     if (cudaMalloc(&d_dens, sizeof(double) * nd) != cudaSuccess) { cudaGetLastError(); cudaFree(d_G); return NEGF_ERR_NOMEM; }
     int rc = 0;
     if (cudaMemcpyAsync(d_G, dm, sizeof(double2) * per, cudaMemcpyHostToDevice, c->stream) != cudaSuccess) rc = NEGF_ERR_CUDA;
-    if (!rc) rc = launch_ptor(c, d_G, c->Nz, Nx, Ny, scale, d_dens, nullptr, c->stream);
+    if (!rc) rc = launch_ptor(c, d_G, nslices, Nx, Ny, scale, d_dens, nullptr, c->stream);
     if (!rc && (cudaMemcpyAsync(density, d_dens, sizeof(double) * nd, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
                 cudaStreamSynchronize(c->stream) != cudaSuccess))
         rc = NEGF_ERR_CUDA;

@@ -111,6 +111,12 @@ class Engine:
             p.max_refinements = int(max_refinements)
         check("negf_set_mixed_policy", lib().negf_set_mixed_policy(self._ctx, C.byref(p)))
 
+    def mixed_policy(self):
+        """The current NEGF_MIXED policy (dict)."""
+        p = MixedPolicy()
+        check("negf_get_mixed_policy", lib().negf_get_mixed_policy(self._ctx, C.byref(p)))
+        return {k: getattr(p, k) for k, _ in p._fields_ if k != "pad"}
+
     def mixed_stats(self):
         """Counts and device times of the last NEGF_MIXED call (dict)."""
         s = MixedStats()
@@ -195,6 +201,17 @@ class Engine:
         dens = np.zeros((N_x, N_y, self.Nz), np.float64, order="F")
         check("negf_dm_real", lib().negf_dm_real(self._ctx, dm.ctypes.data_as(_dp), N_x, N_y,
                                                  self.Nz / (LX_A * LY_A * LZ_A), dens.ctypes.data_as(_dp)))
+        return dens
+
+    def dm_real_slab(self, dm_slab, N_x, N_y, LX_A, LY_A, LZ_A):
+        """Density (N_x, N_y, n) in Angstrom^-3 of n consecutive slices of a Density_Matrix
+        (N, N, n) (the GPU PtoR of main.f90:306-351 on one slab)."""
+        dm = np.asfortranarray(dm_slab, dtype=np.complex128)
+        n = dm.shape[2]
+        dens = np.zeros((N_x, N_y, n), np.float64, order="F")
+        check("negf_dm_real_slab", lib().negf_dm_real_slab(
+            self._ctx, dm.ctypes.data_as(_dp), n, N_x, N_y, self.Nz / (LX_A * LY_A * LZ_A),
+            dens.ctypes.data_as(_dp)))
         return dens
 
     def ldos(self, e_lo, e_hi, N_E, LDOS_GRID, N_x, N_y, LX_A, LY_A, LZ_A):
