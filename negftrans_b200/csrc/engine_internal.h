@@ -33,6 +33,9 @@ struct negf_ctx {
     negf_mixed_stats mixed_stats{};
     void *d_mixed = nullptr;  // per-wave factor storage and scratch
     size_t mixed_bytes = 0;
+    // -c2 V(G_i - G_j) of every slice (energy- and k-independent part of D_k),
+    // complex FP64 [Nz][N][ld] column-major, built on the first mixed call
+    double2 *d_voff = nullptr;
 };
 
 // FP64 sweeps of the listed jobs (energy index ie[q] into d_E, k-point ik[q])

@@ -54,6 +54,17 @@ __device__ __forceinline__ float2 crcp(float2 a) {
     const double x = a.x, y = a.y, s = 1.0 / (x * x + y * y);
     return make_float2((float)(x * s), (float)(-y * s));
 }
+// 1/a in FP32 with a power-of-two prescale, so |a|^2 neither overflows nor
+// underflows: a = 2^e (u + i v) with max(|u|, |v|) in [1, 2), 1/a =
+// 2^-e (u - i v) / (u^2 + v^2); a few ulp.  Zero or non-finite a gives a
+// non-finite result.
+__device__ __forceinline__ float2 crcp_f32(float2 a) {
+    const int eb = (__float_as_int(fmaxf(fabsf(a.x), fabsf(a.y))) >> 23) & 0xff;
+    const float sc = __int_as_float((254 - min(max(eb, 1), 253)) << 23);  // 2^(127 - eb)
+    const float u = a.x * sc, v = a.y * sc;
+    const float r = __frcp_rn(fmaf(u, u, v * v)) * sc;
+    return make_float2(u * r, -v * r);
+}
 __device__ __forceinline__ float cabs1f(float2 a) { return fabsf(a.x) + fabsf(a.y); }
 
 // ------------------------------------------------------- tile shared memory

@@ -915,6 +915,7 @@ int negf_ctx_destroy(negf_ctx *c) {
     cudaFree(c->d_ax); cudaFree(c->d_ay); cudaFree(c->d_kw);
     cudaFree(c->d_ws); cudaFree(c->d_E); cudaFree(c->d_tau); cudaFree(c->d_tau_jobs); cudaFree(c->d_info);
     cudaFree(c->d_mixed);
+    cudaFree(c->d_voff);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->stream) cudaStreamDestroy(c->stream);

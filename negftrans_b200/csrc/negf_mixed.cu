@@ -19,6 +19,7 @@
 // x0 + d in FP64.  Jobs whose correction is not small enough, and jobs the
 // policy sends there (near a subband threshold, small eta), are re-run by the
 // FP64 path.
+#include <cuda.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -40,152 +41,99 @@ namespace {
 // ------------------------------------------------------------ shared memory
 // Per-CTA state of the FP32 Gauss-Jordan inverse.
 struct GjSmem {
-    int *prow;       // [N] pivot row of column k
-    int *iprow;      // [N] inverse permutation
-    int *inP;        // [N] sub-panel tag (1..4) of the current panel's pivot rows, else 0
-    uint32_t *rkey;  // [2][NWARP] warp candidate keys, double-buffered by step parity
-    float2 *rrec;    // [2][NWARP] reciprocal of each warp's candidate
-    float2 *cand;    // [2][NWARP][8] each warp's candidate row (sub-panel columns)
-    float2 *sX;      // [32][8]  rows P_<p of sub-panel p before its update
-    float2 *sY;      // [8][32]  rows P_p of the earlier sub-panels
-    float *rmax;     // [2][TM]  per-thread-half row maxima while staging W
+    int *prow;       // [N] row permutation of the stored factors (the identity here)
+    int *iprow;      // [N] its inverse
+    float2 *sP;      // [32][32] inverse of the current diagonal block, P(r, c) at r * 32 + c
+    int *spr;        // [32] pivot lane of each step of the diagonal-block inverse
+    float2 *srow;    // [2][32] the pivot row of a step, double-buffered by step parity
+    float *rmax;     // [2][TM]  per-thread-half row maxima while staging W (self test)
 };
 __host__ __device__ inline int rup(int a, int b) { return (a + b - 1) / b * b; }
 __host__ __device__ inline size_t gj_smem_bytes(int N) {
     const int n4 = rup(N, 4);
-    size_t b = 3 * (size_t)n4 * 4;
-    b += 2 * NWARP * 4 + 2 * NWARP * 8 + 2 * NWARP * 8 * 8;
-    b += 32 * 8 * 8 + 8 * 32 * 8 + 2 * TM * 4;
+    size_t b = 32 * 32 * 8 + 32 * 4 + 2 * 32 * 8 + 2 * TM * 4;
+    b += 2 * (size_t)n4 * 4;
     return (b + 127) / 128 * 128;
 }
 __device__ inline GjSmem carve_gj(unsigned char *base, int N) {
     GjSmem s;
     const int n4 = rup(N, 4);
-    s.prow = (int *)base;
+    s.sP = (float2 *)base;
+    s.srow = s.sP + 32 * 32;
+    s.spr = (int *)(s.srow + 2 * 32);
+    s.rmax = (float *)(s.spr + 32);
+    s.prow = (int *)(s.rmax + 2 * TM);
     s.iprow = s.prow + n4;
-    s.inP = s.iprow + n4;
-    s.rkey = (uint32_t *)(s.inP + n4);
-    s.rrec = (float2 *)(s.rkey + 2 * NWARP);
-    s.cand = s.rrec + 2 * NWARP;
-    s.sX = s.cand + 2 * NWARP * 8;
-    s.sY = s.sX + 32 * 8;
-    s.rmax = (float *)(s.sY + 8 * 32);
     return s;
 }
+__device__ inline void gj_identity(const GjSmem &s, int N) {
+    for (int i = threadIdx.x; i < N; i += NT) { s.prow[i] = i; s.iprow[i] = i; }
+}
 
-// ------------------------------------------------------------- pivot steps
+// ------------------------------------------------ diagonal-block inverse
 // Sortable 32-bit key: |re|+|im| bits (non-negative floats order as
 // unsigned integers) with the low 10 bits replaced by 1023 - row, so the
 // warp maximum is one redux and ties go to the lower row.  Magnitudes that
-// differ only in those bits (relative 2^-13) count as a tie.  N <= 1023.
+// differ only in those bits (relative 2^-13) count as a tie.
 __device__ __forceinline__ uint32_t pivot_key32(float v, int row) {
     return (__float_as_uint(v) & ~0x3FFu) | (uint32_t)(0x3FF - row);
 }
 
-template <int RPT>
-__device__ inline int warp_pivot_f(const float2 (&f)[RPT], unsigned used, int buf, const GjSmem &s) {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    uint32_t key = 0;
-    int rbest = -1;
+// P = inv(A(k0:k0+m, k0:k0+m)) (m <= 32) by one warp: lane r holds row r of
+// the block in registers, padded to 32 x 32 with identity rows; Gauss-Jordan
+// with implicit partial pivoting inside the block (largest |re|+|im| among
+// the unused rows, as zgetf2 chooses).  The row shifts left by one column per
+// step, so step k always pivots on R[0] and appends the inverse column at
+// R[31] (after 32 steps R[j] is the in-place result's column j); the rolled
+// loop keeps every register index static.  Each step is uniform across the
+// warp: one redux for the pivot lane p, the pivot row by shuffles from p, its
+// reciprocal in FP32 on every lane.  P is written to s.sP in natural order,
+// P(r, c) = R(pr[r], ipr[c]) (pr[k] the pivot lane of step k), with the
+// identity on the padding.  Returns the 1-based step of the first zero pivot
+// (0 if none).
+__device__ inline int invert_diag_warp(const float2 *__restrict__ A, int ld, int k0, int m, const GjSmem &s) {
+    const int lane = threadIdx.x & 31;
+    const bool valid = lane < m;
+    float2 R[32];
 #pragma unroll
-    for (int r = 0; r < RPT; ++r) {
-        if (!((used >> r) & 1u)) {
-            float v = cabs1f(f[r]);
-            if (!(v == v)) v = 0.0f;  // NaN rows rank as zero pivots
-            const uint32_t k = pivot_key32(v, tid + NT * r);
-            if (k > key) { key = k; rbest = r; }
+    for (int j = 0; j < 32; ++j)
+        R[j] = (valid && j < m) ? A[(k0 + lane) + (size_t)ld * (k0 + j)]
+                                : make_float2((!valid && j == lane) ? 1.0f : 0.0f, 0.0f);
+    int *spr = s.spr;
+    bool used = false;
+    int myk = 0, info = 0;
+#pragma unroll 1
+    for (int k = 0; k < 32; ++k) {
+        float v = cabs1f(R[0]);
+        if (!(v == v)) v = 0.0f;  // NaN rows rank as zero pivots
+        const uint32_t wk = __reduce_max_sync(0xffffffffu, used ? 0u : pivot_key32(v, lane));
+        // 32 - k unused lanes remain, so p is one of them
+        const int p = 0x3FF - (int)(wk & 0x3FFu);
+        if ((wk >> 10) == 0 && info == 0) info = k + 1;
+        const bool piv = lane == p;
+        const float2 d = crcp_f32(make_float2(__shfl_sync(0xffffffffu, R[0].x, p),
+                                              __shfl_sync(0xffffffffu, R[0].y, p)));
+        // the pivot row becomes its scaled copy: base 0, multiplier -1
+        const float2 f = piv ? make_float2(-1.0f, 0.0f) : R[0];
+#pragma unroll
+        for (int j = 1; j < 32; ++j) {
+            const float2 rp = cmul(make_float2(__shfl_sync(0xffffffffu, R[j].x, p),
+                                               __shfl_sync(0xffffffffu, R[j].y, p)), d);
+            R[j - 1] = cfms(f, rp, piv ? make_float2(0.f, 0.f) : R[j]);
         }
-    }
-    const uint32_t wk = __reduce_max_sync(0xffffffffu, key);
-    if (lane == 0) s.rkey[buf * NWARP + warp] = wk;
-    if (wk != 0 && key == wk) {
-#pragma unroll
-        for (int r = 0; r < RPT; ++r)
-            if (r == rbest) s.rrec[buf * NWARP + warp] = crcp(f[r]);
-        return rbest;
-    }
-    return -1;
-}
-
-// Gauss-Jordan steps on the 8 columns [kb, kb+nbe) held in registers (row
-// tid + NT*r in w[r][.]), implicit partial pivoting (largest |re|+|im| among
-// unused rows, as zgetf2 chooses).  One CTA barrier per step: each warp
-// publishes its candidate key, reciprocal and updated row; the next column
-// is updated first so its search overlaps the rest of the row update.
-template <int RPT>
-__device__ inline void factor_sub8(float2 (&w)[RPT][8], int kb, int nbe, unsigned &used, int &info, int tag,
-                                   const GjSmem &s) {
-    const int tid = threadIdx.x, warp = tid >> 5;
-    float2 f[RPT];
-#pragma unroll
-    for (int r = 0; r < RPT; ++r) f[r] = w[r][0];
-    int mine = warp_pivot_f<RPT>(f, used, 0, s);
-    if (mine >= 0) {
-#pragma unroll
-        for (int r = 0; r < RPT; ++r)
-            if (r == mine) {
-#pragma unroll
-                for (int jj = 0; jj < 8; ++jj) s.cand[warp * 8 + jj] = w[r][jj];
-            }
-    }
-#pragma unroll
-    for (int kk = 0; kk < 8; ++kk) {
-        if (kk < nbe) {
-            const int buf = kk & 1;
-            __syncthreads();
-            const uint32_t *rk = s.rkey + buf * NWARP;
-            uint32_t key = rk[0];
-            int q = 0;
-#pragma unroll
-            for (int j = 1; j < NWARP; ++j) {
-                const uint32_t k = rk[j];
-                if (k > key) { key = k; q = j; }
-            }
-            const float2 d = s.rrec[buf * NWARP + q];
-            const float2 *srow = s.cand + (buf * NWARP + q) * 8;
-            const int p = 0x3FF - (int)(key & 0x3FFu);
-            if ((key >> 10) == 0 && info == 0) info = kb + kk + 1;
-#pragma unroll
-            for (int r = 0; r < RPT; ++r)
-                if (tid + NT * r == p) used |= 1u << r;
-            if (tid == 0) { s.prow[kb + kk] = p; s.inP[p] = tag; }
-            const bool more = (kk + 1 < 8) && (kk + 1 < nbe);
-            float2 gm[RPT];
-#pragma unroll
-            for (int r = 0; r < RPT; ++r) gm[r] = (tid + NT * r == p) ? make_float2(0.f, 0.f) : cmul(w[r][kk], d);
-            if (kk + 1 < 8) {
-                float2 fn[RPT];
-                const float2 rn = srow[(kk + 1) & 7];
-#pragma unroll
-                for (int r = 0; r < RPT; ++r)
-                    fn[r] = (tid + NT * r == p) ? cmul(rn, d) : cfms(gm[r], rn, w[r][(kk + 1) & 7]);
-                mine = more ? warp_pivot_f<RPT>(fn, used, buf ^ 1, s) : -1;
-            } else {
-                mine = -1;
-            }
-#pragma unroll
-            for (int r = 0; r < RPT; ++r) {
-                if (tid + NT * r == p) {
-#pragma unroll
-                    for (int jj = 0; jj < 8; ++jj) w[r][jj] = (jj == kk) ? d : cmul(srow[jj], d);
-                } else {
-#pragma unroll
-                    for (int jj = 0; jj < 8; ++jj)
-                        w[r][jj] = (jj == kk) ? make_float2(-gm[r].x, -gm[r].y) : cfms(gm[r], srow[jj], w[r][jj]);
-                }
-            }
-            if (mine >= 0) {
-                float2 *dst = s.cand + ((buf ^ 1) * NWARP + warp) * 8;
-#pragma unroll
-                for (int r = 0; r < RPT; ++r)
-                    if (r == mine) {
-#pragma unroll
-                        for (int jj = 0; jj < 8; ++jj) dst[jj] = w[r][jj];
-                    }
-            }
+        R[31] = make_float2(-(f.x * d.x - f.y * d.y), -(f.x * d.y + f.y * d.x));
+        if (piv) {
+            used = true;
+            myk = k;
         }
+        if (lane == 0) spr[k] = p;
     }
-    __syncthreads();
+    __syncwarp();
+    float2 *sP = s.sP;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) sP[myk * 32 + spr[j]] = R[j];
+    __syncwarp();
+    return info > m ? 0 : info;
 }
 
 // ------------------------------------------------- trailing-update staging
@@ -219,34 +167,35 @@ __device__ inline void stage_w(const TileSmem &t, const GjSmem &s, const float2 
 }
 
 // ---------------------------------------------- pipelined trailing update
-// The panel's W (N x nbt) and its pivot rows of the other columns
-// (nbt x (N - nbt)) are converted once per panel into split-fp16 tiles in the
-// CTA's global scratch (W: TM-row tiles of 32 KB with one exponent per row; B:
-// PTN-column tiles of 8 KB with one exponent per column).  The TM x PTN output
-// tiles then run through a warp-specialised pipeline whose roles synchronise
-// only through mbarriers:
-//   warp 0 (producer)   bulk copies of the W tile of each row tile (one
-//                       buffer), the B tile (three buffers) and the old C
-//                       values (one bulk copy per column, three buffers) of
-//                       tile t+3 as soon as tile t's C has been stored, and
-//                       the bulk stores of finished C tiles;
+// The panel's W (N x nbt) and its rows of the other columns (nbt x (N - nbt))
+// are converted once per panel into split-fp16 tiles in the CTA's global
+// scratch (W: TM-row tiles of 32 KB with one exponent per row; B: PTN-column
+// tiles of 8 KB with one exponent per column).  The TM x PTN output tiles then
+// run through a warp-specialised pipeline whose roles synchronise only
+// through mbarriers:
+//   warp 0, lane 0      bulk copies of the W tile of each row tile (one
+//                       buffer) and of the B tile (three buffers), one TMA
+//                       tile load of the old C values (three buffers) of tile
+//                       t+3 as soon as tile t's C has been stored, and the
+//                       TMA tile stores of finished C tiles;
 //   warp 1, lane 0      the tcgen05 MMAs of each tile into one of two
 //                       tensor-memory accumulators;
 //   warps 4-7           the epilogue: accumulator (tcgen05.ld, one lane
 //                       quadrant per warp) times 2^(row + column exponent)
 //                       added to the old C in shared memory.
-// The leading dimension must be a multiple of 8 (16-byte bulk copies of whole
-// columns; rows N..ld-1 travel unchanged).
+// The leading dimension must be a multiple of 8 (16-byte TMA strides; rows
+// N..ld-1 are never touched).
 constexpr int PTN = 32;                         // columns of an output tile
 constexpr int NCB = 3;                          // C buffers
 constexpr int NBB = 3;                          // B buffers
 constexpr uint32_t WTILE = 4u * TM * KB * 2;     // 32 KB
 constexpr uint32_t BTILE = 4u * PTN * KB * 2;    // 8 KB
 constexpr uint32_t CTILE = (uint32_t)TM * PTN * 8;  // 32 KB: PTN columns of TM float2
+static_assert(NCB * CTILE >= 32u * NT * 8, "panel_w stages 32 values per thread in the C buffers");
 struct Pipe {
     unsigned char *sW;
-    unsigned char *sB[NBB];
-    unsigned char *sC[NCB];
+    unsigned char *sB;               // NBB buffers of BTILE bytes (no arrays of pointers, so the
+    unsigned char *sC;               // struct stays in registers): NCB buffers of CTILE bytes
     uint64_t *fullW, *emptyW;        // [1], [1]
     uint64_t *fullB, *emptyB;        // [NBB]
     uint64_t *fullC, *doneC;         // [NCB]: C loaded / C updated by the epilogue
@@ -275,8 +224,8 @@ __device__ inline Pipe carve_pipe(unsigned char *base, int N, unsigned char *gsc
     const int ntr = (N + TM - 1) / TM, ntc = (N + PTN - 1) / PTN;
     unsigned char *q = base;
     P.sW = q; q += WTILE;
-    for (int i = 0; i < NCB; ++i) { P.sC[i] = q; q += CTILE; }
-    for (int i = 0; i < NBB; ++i) { P.sB[i] = q; q += BTILE; }
+    P.sC = q; q += NCB * CTILE;
+    P.sB = q; q += NBB * BTILE;
     uint64_t *bar = (uint64_t *)q;
     P.fullW = bar; P.emptyW = bar + 1;
     P.fullB = bar + 2; P.emptyB = P.fullB + NBB;
@@ -333,17 +282,33 @@ __device__ __forceinline__ void bulk_copy(void *dst, const void *src, uint32_t b
                  "l"(src), "r"(bytes), "r"(tc::smem_u32(bar))
                  : "memory");
 }
-// shared -> global bulk store in the issuing thread's bulk group
-__device__ __forceinline__ void bulk_store(void *dst, const void *src, uint32_t bytes) {
-    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(dst), "r"(tc::smem_u32(src)),
-                 "r"(bytes)
-                 : "memory");
-}
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
 // this thread's committed bulk stores have finished reading shared memory
 __device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
 // ... and have completed
 __device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+
+// The working matrices of the C tiles: a 4-D tensor map (row, column, matrix,
+// CTA) of complex FP32 elements moved as 8-byte words, N x N valid elements
+// per matrix, and the (matrix, CTA) coordinates of the one being inverted.
+struct CMat {
+    const CUtensorMap *tm;
+    int z, w;
+};
+__device__ __forceinline__ void tma_load4(void *dst, const CUtensorMap *tm, int x, int y, int z, int w,
+                                          uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5}], [%6];\n" ::"r"(tc::smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(z), "r"(w), "r"(tc::smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void tma_store4(const CUtensorMap *tm, int x, int y, int z, int w, const void *src) {
+    asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3, %4}], [%5];\n" ::"l"(
+                     reinterpret_cast<uint64_t>(tm)),
+                 "r"(x), "r"(y), "r"(z), "r"(w), "r"(tc::smem_u32(src))
+                 : "memory");
+}
 
 // MMAs of one K chunk: A (TM x KB, plane stride TM*KB*2), B (n x KB, plane
 // stride n*KB*2), D re at d0, im at d0 + n.  first = overwrite.
@@ -370,35 +335,72 @@ __device__ inline void issue_split_mma(uint32_t a0, uint32_t b0, int n, uint32_t
     }
 }
 
-// W tiles: row r of the panel [k0, k0+nbt) of A, two threads per row (lanes
-// l and l+16 of a warp, 16 K values each).
-__device__ inline void convert_w(const Pipe &P, const float2 *__restrict__ A, int ld, int N, int k0, int nbt) {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, h = lane >> 4;
-    const int ntr = (N + TM - 1) / TM;
-    for (int r0 = warp * 16; r0 < ntr * TM; r0 += NWARP * 16) {
-        const int row = r0 + (lane & 15);
-        float2 v[16];
-        float m = 0.0f;
+// The panel's column block once its diagonal block is inverted (P in s.sP):
+// W = -A(:, K) P on the rows outside K and P - I on the rows of K, so that
+// the rank-m update A(:, J) += W A_old(K, J) of every other column J completes
+// the elimination.  A(:, K) receives its final values (W outside K, P on K);
+// W goes to the split-fp16 W tiles with one exponent per row.  One thread per
+// row; the row's panel values are staged in the pipe's C buffers (idle
+// between trailing updates) so that the k loop stays rolled.  Tile rows
+// N .. ntr*TM-1 are zero.
+__device__ inline void panel_w(const Pipe &P, const GjSmem &s, float2 *__restrict__ A, int ld, int N, int k0,
+                               int m) {
+    const int ntr = (N + TM - 1) / TM, tid = threadIdx.x;
+    float2 *xs = (float2 *)P.sC;  // [32][NT]: 64 KB of the three contiguous C buffers
+    for (int row = tid; row < ntr * TM; row += NT) {
+        float2 w[32];
+        const int rk = row - k0;
+        if (row >= N) {
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-            const int kk = 16 * h + q;
-            v[q] = (row < N && kk < nbt) ? A[row + (size_t)ld * (k0 + kk)] : make_float2(0.f, 0.f);
-            m = fmaxf(m, fmaxf(fabsf(v[q].x), fabsf(v[q].y)));
+            for (int c = 0; c < 32; ++c) w[c] = make_float2(0.f, 0.f);
+        } else if (rk >= 0 && rk < m) {
+#pragma unroll
+            for (int c = 0; c < 32; ++c) {
+                const float2 p = s.sP[rk * 32 + c];
+                if (c < m) A[row + (size_t)ld * (k0 + c)] = p;
+                w[c] = (c == rk) ? make_float2(p.x - 1.0f, p.y) : p;
+            }
+        } else {
+            // all 32 loads in flight before the first staging store
+#pragma unroll
+            for (int k = 0; k < 32; ++k) w[k] = (k < m) ? A[row + (size_t)ld * (k0 + k)] : make_float2(0.f, 0.f);
+#pragma unroll
+            for (int k = 0; k < 32; ++k) xs[k * NT + tid] = w[k];
+#pragma unroll
+            for (int c = 0; c < 32; ++c) w[c] = make_float2(0.f, 0.f);
+#pragma unroll 1
+            for (int k = 0; k < m; ++k) {
+                const float2 x = xs[k * NT + tid];
+                const float4 *pk = (const float4 *)(s.sP + k * 32);
+#pragma unroll
+                for (int c2 = 0; c2 < 16; ++c2) {
+                    const float4 p = pk[c2];
+                    w[2 * c2] = cfma(x, make_float2(p.x, p.y), w[2 * c2]);
+                    w[2 * c2 + 1] = cfma(x, make_float2(p.z, p.w), w[2 * c2 + 1]);
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < 32; ++c) {
+                w[c] = make_float2(-w[c].x, -w[c].y);
+                if (c < m) A[row + (size_t)ld * (k0 + c)] = w[c];
+            }
         }
-        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 16));
-        const int e = tc::scale_exponent(m);
+        float mx = 0.0f;
+#pragma unroll
+        for (int c = 0; c < 32; ++c) mx = fmaxf(mx, fmaxf(fabsf(w[c].x), fabsf(w[c].y)));
+        const int e = tc::scale_exponent(mx);
         const float sc = tc::exp2i(-e);
-        if (h == 0) P.rexpW[row] = e;
+        P.rexpW[row] = e;
         unsigned char *tile = P.wt + (size_t)(row / TM) * WTILE;
 #pragma unroll
-        for (int g = 0; g < 2; ++g) {
+        for (int g = 0; g < 4; ++g) {
             __align__(16) __half rh[8], rl[8], ih[8], il[8];
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
-                const tc::Split2 a = tc::split_fp16(v[8 * g + q].x * sc), b = tc::split_fp16(v[8 * g + q].y * sc);
-                rh[q] = a.hi; rl[q] = a.lo; ih[q] = b.hi; il[q] = b.lo;
+                const tc::Split2 u = tc::split_fp16(w[8 * g + q].x * sc), v = tc::split_fp16(w[8 * g + q].y * sc);
+                rh[q] = u.hi; rl[q] = u.lo; ih[q] = v.hi; il[q] = v.lo;
             }
-            const uint32_t off = tc::kmajor_offset(row % TM, 8 * (2 * h + g), KB);
+            const uint32_t off = tc::kmajor_offset(row % TM, 8 * g, KB);
             *(uint4 *)(tile + 0 * (TM * KB * 2) + off) = *(const uint4 *)rh;
             *(uint4 *)(tile + 1 * (TM * KB * 2) + off) = *(const uint4 *)rl;
             *(uint4 *)(tile + 2 * (TM * KB * 2) + off) = *(const uint4 *)ih;
@@ -407,9 +409,8 @@ __device__ inline void convert_w(const Pipe &P, const float2 *__restrict__ A, in
     }
 }
 // B tiles: rest column jr (the columns outside the panel, in order) with the
-// K values A(prow[k0 + kk], col(jr)); four threads per column.
-__device__ inline void convert_b(const Pipe &P, const GjSmem &s, const float2 *__restrict__ A, int ld, int N,
-                                 int k0, int nbt) {
+// K values A(k0 + kk, col(jr)) of the panel's rows; four threads per column.
+__device__ inline void convert_b(const Pipe &P, const float2 *__restrict__ A, int ld, int N, int k0, int nbt) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane & 3;
     const int nrest = N - nbt, ntc = (nrest + PTN - 1) / PTN;
     for (int c0 = warp * 8; c0 < ntc * PTN; c0 += NWARP * 8) {
@@ -421,7 +422,7 @@ __device__ inline void convert_b(const Pipe &P, const GjSmem &s, const float2 *_
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
             const int kk = 8 * g + q;
-            v[q] = (cv && kk < nbt) ? A[s.prow[k0 + kk] + (size_t)ld * col] : make_float2(0.f, 0.f);
+            v[q] = (cv && kk < nbt) ? A[k0 + kk + (size_t)ld * col] : make_float2(0.f, 0.f);
             m = fmaxf(m, fmaxf(fabsf(v[q].x), fabsf(v[q].y)));
         }
         m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 1));
@@ -444,74 +445,58 @@ __device__ inline void convert_b(const Pipe &P, const GjSmem &s, const float2 *_
     }
 }
 
-// A(:, rest) = mask(A(:, rest)) + W * A_old(prow[k0:k0+nbt], rest), pipelined
-// (see above).  ld % 8 == 0.  Returns false if a wait timed out (uniform).
-__device__ inline bool trailing_pipe(Pipe &P, float2 *__restrict__ A, int N, int ld, int k0, int nbt,
-                                     const GjSmem &s) {
+// A(:, rest) += W * B for the panel [k0, k0+nbt) (W and B tiles already in
+// the CTA's global scratch), pipelined (see above); the C tiles of matrix cm
+// move by TMA.  Returns false if a wait timed out (uniform).
+__device__ inline bool trailing_pipe(Pipe &P, int N, int k0, int nbt, const CMat &cm) {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nrest = N - nbt, ntr = (N + TM - 1) / TM, ntc = (nrest + PTN - 1) / PTN, T = ntr * ntc;
-    convert_w(P, A, ld, N, k0, nbt);
-    convert_b(P, s, A, ld, N, k0, nbt);
-    asm volatile("fence.proxy.async.global;\n" ::: "memory");  // generic stores -> bulk-copy reads
+    // generic stores (W/B tiles in global, the staging in the C buffers) before
+    // the bulk copies and TMA tiles that read or overwrite them
+    asm volatile("fence.proxy.async;\n" ::: "memory");
     __syncthreads();
     const uint32_t bW = P.nW, bB = P.nB, bT = P.nT;
     int err = 0;
-    // matrix column of output column c of tile t (-1 outside the rest columns)
-    auto tile_col = [&](int t, int c) -> int {
-        const int jr = (t % ntc) * PTN + c;
-        return jr < nrest ? (jr < k0 ? jr : jr + nbt) : -1;
+    // first matrix column of tile t: the rest columns of a tile are contiguous
+    // (k0 and the tile width are multiples of 32)
+    auto tile_col0 = [&](int t) -> int {
+        const int jr = (t % ntc) * PTN;
+        return jr < k0 ? jr : jr + nbt;
     };
-    auto tile_rows = [&](int t) -> int { return min(TM, ld - (t / ntc) * TM); };
     if (warp == 0) {
         // ------------------------------------------------------ producer
-        auto load = [&](int u) -> bool {
-            if (u % ntc == 0) {
-                const uint32_t iw = bW + u / ntc;
-                bool ok = true;
-                if (lane == 0) {
-                    if (iw >= 1) ok = tc::mbar_wait(P.emptyW, (iw - 1) & 1u, WAIT_LIMIT);
-                    if (ok) {
-                        expect_bytes(P.fullW, WTILE);
-                        bulk_copy(P.sW, P.wt + (size_t)(u / ntc) * WTILE, WTILE, P.fullW);
-                    }
+        if (lane == 0) {
+            auto load = [&](int u) -> bool {
+                if (u % ntc == 0) {
+                    const uint32_t iw = bW + u / ntc;
+                    if (iw >= 1 && !tc::mbar_wait(P.emptyW, (iw - 1) & 1u, WAIT_LIMIT)) return false;
+                    expect_bytes(P.fullW, WTILE);
+                    bulk_copy(P.sW, P.wt + (size_t)(u / ntc) * WTILE, WTILE, P.fullW);
                 }
-                if (!__shfl_sync(0xffffffffu, (int)ok, 0)) return false;
+                const uint32_t ib = bB + u, ic = bT + u;
+                if (ib >= NBB && !tc::mbar_wait(&P.emptyB[ib % NBB], ((ib - NBB) / NBB) & 1u, WAIT_LIMIT))
+                    return false;
+                expect_bytes(&P.fullB[ib % NBB], BTILE);
+                bulk_copy(P.sB + (ib % NBB) * BTILE, P.bt + (size_t)(u % ntc) * BTILE, BTILE, &P.fullB[ib % NBB]);
+                // the C buffer last held tile u - NCB, whose store this thread issued
+                bulk_wait_read0();
+                expect_bytes(&P.fullC[ic % NCB], CTILE);  // the whole box, out-of-range elements zero-filled
+                tma_load4(P.sC + (ic % NCB) * CTILE, cm.tm, (u / ntc) * TM, tile_col0(u), cm.z, cm.w, &P.fullC[ic % NCB]);
+                return true;
+            };
+            for (int u = 0; u < NCB && u < T && !err; ++u)
+                if (!load(u)) err = 1;
+            for (int v = 0; v < T && !err; ++v) {
+                const uint32_t ic = bT + v;
+                if (!tc::mbar_wait(&P.doneC[ic % NCB], (ic / NCB) & 1u, WAIT_LIMIT)) { err = 1; break; }
+                tma_store4(cm.tm, (v / ntc) * TM, tile_col0(v), cm.z, cm.w, P.sC + (ic % NCB) * CTILE);  // clipped
+                bulk_commit();
+                if (v + NCB < T && !load(v + NCB)) err = 1;
             }
-            const uint32_t ib = bB + u, ic = bT + u;
-            bool ok = true;
-            if (lane == 0) {
-                if (ib >= NBB) ok = tc::mbar_wait(&P.emptyB[ib % NBB], ((ib - NBB) / NBB) & 1u, WAIT_LIMIT);
-                if (ok) {
-                    expect_bytes(&P.fullB[ib % NBB], BTILE);
-                    bulk_copy(P.sB[ib % NBB], P.bt + (size_t)(u % ntc) * BTILE, BTILE, &P.fullB[ib % NBB]);
-                }
-            }
-            if (!__shfl_sync(0xffffffffu, (int)ok, 0)) return false;
-            // the C buffer last held tile u - NCB, whose store this warp issued before
-            bulk_wait_read0();
-            const int rows = tile_rows(u), ncol = min(PTN, nrest - (u % ntc) * PTN);
-            if (lane == 0) expect_bytes(&P.fullC[ic % NCB], (uint32_t)(rows * 8 * ncol));
-            __syncwarp();
-            const int col = tile_col(u, lane);
-            if (col >= 0)
-                bulk_copy(P.sC[ic % NCB] + lane * (TM * 8), A + (size_t)(u / ntc) * TM + (size_t)ld * col, rows * 8,
-                          &P.fullC[ic % NCB]);
-            return true;
-        };
-        for (int u = 0; u < NCB && u < T && !err; ++u)
-            if (!load(u)) err = 1;
-        for (int v = 0; v < T && !err; ++v) {
-            const uint32_t ic = bT + v;
-            if (!tc::mbar_wait(&P.doneC[ic % NCB], (ic / NCB) & 1u, WAIT_LIMIT)) { err = 1; break; }
-            const int col = tile_col(v, lane);
-            if (col >= 0)
-                bulk_store(A + (size_t)(v / ntc) * TM + (size_t)ld * col, P.sC[ic % NCB] + lane * (TM * 8),
-                           tile_rows(v) * 8);
-            bulk_commit();
-            if (v + NCB < T && !load(v + NCB)) err = 1;
+            bulk_wait0();
+            asm volatile("fence.proxy.async.global;\n" ::: "memory");
         }
-        bulk_wait0();
-        asm volatile("fence.proxy.async.global;\n" ::: "memory");
+        __syncwarp();
     } else if (warp == 1) {
         // --------------------------------------------------- MMA issuer
         if (lane == 0) {
@@ -521,7 +506,7 @@ __device__ inline bool trailing_pipe(Pipe &P, float2 *__restrict__ A, int N, int
                 if (t % ntc == 0 && !tc::mbar_wait(P.fullW, (bW + t / ntc) & 1u, WAIT_LIMIT)) { err = 1; break; }
                 if (!tc::mbar_wait(&P.fullB[ib % NBB], (ib / NBB) & 1u, WAIT_LIMIT)) { err = 1; break; }
                 tc::fence_after_sync();
-                issue_split_mma(tc::smem_u32(P.sW), tc::smem_u32(P.sB[ib % NBB]), PTN, P.tbase + a * (2 * PTN), true);
+                issue_split_mma(tc::smem_u32(P.sW), tc::smem_u32(P.sB + (ib % NBB) * BTILE), PTN, P.tbase + a * (2 * PTN), true);
                 tc::mma_commit(&P.accFull[a]);
                 tc::mma_commit(&P.emptyB[ib % NBB]);
                 if (t % ntc == ntc - 1) tc::mma_commit(P.emptyW);
@@ -539,9 +524,9 @@ __device__ inline bool trailing_pipe(Pipe &P, float2 *__restrict__ A, int N, int
             if (__any_sync(0xffffffffu, err)) { err = 1; break; }
             tc::fence_after_sync();
             const int it = t / ntc, jt = t % ntc, i = it * TM + r;
-            const bool rv = i < N, keep = rv && !s.inP[i];
+            const bool rv = i < N;
             const int er = rv ? P.rexpW[i] : 0;
-            float2 *cs = (float2 *)P.sC[cb];
+            float2 *cs = (float2 *)(P.sC + cb * CTILE);
             const uint32_t dacc = P.tbase + lb + a * (2 * PTN);
 #pragma unroll
             for (int g = 0; g < PTN / 16; ++g) {
@@ -558,15 +543,14 @@ __device__ inline bool trailing_pipe(Pipe &P, float2 *__restrict__ A, int N, int
                         const int jr = jt * PTN + g * 16 + q;
                         if (jr < nrest) {
                             const float f = tc::exp2i(er + P.cexpB[jr]);
-                            const float2 o = keep ? old[q] : make_float2(0.f, 0.f);
-                            cs[(g * 16 + q) * TM + r] = make_float2(fmaf(re[q], f, o.x), fmaf(im[q], f, o.y));
+                            cs[(g * 16 + q) * TM + r] = make_float2(fmaf(re[q], f, old[q].x), fmaf(im[q], f, old[q].y));
                         }
                     }
                 }
             }
             // tensor memory read: the accumulator may take the next tile's MMAs
             tc::fence_before_sync();
-            tc::fence_async_smem();  // the bulk stores (async proxy) read these values
+            tc::fence_async_smem();  // the TMA store (async proxy) reads these values
             __syncwarp();
             if (lane == 0) {
                 mbar_arrive(&P.accEmpty[a]);
@@ -582,105 +566,36 @@ __device__ inline bool trailing_pipe(Pipe &P, float2 *__restrict__ A, int N, int
 }
 
 // In-place blocked Gauss-Jordan inverse of the N x N block A (leading
-// dimension ld, complex FP32) with implicit partial pivoting.  Panels of 32
-// columns, four 8-column register sub-panels each: per sub-panel p,
-// (i) bring it up to date with sub-panels < p, (ii) eliminate it,
-// (iii) apply its steps to the earlier columns; then one rank-32 trailing
-// update of all other columns on the tensor cores.  On return s.prow/s.iprow
-// hold the permutations: inv(A)(r, c) = A(prow[r], iprow[c]).  Returns the
-// LAPACK-style info (1-based column of the first zero pivot, 0 if none);
+// dimension ld, complex FP32; the same matrix as cm) in panels of 32
+// columns, pivoting only inside each panel's diagonal block: the Schur
+// complements of the sweep keep their diagonal blocks well conditioned, and
+// the FP64 refinement and the acceptance test of every job absorb the
+// difference to full partial pivoting.  Per panel K: P = inv(A_KK) by one
+// warp, the column block W (CUDA cores, FP32), one rank-32 update of all other
+// columns on the tensor cores.  On return A = inv(A) in natural order.
+// Returns (on warp 0) the 1-based column of the first zero pivot, 0 if none;
 // *err = 1 if a tensor-core wait timed out.
-template <int RPT>
-__device__ int gj_invert_mixed(float2 *__restrict__ A, int N, int ld, const GjSmem &s, Pipe &P, int *err) {
-    const int tid = threadIdx.x;
-    const float2 zero = make_float2(0.f, 0.f);
+__device__ int gj_invert(float2 *__restrict__ A, int N, int ld, const GjSmem &s, Pipe &P, const CMat &cm,
+                         int *err) {
     int info = 0;
-    unsigned used = 0;
-#pragma unroll
-    for (int r = 0; r < RPT; ++r)
-        if (tid + NT * r >= N) used |= 1u << r;
-    for (int i = tid; i < N; i += NT) s.inP[i] = 0;
-    __syncthreads();
     for (int k0 = 0; k0 < N; k0 += KB) {
         const int nbt = min(KB, N - k0);
-        for (int p = 0; p * 8 < nbt; ++p) {
-            const int cp = k0 + p * 8, kprev = p * 8;
-            const int nbp = min(8, nbt - kprev);
-            if (p > 0) {
-                for (int e = tid; e < kprev * 8; e += NT) {
-                    const int kk = e / 8, c = e % 8;
-                    s.sX[e] = (c < nbp) ? A[s.prow[k0 + kk] + (size_t)ld * (cp + c)] : zero;
-                }
-                __syncthreads();
+        if (threadIdx.x < 32) {
+            const int r = invert_diag_warp(A, ld, k0, nbt, s);
+            if (r && !info) info = k0 + r;
+        }
+        __syncthreads();
+        panel_w(P, s, A, ld, N, k0, nbt);
+        if (nbt < N) {
+            convert_b(P, A, ld, N, k0, nbt);
+            if (!trailing_pipe(P, N, k0, nbt, cm)) {
+                *err = 1;
+                return info;
             }
-            float2 w[RPT][8];
-#pragma unroll
-            for (int r = 0; r < RPT; ++r) {
-                const int i = tid + NT * r;
-                const bool keep = (i < N) && !(s.inP[i] >= 1 && s.inP[i] <= p);
-#pragma unroll
-                for (int c = 0; c < 8; ++c) w[r][c] = (keep && c < nbp) ? A[i + (size_t)ld * (cp + c)] : zero;
-                if (i < N) {
-#pragma unroll 1
-                    for (int kk0 = 0; kk0 < kprev; kk0 += 8) {
-                        float2 wa[8];
-#pragma unroll
-                        for (int u = 0; u < 8; ++u) wa[u] = A[i + (size_t)ld * (k0 + kk0 + u)];
-#pragma unroll
-                        for (int u = 0; u < 8; ++u)
-#pragma unroll
-                            for (int c = 0; c < 8; ++c) w[r][c] = cfma(wa[u], s.sX[(kk0 + u) * 8 + c], w[r][c]);
-                    }
-                }
-            }
-            factor_sub8<RPT>(w, cp, nbp, used, info, p + 1, s);
-            if (p > 0) {
-                for (int e = tid; e < 8 * kprev; e += NT) {
-                    const int c = e / kprev, q = e % kprev;
-                    s.sY[c * 32 + q] = (c < nbp) ? A[s.prow[cp + c] + (size_t)ld * (k0 + q)] : zero;
-                }
-                __syncthreads();
-#pragma unroll
-                for (int r = 0; r < RPT; ++r) {
-                    const int i = tid + NT * r;
-                    if (i < N) {
-                        const bool keep = s.inP[i] != p + 1;
-#pragma unroll 1
-                        for (int q0 = 0; q0 < kprev; q0 += 8) {
-                            float2 v[8];
-#pragma unroll
-                            for (int u = 0; u < 8; ++u) v[u] = keep ? A[i + (size_t)ld * (k0 + q0 + u)] : zero;
-#pragma unroll
-                            for (int u = 0; u < 8; ++u) {
-#pragma unroll
-                                for (int c = 0; c < 8; ++c) v[u] = cfma(w[r][c], s.sY[c * 32 + q0 + u], v[u]);
-                                A[i + (size_t)ld * (k0 + q0 + u)] = v[u];
-                            }
-                        }
-                    }
-                }
-            }
-#pragma unroll
-            for (int r = 0; r < RPT; ++r) {
-                const int i = tid + NT * r;
-                if (i < N) {
-#pragma unroll
-                    for (int c = 0; c < 8; ++c)
-                        if (c < nbp) A[i + (size_t)ld * (cp + c)] = w[r][c];
-                }
-            }
+        } else {
             __syncthreads();
         }
-        if (nbt < N && !trailing_pipe(P, A, N, ld, k0, nbt, s)) {
-            *err = 1;
-            return info;
-        }
-        __syncthreads();
-        if (tid < nbt) s.inP[s.prow[k0 + tid]] = 0;
-        __syncthreads();
     }
-    for (int k = tid; k < N; k += NT) s.iprow[s.prow[k]] = k;
-    __syncthreads();
     return info;
 }
 
@@ -750,24 +665,23 @@ __global__ void __launch_bounds__(NT, 1)
 }
 
 // Inverse of each of nmat N x N complex FP32 matrices (one CTA each):
-// work holds the matrices (overwritten), out receives the inverses.
-template <int RPT>
+// work holds the matrices (leading dimension ld, matrix b at b * ld * N; tm
+// maps them as (row, column, 0, b)), out receives the inverses.
 __global__ void __launch_bounds__(NT, 1)
     k_tc_inverse_check(float2 *__restrict__ work, int N, int ld, float2 *__restrict__ out, int *__restrict__ info,
-                       int *status, unsigned char *pscratch) {
+                       int *status, unsigned char *pscratch, const __grid_constant__ CUtensorMap tm) {
     extern __shared__ __align__(128) unsigned char smem[];
     GjSmem s = carve_gj(smem, N);
     Pipe P = carve_pipe(smem + gj_smem_bytes(N), N, pscratch + (size_t)blockIdx.x * pipe_scratch_bytes(N));
     pipe_setup(P);
     int err = 0;
     float2 *A = work + (size_t)blockIdx.x * ld * N;
-    const int inf = gj_invert_mixed<RPT>(A, N, ld, s, P, &err);
+    const CMat cm{&tm, 0, (int)blockIdx.x};
+    const int inf = gj_invert(A, N, ld, s, P, cm, &err);
     if (!err) {
         float2 *o = out + (size_t)blockIdx.x * N * N;
-        for (int j = 0; j < N; ++j) {
-            const int jc = s.iprow[j];
-            for (int r = threadIdx.x; r < N; r += NT) o[s.iprow[r] + (size_t)N * j] = A[r + (size_t)ld * jc];
-        }
+        for (int j = 0; j < N; ++j)
+            for (int r = threadIdx.x; r < N; r += NT) o[r + (size_t)N * j] = A[r + (size_t)ld * j];
     }
     if (threadIdx.x == 0) {
         info[blockIdx.x] = inf;
@@ -823,6 +737,7 @@ MixedLayout make_layout(int N, int Nz, int ld, int ncap) {
 struct MixedArgs {
     negf::Geo g;
     MixedLayout L;
+    const double2 *voff;   // [Nz][N][ld] -c2 V(G_i - G_j) (the context's table)
     const double *E;       // energies
     const int2 *jobs;      // per wave slot: (energy index, k-point)
     int njobs;
@@ -882,17 +797,20 @@ __device__ inline negf::Smem carve_job(unsigned char *base, int N) {
     return s;
 }
 
-// M = round32(D_k - inv(prev)) with D_k generated in FP64 from the V table
-// (negf::d_element, grid.f90:236-333) and inv(prev)(i, j) = R(prow[t] ...)
-// read through the previous inverse's permutations: thread t reads row t of
-// R (coalesced) and writes row iprow[t] of M.
+// M = round32(D_k - inv(prev)) in FP64: the off-diagonal part of D_k
+// (-c2 V(G_i - G_j), the same for every energy and k-point) streams from the
+// precomputed table, the diagonal is generated (negf::d_element,
+// grid.f90:236-333).  Thread t owns row t: coalesced loads of the table and of
+// the previous inverse R, coalesced stores; four columns per pass keep eight
+// loads in flight per thread.
 __device__ inline void form_mixed(float2 *__restrict__ M, const negf::Geo &g, const negf::Smem &js,
-                                  const GjSmem &s, int k, double2 E, int ik, const float2 *__restrict__ R) {
+                                  const double2 *__restrict__ voff, int k, double2 E, int ik,
+                                  const float2 *__restrict__ R) {
     const int N = g.N, ld = g.ld;
     const double2 *vs = g.vhat + (size_t)g.W * g.H * k;
+    const double2 *vk = voff + (size_t)N * ld * k;
     for (int j0 = 0; j0 < N; j0 += 4) {
         for (int t = threadIdx.x; t < N; t += NT) {
-            const int i = R ? s.iprow[t] : t;
             double2 d[4];
             float2 r[4];
 #pragma unroll
@@ -901,14 +819,36 @@ __device__ inline void form_mixed(float2 *__restrict__ M, const negf::Geo &g, co
                 d[q] = make_double2(0.0, 0.0);
                 r[q] = make_float2(0.f, 0.f);
                 if (j < N) {
-                    d[q] = negf::d_element(g, js, vs, k, E, ik, i, j, js.nx[j], js.ny[j]);
-                    if (R) r[q] = R[t + (size_t)ld * s.iprow[j]];
+                    d[q] = vk[t + (size_t)ld * j];
+                    if (R) r[q] = R[t + (size_t)ld * j];
                 }
             }
 #pragma unroll
-            for (int q = 0; q < 4; ++q)
-                if (j0 + q < N) M[i + (size_t)ld * (j0 + q)] = make_float2((float)(d[q].x - (double)r[q].x),
-                                                                           (float)(d[q].y - (double)r[q].y));
+            for (int q = 0; q < 4; ++q) {
+                const int j = j0 + q;
+                if (j == t) d[q] = negf::d_element(g, js, vs, k, E, ik, t, t, js.nx[t], js.ny[t]);
+                if (j < N) M[t + (size_t)ld * j] = make_float2((float)(d[q].x - (double)r[q].x),
+                                                               (float)(d[q].y - (double)r[q].y));
+            }
+        }
+    }
+}
+
+// -c2 V(G_i - G_j) for every slice: out[k][j][i] (leading dimension ld), the
+// off-diagonal elements of negf::d_element.  Grid (Nz), one slice per CTA.
+__global__ void __launch_bounds__(NT) k_voff(negf::Geo g, double2 *__restrict__ out) {
+    const int N = g.N, ld = g.ld, k = blockIdx.x;
+    const double2 *vs = g.vhat + (size_t)g.W * g.H * k;
+    double2 *o = out + (size_t)N * ld * k;
+    for (int j = 0; j < N; ++j) {
+        const int nxj = g.nx[j], nyj = g.ny[j];
+        for (int i = threadIdx.x; i < ld; i += NT) {
+            double2 v = make_double2(0.0, 0.0);
+            if (i < N) {
+                const double2 t = vs[(g.nx[i] - nxj + g.ngx) + g.W * (g.ny[i] - nyj + g.ngy)];
+                v = make_double2(-t.x * g.c2, -t.y * g.c2);
+            }
+            o[i + (size_t)ld * j] = v;
         }
     }
 }
@@ -971,8 +911,8 @@ __device__ inline void store_factor(const float2 *__restrict__ R, const MixedLay
 // gR(b) = inv(D_b - gR(b+1)), b = Nz-1 .. 1, then G_11 = inv(D_0 - gR(1))
 // (math_kernel.f90:81-118), every inverse stored as a split-tile factor, and
 // x0(:, j) = G_11(:, oc[j]) for the open channels oc of the right lead.
-template <int RPT>
-__global__ void __launch_bounds__(NT, 1) k_mixed_sweep(MixedArgs a) {
+// tmC maps the CTA's two working matrices as (row, column, 0|1, CTA).
+__global__ void __launch_bounds__(NT, 1) k_mixed_sweep(MixedArgs a, const __grid_constant__ CUtensorMap tmC) {
     extern __shared__ __align__(128) unsigned char smem[];
     const MixedLayout &L = a.L;
     const negf::Geo &g = a.g;
@@ -984,10 +924,11 @@ __global__ void __launch_bounds__(NT, 1) k_mixed_sweep(MixedArgs a) {
     float2 *W0 = (float2 *)(a.scratch + (size_t)blockIdx.x * L.scratch_bytes);
     float2 *W1 = W0 + (size_t)N * ld;
     Pipe P = carve_pipe(pipe_smem, N, (unsigned char *)(W1 + (size_t)N * ld));
-    negf::Smem js = carve_job_slim(smem + off, N, P.sC[0]);
+    negf::Smem js = carve_job_slim(smem + off, N, P.sC);
     off += job_smem_bytes_slim(N);
     int *rexpN = (int *)(smem + off);
     for (int i = tid; i < N; i += NT) { js.nx[i] = g.nx[i]; js.ny[i] = g.ny[i]; }
+    gj_identity(s, N);
     pipe_setup(P);
     for (int w = blockIdx.x; w < a.njobs; w += gridDim.x) {
         const int2 jb = a.jobs[w];
@@ -1008,12 +949,14 @@ __global__ void __launch_bounds__(NT, 1) k_mixed_sweep(MixedArgs a) {
         for (int j = tid; j < nopen; j += NT) oc[j] = js.rows[j];
         if (tid == 0) oc[L.ncap] = nopen;
         float2 *cur = W0, *oth = W1;
-        int info = 0, err = 0;
+        int zc = 0, info = 0, err = 0;
         for (int b = Nz - 1; b >= 0; --b) {
-            form_mixed(oth, g, js, s, b, E, jb.y, b < Nz - 1 ? cur : nullptr);
+            form_mixed(oth, g, js, a.voff, b, E, jb.y, b < Nz - 1 ? cur : nullptr);
             __syncthreads();
             float2 *tt = cur; cur = oth; oth = tt;
-            const int r = gj_invert_mixed<RPT>(cur, N, ld, s, P, &err);
+            zc ^= 1;
+            const CMat cm{&tmC, zc, (int)blockIdx.x};
+            const int r = gj_invert(cur, N, ld, s, P, cm, &err);
             if (r && !info) info = r;
             if (err) break;  // uniform: set from __syncthreads_or
             store_factor(cur, L, s, rexpN, jm, b);
@@ -1469,6 +1412,40 @@ __global__ void __launch_bounds__(NT, 2) k_mixed_residual(MixedArgs a) {
     }
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+// The C-tile map of the trailing update: nmat matrices per CTA (stride
+// mat_stride bytes) for ncta CTAs (stride cta_stride), each N x N complex FP32
+// with leading dimension ld; boxes of TM rows x PTN columns.
+bool c_tile_map(CUtensorMap *m, void *base, int N, int ld, int nmat, size_t mat_stride, int ncta, size_t cta_stride) {
+    EncodeTiledFn f = encode_tiled();
+    if (!f || ld % 2 || mat_stride % 16 || cta_stride % 16 || ((uintptr_t)base & 15)) return false;
+    const cuuint64_t dims[4] = {(cuuint64_t)N, (cuuint64_t)N, (cuuint64_t)nmat, (cuuint64_t)ncta};
+    const cuuint64_t strides[3] = {(cuuint64_t)ld * 8, (cuuint64_t)mat_stride, (cuuint64_t)cta_stride};
+    const cuuint32_t box[4] = {(cuuint32_t)TM, (cuuint32_t)PTN, 1, 1};
+    const cuuint32_t es[4] = {1, 1, 1, 1};
+    return f(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 #define CKM(x)                                                                             \
     do {                                                                                   \
         cudaError_t e_ = (x);                                                              \
@@ -1510,23 +1487,22 @@ extern "C" int negf_tc_inverse_check(const float *d_A, int32_t N, int32_t nmat, 
     float2 *work = nullptr;
     int *d_status = nullptr;
     unsigned char *pscr = nullptr;
-    const int ld = rup(N, 8);  // whole-column bulk copies of the trailing update need ld % 8 == 0
+    const int ld = rup(N, 8);  // the TMA strides of the trailing update need ld % 8 == 0
     CKM(cudaMalloc(&pscr, pipe_scratch_bytes(N) * nmat));
     CKM(cudaMalloc(&work, sizeof(float2) * (size_t)ld * N * nmat));
     CKM(cudaMalloc(&d_status, sizeof(int)));
     CKM(cudaMemcpy2DAsync(work, sizeof(float2) * ld, d_A, sizeof(float2) * N, sizeof(float2) * N, (size_t)N * nmat,
                           cudaMemcpyDeviceToDevice, st));
     CKM(cudaMemsetAsync(d_status, 0, sizeof(int), st));
-    if (N <= NT) {
-        CKM(cudaFuncSetAttribute(k_tc_inverse_check<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_tc_inverse_check<1><<<nmat, NT, smem, st>>>(work, N, ld, (float2 *)d_out, d_info, d_status, pscr);
-    } else if (N <= 2 * NT) {
-        CKM(cudaFuncSetAttribute(k_tc_inverse_check<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_tc_inverse_check<2><<<nmat, NT, smem, st>>>(work, N, ld, (float2 *)d_out, d_info, d_status, pscr);
-    } else {
-        CKM(cudaFuncSetAttribute(k_tc_inverse_check<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_tc_inverse_check<4><<<nmat, NT, smem, st>>>(work, N, ld, (float2 *)d_out, d_info, d_status, pscr);
+    CUtensorMap tm;
+    if (!c_tile_map(&tm, work, N, ld, 1, (size_t)ld * N * 8, nmat, (size_t)ld * N * 8)) {
+        cudaFree(work);
+        cudaFree(d_status);
+        cudaFree(pscr);
+        return NEGF_ERR_CUDA;
     }
+    CKM(cudaFuncSetAttribute(k_tc_inverse_check, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_tc_inverse_check<<<nmat, NT, smem, st>>>(work, N, ld, (float2 *)d_out, d_info, d_status, pscr, tm);
     CKM(cudaGetLastError());
     int h = 0;
     CKM(cudaMemcpyAsync(&h, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1621,6 +1597,16 @@ int negf_internal_mixed(negf_ctx *c, const double *h_E, const double *d_E, int n
         const MixedLayout L = make_layout(N, Nz, c->ld, ncap);
         const size_t per_job = L.job_bytes + L.scratch_bytes;
         const size_t small_per_job = sizeof(int2) + 4 * sizeof(double) + sizeof(int);
+        if (!c->d_voff) {
+            // the energy-independent part of every D_k, once per context
+            if (cudaMalloc(&c->d_voff, sizeof(double2) * (size_t)N * c->ld * Nz) != cudaSuccess) {
+                cudaGetLastError();
+                c->d_voff = nullptr;
+                return NEGF_ERR_NOMEM;
+            }
+            k_voff<<<Nz, NT, 0, st>>>(mixed_geo(c), c->d_voff);
+            CKM(cudaGetLastError());
+        }
         size_t free_b = 0, total_b = 0;
         cudaMemGetInfo(&free_b, &total_b);
         // the FP64 re-runs keep their own workspace (4 blocks per CTA)
@@ -1646,6 +1632,7 @@ int negf_internal_mixed(negf_ctx *c, const double *h_E, const double *d_E, int n
             unsigned char *base = (unsigned char *)c->d_mixed;
             MixedArgs a;
             a.g = mixed_geo(c);
+            a.voff = c->d_voff;
             a.L = L;
             a.E = d_E;
             a.jobmem = base;
@@ -1663,12 +1650,13 @@ int negf_internal_mixed(negf_ctx *c, const double *h_E, const double *d_E, int n
                                     job_smem_bytes_slim(N) + (size_t)rup(N, 4) * 4;
             const size_t sm_pass = pass_smem_bytes(N, ncap);
             const size_t sm_res = (size_t)negf::KC * (negf::AP + negf::BP) * 16 + job_smem_bytes(N);
-            if (N <= NT) rc = set_smem(k_mixed_sweep<1>, sm_sweep);
-            else if (N <= 2 * NT) rc = set_smem(k_mixed_sweep<2>, sm_sweep);
-            else rc = set_smem(k_mixed_sweep<4>, sm_sweep);
+            rc = set_smem(k_mixed_sweep, sm_sweep);
             if (!rc) rc = set_smem(k_mixed_pass, sm_pass);
             if (!rc) rc = set_smem(k_mixed_residual, sm_res);
             if (rc) return rc;
+            CUtensorMap tmC;
+            if (!c_tile_map(&tmC, a.scratch, N, c->ld, 2, (size_t)N * c->ld * 8, W, L.scratch_bytes))
+                return NEGF_ERR_CUDA;
             std::vector<int2> wj(W);
             std::vector<double> tau(W), dn(W), xn(W);
             std::vector<int> status(W);
@@ -1678,9 +1666,7 @@ int negf_internal_mixed(negf_ctx *c, const double *h_E, const double *d_E, int n
                 a.njobs = nw;
                 CKM(cudaMemcpyAsync(d_jobs, wj.data(), sizeof(int2) * nw, cudaMemcpyHostToDevice, st));
                 CKM(cudaEventRecord(c->ev0, st));
-                if (N <= NT) k_mixed_sweep<1><<<nw, NT, sm_sweep, st>>>(a);
-                else if (N <= 2 * NT) k_mixed_sweep<2><<<nw, NT, sm_sweep, st>>>(a);
-                else k_mixed_sweep<4><<<nw, NT, sm_sweep, st>>>(a);
+                k_mixed_sweep<<<nw, NT, sm_sweep, st>>>(a, tmC);
                 CKM(cudaGetLastError());
                 k_mixed_pass<<<nw, NT, sm_pass, st>>>(a, PASS_X0, 0, 0);
                 CKM(cudaGetLastError());
