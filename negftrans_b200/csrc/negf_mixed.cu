@@ -985,37 +985,40 @@ __global__ void __launch_bounds__(NT, 1) k_mixed_sweep(MixedArgs a, const __grid
 // each 128-row tile of R the K chunks stream through a 3-stage pipeline of
 // bulk copies (A: one 32 KB tile, B: one chunk) into tcgen05 MMAs.
 enum PassMode { PASS_X0 = 0, PASS_BACK = 1, PASS_CORR = 2 };
-constexpr int PSTAGES = 3;
+constexpr int PA = 3;  // A ring stages (one 32 KB factor tile each)
+constexpr int PB = 3;  // B ring stages (one K chunk of the vector block each)
 
 struct PassSmem {
-    unsigned char *stA[PSTAGES];
-    unsigned char *stB[PSTAGES];
-    int *prow, *iprow, *rexp, *cexp;
-    uint64_t *full, *empty, *accf;
+    unsigned char *stA;   // PA x TILE_BYTES
+    unsigned char *stB;   // PB x (ncap * 256)
+    int *cexp;            // [ncap] column exponents of the current product's v
+    unsigned *cmax;       // [ncap] column maxima (float bits) of the next product's v
+    uint64_t *fullA, *emptyA, *fullB, *emptyB, *accFull, *accEmpty, *bReady;
     uint32_t *tslot;
-    double *red;
+    double *red;          // [2 * NWARP]
 };
+constexpr int PASS_BARS = 2 * PA + 2 * PB + 2 + 2 + 1;
 __host__ __device__ inline size_t pass_smem_bytes(int N, int ncap) {
-    size_t b = PSTAGES * (TILE_BYTES + (size_t)ncap * 256);
-    b += 3 * (size_t)rup(N, 4) * 4 + (size_t)ncap * 4;
-    b += (2 * PSTAGES + 1) * 8 + 16 + NWARP * 8 * 2;
-    b += job_smem_bytes(N);
+    size_t b = PA * TILE_BYTES + PB * (size_t)ncap * 256;
+    b += 2 * (size_t)ncap * 4 + PASS_BARS * 8 + 16 + 2 * NWARP * 8;
+    (void)N;
     return (b + 127) / 128 * 128;
 }
-__device__ inline PassSmem carve_pass(unsigned char *base, int N, int ncap) {
+__device__ inline PassSmem carve_pass(unsigned char *base, int ncap) {
     PassSmem p;
     unsigned char *q = base;
-    for (int s = 0; s < PSTAGES; ++s) { p.stA[s] = q; q += TILE_BYTES; }
-    for (int s = 0; s < PSTAGES; ++s) { p.stB[s] = q; q += (size_t)ncap * 256; }
-    p.prow = (int *)q; q += (size_t)rup(N, 4) * 4;
-    p.iprow = (int *)q; q += (size_t)rup(N, 4) * 4;
-    p.rexp = (int *)q; q += (size_t)rup(N, 4) * 4;
+    p.stA = q; q += PA * TILE_BYTES;
+    p.stB = q; q += PB * (size_t)ncap * 256;
     p.cexp = (int *)q; q += (size_t)ncap * 4;
+    p.cmax = (unsigned *)q; q += (size_t)ncap * 4;
     q = (unsigned char *)(((uintptr_t)q + 15) & ~(uintptr_t)15);
-    p.full = (uint64_t *)q; q += PSTAGES * 8;
-    p.empty = (uint64_t *)q; q += PSTAGES * 8;
-    p.accf = (uint64_t *)q; q += 8;
-    p.tslot = (uint32_t *)q; q += 8;
+    uint64_t *bar = (uint64_t *)q;
+    p.fullA = bar; p.emptyA = bar + PA;
+    p.fullB = bar + 2 * PA; p.emptyB = p.fullB + PB;
+    p.accFull = p.emptyB + PB; p.accEmpty = p.accFull + 2;
+    p.bReady = p.accEmpty + 2;
+    q += PASS_BARS * 8;
+    p.tslot = (uint32_t *)q; q += 16;
     p.red = (double *)q;
     return p;
 }
@@ -1030,8 +1033,20 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
                  "l"(src), "r"(bytes), "r"(tc::smem_u32(bar))
                  : "memory");
 }
+// barrier 1 of the four epilogue warps; and its OR-reduction (a uniform
+// decision for all four)
+__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, 128;\n" ::: "memory"); }
+__device__ __forceinline__ int epi_any(int v) {
+    int r;
+    asm volatile(
+        "{\n .reg .pred q;\n setp.ne.s32 q, %1, 0;\n bar.red.or.pred q, 1, 128, q;\n selp.s32 %0, 1, 0, q;\n}\n"
+        : "=r"(r)
+        : "r"(v)
+        : "memory");
+    return r;
+}
 
-// MMAs of one staged K chunk with N = npad output columns (thread 0).
+// MMAs of one staged K chunk with N = npad output columns (one thread).
 __device__ inline void issue_pass_chunk(const unsigned char *sA, const unsigned char *sB, int npad,
                                         uint32_t tbase, bool first) {
     constexpr uint32_t SBO = (KB / 8) * 128, LBO = 128;
@@ -1058,151 +1073,265 @@ __device__ inline void issue_pass_chunk(const unsigned char *sA, const unsigned 
     }
 }
 
-// One product of a pass (see above).  Returns false on a tensor wait timeout
-// (uniform over the CTA).  phases: bit s = full[s], bit 8+s = empty[s], bit
-// 16 = accf (thread 0 tracks full/empty, every thread accf).
-__device__ bool pass_product(const MixedLayout &L, const PassSmem &p, unsigned char *jm, unsigned char *bscr,
-                             int slot, const float2 *__restrict__ v1, const float2 *__restrict__ v2,
-                             float2 *__restrict__ out, float alpha, const float2 *__restrict__ wadd, int nopen,
-                             int npad, uint32_t tbase, uint32_t &phases, float2 *__restrict__ xacc = nullptr) {
-    const int N = L.N, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int *prow_g = (const int *)(jm + L.off_prow) + (size_t)slot * N;
-    const int *rexp_g = (const int *)(jm + L.off_rexp) + (size_t)slot * N;
-    const unsigned char *tiles = jm + L.off_tiles + (size_t)slot * L.mat_bytes;
-    for (int k = tid; k < N; k += NT) {
-        const int pr = prow_g[k];
-        p.prow[k] = pr;
-        p.iprow[pr] = k;
-        p.rexp[k] = rexp_g[k];
+// Product s of a pass: y = alpha gR(slot) (v1 - v2) + wadd, written to out
+// (and xacc += y); the next product's v is vn1 - y (vn1 null: y itself).
+struct Prod {
+    int slot;
+    const float2 *v1, *v2;
+    float2 *out;
+    float alpha;
+    const float2 *wadd;
+    float2 *xacc;
+    const float2 *vn1;
+};
+__device__ inline int pass_nprod(int mode, int Nz) { return mode == PASS_CORR ? Nz : Nz - 1; }
+// x = x0 slices, rc = residual / correction stage, d = two correction slices,
+// xa = the solution that d accumulates into (CORR, null on the last iteration)
+__device__ inline Prod pass_prod(int mode, int s, int Nz, size_t sl, float2 *x, float2 *rc, float2 *d, float2 *xa) {
+    Prod q;
+    q.wadd = nullptr;
+    q.xacc = nullptr;
+    q.vn1 = nullptr;
+    q.v2 = nullptr;
+    if (mode == PASS_X0) {          // x0(b) = -gR(b) x0(b-1), b = s + 1
+        const int b = s + 1;
+        q.slot = b; q.v1 = x + (b - 1) * sl; q.out = x + b * sl; q.alpha = -1.f;
+    } else if (mode == PASS_BACK) { // c(b) = r(b) - gR(b+1) c(b+1), b = Nz-2-s, in place of r
+        const int b = Nz - 2 - s;
+        q.slot = b + 1; q.v1 = rc + (b + 1) * sl; q.out = rc + b * sl; q.alpha = -1.f; q.wadd = rc + b * sl;
+    } else {                        // d(b) = gR(b) (c(b) - d(b-1)), b = s
+        const int b = s;
+        q.slot = b; q.v1 = rc + b * sl; q.v2 = b ? d + ((b - 1) & 1) * sl : nullptr;
+        q.out = d + (b & 1) * sl; q.alpha = 1.f;
+        q.xacc = (b < Nz - 1 && xa) ? xa + b * sl : nullptr;
+        q.vn1 = b + 1 < Nz ? rc + (b + 1) * sl : nullptr;  // the next product reads c(b+1) - d(b)
     }
-    __syncthreads();
-    // column exponents of v_p (= of v: a row permutation)
-    for (int j = warp; j < npad; j += NWARP) {
-        float m = 0.0f;
-        if (j < nopen)
-            for (int k = lane; k < N; k += 32) {
-                float2 x = v1[k + (size_t)N * j];
-                if (v2) { const float2 y = v2[k + (size_t)N * j]; x.x -= y.x; x.y -= y.y; }
-                m = fmaxf(m, fmaxf(fabsf(x.x), fabsf(x.y)));
-            }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-        if (lane == 0) p.cexp[j] = tc::scale_exponent(m);
+    return q;
+}
+
+// The epilogue warps' conversion of v = v1 - v2 into the split-fp16 B chunks
+// (chunk kc at kc * npad * 256 B of bscr, planes of npad * KB fp16), one
+// exponent per column.  First, if cmax is null, the column maxima by a pass
+// over v; else the maxima the previous epilogue accumulated in cmax.
+__device__ inline void pass_convert(const MixedLayout &L, const PassSmem &p, const float2 *__restrict__ v1,
+                                    const float2 *__restrict__ v2, int nopen, int npad, unsigned char *bscr,
+                                    bool from_cmax) {
+    const int N = L.N, et = threadIdx.x - 128, ew = et >> 5, lane = et & 31;
+    if (!from_cmax) {
+        for (int j = ew; j < npad; j += 4) {
+            float m = 0.0f;
+            if (j < nopen)
+                for (int k = lane; k < N; k += 32) {
+                    float2 x = v1[k + (size_t)N * j];
+                    if (v2) { const float2 y = v2[k + (size_t)N * j]; x.x -= y.x; x.y -= y.y; }
+                    m = fmaxf(m, fmaxf(fabsf(x.x), fabsf(x.y)));
+                }
+            m = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(m)));
+            if (lane == 0) p.cexp[j] = tc::scale_exponent(m);
+        }
+    } else {
+        for (int j = et; j < npad; j += 128) p.cexp[j] = tc::scale_exponent(__uint_as_float(p.cmax[j]));
     }
-    __syncthreads();
-    // B operand split tiles: chunk kc at kc * npad * 256 B, planes of npad * KB fp16
+    epi_bar();
+    for (int j = et; j < npad; j += 128) p.cmax[j] = 0u;
     const uint32_t bplane = npad * KB * 2;
-    for (int item = tid; item < L.nkc * npad * 4; item += NT) {
-        const int g4 = item & 3, j = (item >> 2) % npad, kc = (item >> 2) / npad;
-        const float sc = tc::exp2i(-p.cexp[j]);
-        float2 v[8];
+    const int nitem = L.nkc * npad * 4;
+    // two items per thread per round: all 32 loads in flight before the first use
+    for (int i0 = et; i0 < nitem; i0 += 256) {
+        float2 x1[2][8], x2[2][8];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const int k = kc * KB + 8 * g4 + q;
-            float2 x = make_float2(0.f, 0.f);
-            if (k < N && j < nopen) {
-                const int pr = p.prow[k];
-                x = v1[pr + (size_t)N * j];
-                if (v2) { const float2 y = v2[pr + (size_t)N * j]; x.x -= y.x; x.y -= y.y; }
+        for (int h = 0; h < 2; ++h) {
+            const int item = i0 + 128 * h;
+            const int g4 = item & 3, j = (item >> 2) % npad, kc = (item >> 2) / npad;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int k = kc * KB + 8 * g4 + q;
+                const bool ok = item < nitem && k < N && j < nopen;
+                x1[h][q] = ok ? v1[k + (size_t)N * j] : make_float2(0.f, 0.f);
+                x2[h][q] = (ok && v2) ? v2[k + (size_t)N * j] : make_float2(0.f, 0.f);
             }
-            v[q] = make_float2(x.x * sc, x.y * sc);
         }
-        __align__(16) __half rh[8], rl[8], ih[8], il[8];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const tc::Split2 a = tc::split_fp16(v[q].x), b = tc::split_fp16(v[q].y);
-            rh[q] = a.hi; rl[q] = a.lo; ih[q] = b.hi; il[q] = b.lo;
+        for (int h = 0; h < 2; ++h) {
+            const int item = i0 + 128 * h;
+            if (item >= nitem) break;
+            const int g4 = item & 3, j = (item >> 2) % npad, kc = (item >> 2) / npad;
+            const float sc = tc::exp2i(-p.cexp[j]);
+            __align__(16) __half rh[8], rl[8], ih[8], il[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const tc::Split2 a = tc::split_fp16((x1[h][q].x - x2[h][q].x) * sc),
+                                 b = tc::split_fp16((x1[h][q].y - x2[h][q].y) * sc);
+                rh[q] = a.hi; rl[q] = a.lo; ih[q] = b.hi; il[q] = b.lo;
+            }
+            unsigned char *dst = bscr + (size_t)kc * npad * 256 + tc::kmajor_offset(j, 8 * g4, KB);
+            *(uint4 *)(dst + 0 * bplane) = *(const uint4 *)rh;
+            *(uint4 *)(dst + 1 * bplane) = *(const uint4 *)rl;
+            *(uint4 *)(dst + 2 * bplane) = *(const uint4 *)ih;
+            *(uint4 *)(dst + 3 * bplane) = *(const uint4 *)il;
         }
-        unsigned char *dst = bscr + (size_t)kc * npad * 256 + tc::kmajor_offset(j, 8 * g4, KB);
-        *(uint4 *)(dst + 0 * bplane) = *(const uint4 *)rh;
-        *(uint4 *)(dst + 1 * bplane) = *(const uint4 *)rl;
-        *(uint4 *)(dst + 2 * bplane) = *(const uint4 *)ih;
-        *(uint4 *)(dst + 3 * bplane) = *(const uint4 *)il;
     }
     // the bulk copies (async proxy) read what these generic stores wrote
     asm volatile("fence.proxy.async.global;\n" ::: "memory");
-    __syncthreads();
-    const uint32_t bbytes = (uint32_t)npad * 256;
+    epi_bar();
+}
+
+// Pipeline counters of the roles, carried across the jobs of a CTA.
+struct PassCnt {
+    uint32_t a, b, u, r;  // A stages, B stages, accumulators, products
+};
+
+// All products of one pass of one job through the warp-specialised pipeline:
+//   warp 0, lane 0   streams the factor tiles of every product (row tile by
+//                    row tile, K chunk by K chunk) through the A ring; they do
+//                    not depend on the data, so it runs as far ahead as the
+//                    ring allows, across products;
+//   warp 2, lane 0   streams the B chunks of product s (the split vector
+//                    block in the CTA's global scratch) through the B ring,
+//                    once per row tile, as soon as the epilogue warps have
+//                    converted v_s;
+//   warp 1, lane 0   the MMAs of each row tile into one of two tensor-memory
+//                    accumulators (2 ncap columns each);
+//   warps 4-7        the epilogue of each row tile: y from the accumulator
+//                    (tcgen05.ld, one lane quadrant per warp) times
+//                    2^(row + column exponent), the stores, the column maxima
+//                    of the next product's v (one redux per column); after the
+//                    last row tile, the conversion of v_{s+1}.
+// Returns false if a wait timed out (uniform over the CTA).
+__device__ bool pass_run(const MixedLayout &L, const PassSmem &p, unsigned char *jm, unsigned char *bscr, int mode,
+                         float2 *x, float2 *rc, float2 *d, float2 *xa, int nopen, int npad, uint32_t tbase,
+                         PassCnt &cnt) {
+    const int N = L.N, Nz = L.Nz, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nprod = pass_nprod(mode, Nz), ntr = L.ntr, nkc = L.nkc;
+    const size_t sl = (size_t)L.ncap * N;
+    const uint32_t bbytes = (uint32_t)npad * 256, bst = (uint32_t)L.ncap * 256;
     int err = 0;
-    for (int rt = 0; rt < L.ntr; ++rt) {
-        if (tid == 0) {
-            tc::fence_after_sync();
-            const unsigned char *arow = tiles + (size_t)rt * L.nkc * TILE_BYTES;
-            auto produce = [&](int kc) {
-                const int st = kc % PSTAGES;
-                mbar_expect_tx(&p.full[st], (uint32_t)TILE_BYTES + bbytes);
-                bulk_g2s(p.stA[st], arow + (size_t)kc * TILE_BYTES, (uint32_t)TILE_BYTES, &p.full[st]);
-                bulk_g2s(p.stB[st], bscr + (size_t)kc * bbytes, bbytes, &p.full[st]);
-            };
-            const int nk = L.nkc;
-            for (int kc = 0; kc < nk && kc < PSTAGES; ++kc) produce(kc);
-            for (int kc = 0; kc < nk && !err; ++kc) {
-                const int st = kc % PSTAGES;
-                if (!tc::mbar_wait(&p.full[st], (phases >> st) & 1u, WAIT_LIMIT)) { err = 1; break; }
-                phases ^= 1u << st;
+    if (warp == 0) {
+        // -------------------------------------------------------- A producer
+        if (lane == 0) {
+            uint32_t ia = cnt.a;
+            for (int s = 0; s < nprod && !err; ++s) {
+                const Prod q = pass_prod(mode, s, Nz, sl, x, rc, d, xa);
+                const unsigned char *tiles = jm + L.off_tiles + (size_t)q.slot * L.mat_bytes;
+                for (int t = 0; t < ntr * nkc && !err; ++t, ++ia) {
+                    const uint32_t st = ia % PA;
+                    if (ia >= PA && !tc::mbar_wait(&p.emptyA[st], ((ia / PA) - 1) & 1u, WAIT_LIMIT)) { err = 1; break; }
+                    mbar_expect_tx(&p.fullA[st], (uint32_t)TILE_BYTES);
+                    bulk_g2s(p.stA + st * TILE_BYTES, tiles + (size_t)t * TILE_BYTES, (uint32_t)TILE_BYTES,
+                             &p.fullA[st]);
+                }
+            }
+        }
+        __syncwarp();
+    } else if (warp == 2) {
+        // -------------------------------------------------------- B producer
+        if (lane == 0) {
+            uint32_t ib = cnt.b;
+            for (int s = 0; s < nprod && !err; ++s) {
+                if (!tc::mbar_wait(p.bReady, (cnt.r + s) & 1u, WAIT_LIMIT)) { err = 1; break; }
+                for (int t = 0; t < ntr * nkc && !err; ++t, ++ib) {
+                    const uint32_t st = ib % PB;
+                    if (ib >= PB && !tc::mbar_wait(&p.emptyB[st], ((ib / PB) - 1) & 1u, WAIT_LIMIT)) { err = 1; break; }
+                    mbar_expect_tx(&p.fullB[st], bbytes);
+                    bulk_g2s(p.stB + st * bst, bscr + (size_t)(t % nkc) * bbytes, bbytes, &p.fullB[st]);
+                }
+            }
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        // ------------------------------------------------------ MMA issuer
+        if (lane == 0) {
+            uint32_t ia = cnt.a, ib = cnt.b, iu = cnt.u;
+            for (int s = 0; s < nprod && !err; ++s) {
+                for (int rt = 0; rt < ntr && !err; ++rt, ++iu) {
+                    const uint32_t buf = iu & 1u, dacc = tbase + buf * (2 * L.ncap);
+                    if (iu >= 2 && !tc::mbar_wait(&p.accEmpty[buf], ((iu >> 1) - 1) & 1u, WAIT_LIMIT)) { err = 1; break; }
+                    for (int kc = 0; kc < nkc; ++kc, ++ia, ++ib) {
+                        const uint32_t sa = ia % PA, sb = ib % PB;
+                        if (!tc::mbar_wait(&p.fullA[sa], (ia / PA) & 1u, WAIT_LIMIT) ||
+                            !tc::mbar_wait(&p.fullB[sb], (ib / PB) & 1u, WAIT_LIMIT)) { err = 1; break; }
+                        tc::fence_after_sync();
+                        issue_pass_chunk(p.stA + sa * TILE_BYTES, p.stB + sb * bst, npad, dacc, kc == 0);
+                        tc::mma_commit(&p.emptyA[sa]);
+                        tc::mma_commit(&p.emptyB[sb]);
+                    }
+                    if (!err) tc::mma_commit(&p.accFull[buf]);
+                }
+            }
+        }
+        __syncwarp();
+    } else if (warp >= 4) {
+        // -------------------------------------------------------- epilogue
+        const int q4 = warp & 3;
+        const uint32_t lb = (uint32_t)(32 * q4) << 16;
+        uint32_t iu = cnt.u;
+        {
+            const Prod q0 = pass_prod(mode, 0, Nz, sl, x, rc, d, xa);
+            pass_convert(L, p, q0.v1, q0.v2, nopen, npad, bscr, false);
+            if (tid == 128) mbar_arrive(p.bReady);
+        }
+        for (int s = 0; s < nprod && !err; ++s) {
+            const Prod q = pass_prod(mode, s, Nz, sl, x, rc, d, xa);
+            const int *rexp_g = (const int *)(jm + L.off_rexp) + (size_t)q.slot * N;
+            for (int rt = 0; rt < ntr; ++rt, ++iu) {
+                const uint32_t buf = iu & 1u, dacc = tbase + lb + buf * (2 * L.ncap);
+                const int r = 32 * q4 + lane, i = rt * TM + r;
+                const bool rv = i < N;
+                const int er = rv ? rexp_g[i] : 0;
+                if (epi_any(!tc::mbar_wait(&p.accFull[buf], (iu >> 1) & 1u, WAIT_LIMIT))) { err = 1; break; }
                 tc::fence_after_sync();
-                issue_pass_chunk(p.stA[st], p.stB[st], npad, tbase, kc == 0);
-                tc::mma_commit(&p.empty[st]);
-                // refill the stage of chunk kc-1 (its MMAs ran ahead of chunk kc's)
-                if (kc >= 1 && kc - 1 + PSTAGES < nk) {
-                    const int s1 = (kc - 1) % PSTAGES;
-                    if (!tc::mbar_wait(&p.empty[s1], (phases >> (8 + s1)) & 1u, WAIT_LIMIT)) { err = 1; break; }
-                    phases ^= 1u << (8 + s1);
-                    produce(kc - 1 + PSTAGES);
-                }
-            }
-            // empty barriers of the chunks whose refill wait was skipped
-            for (int kc = max(0, nk - PSTAGES); kc < nk && !err; ++kc) {
-                if (kc == 0 && nk > PSTAGES) continue;
-                const int st = kc % PSTAGES;
-                if (!tc::mbar_wait(&p.empty[st], (phases >> (8 + st)) & 1u, WAIT_LIMIT)) { err = 1; break; }
-                phases ^= 1u << (8 + st);
-            }
-            tc::mma_commit(p.accf);
-        }
-        if (!tc::mbar_wait(p.accf, (phases >> 16) & 1u, WAIT_LIMIT)) err = 1;
-        phases ^= 1u << 16;
-        tc::fence_after_sync();
-        // epilogue: tile row r -> matrix row t of R -> output row iprow[t]
-        const int r = 32 * (warp & 3) + lane, t = rt * TM + r;
-        const bool rv = t < N;
-        const int i = rv ? p.iprow[t] : 0;
-        const int er = rv ? p.rexp[t] : 0;
-        for (int c16 = warp >> 2; c16 < npad / 16; c16 += 2) {
-            float re[16], im[16];
-            {
-                const uint32_t lb = (uint32_t)(32 * (warp & 3)) << 16;
-                tc::tmem_ld16(tbase + lb + c16 * 16, re);
-                tc::tmem_ld16(tbase + lb + npad + c16 * 16, im);
-                tc::tmem_wait_ld();
-            }
-            if (rv) {
-                float2 wv[16], xv[16];
+                for (int c16 = 0; c16 < npad / 16; ++c16) {
+                    float re[16], im[16];
+                    tc::tmem_ld16(dacc + c16 * 16, re);
+                    tc::tmem_ld16(dacc + npad + c16 * 16, im);
+                    float2 wv[16], xv[16], nv[16];
 #pragma unroll
-                for (int q = 0; q < 16; ++q) {
-                    const int j = c16 * 16 + q;
-                    wv[q] = (wadd && j < nopen) ? wadd[i + (size_t)N * j] : make_float2(0.f, 0.f);
-                    xv[q] = (xacc && j < nopen) ? xacc[i + (size_t)N * j] : make_float2(0.f, 0.f);
-                }
-#pragma unroll
-                for (int q = 0; q < 16; ++q) {
-                    const int j = c16 * 16 + q;
-                    float2 y = make_float2(0.f, 0.f);
-                    if (j < nopen) {
-                        const float f = alpha * tc::exp2i(er + p.cexp[j]);
-                        y = make_float2(fmaf(re[q], f, wv[q].x), fmaf(im[q], f, wv[q].y));
+                    for (int u = 0; u < 16; ++u) {
+                        const int j = c16 * 16 + u;
+                        const bool ok = rv && j < nopen;
+                        wv[u] = (ok && q.wadd) ? q.wadd[i + (size_t)N * j] : make_float2(0.f, 0.f);
+                        xv[u] = (ok && q.xacc) ? q.xacc[i + (size_t)N * j] : make_float2(0.f, 0.f);
+                        nv[u] = (ok && q.vn1) ? q.vn1[i + (size_t)N * j] : make_float2(0.f, 0.f);
                     }
-                    if (j < L.ncap) {
-                        out[i + (size_t)N * j] = y;
-                        // the refined solution of the next iteration, x += d
-                        if (xacc && j < nopen) xacc[i + (size_t)N * j] = make_float2(xv[q].x + y.x, xv[q].y + y.y);
+                    tc::tmem_wait_ld();
+#pragma unroll
+                    for (int u = 0; u < 16; ++u) {
+                        const int j = c16 * 16 + u;
+                        float2 y = make_float2(0.f, 0.f);
+                        if (rv && j < nopen) {
+                            const float f = q.alpha * tc::exp2i(er + p.cexp[j]);
+                            y = make_float2(fmaf(re[u], f, wv[u].x), fmaf(im[u], f, wv[u].y));
+                        }
+                        if (rv && j < L.ncap) {
+                            q.out[i + (size_t)N * j] = y;
+                            if (q.xacc && j < nopen) q.xacc[i + (size_t)N * j] = make_float2(xv[u].x + y.x, xv[u].y + y.y);
+                        }
+                        // |entry| of the next product's v in this column
+                        const float2 vn = q.vn1 ? make_float2(nv[u].x - y.x, nv[u].y - y.y) : y;
+                        const float m = (rv && j < nopen) ? fmaxf(fabsf(vn.x), fabsf(vn.y)) : 0.0f;
+                        const unsigned wm = __reduce_max_sync(0xffffffffu, __float_as_uint(m));
+                        if (lane == 0 && wm) atomicMax(&p.cmax[j], wm);
                     }
                 }
+                // accumulator read: it may take the row tile after next
+                tc::fence_before_sync();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&p.accEmpty[buf]);
+            }
+            if (err) break;
+            if (s + 1 < nprod) {
+                epi_bar();  // every store of y and every column maximum of this product
+                const Prod qn = pass_prod(mode, s + 1, Nz, sl, x, rc, d, xa);
+                pass_convert(L, p, qn.v1, qn.v2, nopen, npad, bscr, true);
+                if (tid == 128) mbar_arrive(p.bReady);
             }
         }
-        tc::fence_before_sync();
-        if (__syncthreads_or(err)) return false;
     }
+    if (__syncthreads_or(err)) return false;
+    cnt.a += (uint32_t)(nprod * ntr * nkc);
+    cnt.b += (uint32_t)(nprod * ntr * nkc);
+    cnt.u += (uint32_t)(nprod * ntr);
+    cnt.r += (uint32_t)nprod;
     return true;
 }
 
@@ -1215,20 +1344,23 @@ __global__ void __launch_bounds__(NT, 1) k_mixed_pass(MixedArgs a, int mode, int
     extern __shared__ __align__(128) unsigned char smem[];
     const MixedLayout &L = a.L;
     const int N = L.N, Nz = L.Nz, tid = threadIdx.x;
-    PassSmem p = carve_pass(smem, N, L.ncap);
-    negf::Smem js = carve_job(smem + pass_smem_bytes(N, L.ncap) - job_smem_bytes(N), N);
+    PassSmem p = carve_pass(smem, L.ncap);
+    // the job vectors of the tau step live in the A ring, idle by then
+    negf::Smem js = carve_job(p.stA, N);
     uint32_t ncols = 32;
-    while (ncols < 2u * L.ncap) ncols <<= 1;
+    while (ncols < 4u * L.ncap) ncols <<= 1;  // two accumulators of 2 ncap columns
     if (tid < 32) tc::tmem_alloc(p.tslot, ncols);
     if (tid == 0) {
-        for (int s = 0; s < PSTAGES; ++s) { tc::mbar_init(&p.full[s], 1); tc::mbar_init(&p.empty[s], 1); }
-        tc::mbar_init(p.accf, 1);
+        for (int s = 0; s < PA; ++s) { tc::mbar_init(&p.fullA[s], 1); tc::mbar_init(&p.emptyA[s], 1); }
+        for (int s = 0; s < PB; ++s) { tc::mbar_init(&p.fullB[s], 1); tc::mbar_init(&p.emptyB[s], 1); }
+        for (int s = 0; s < 2; ++s) { tc::mbar_init(&p.accFull[s], 1); tc::mbar_init(&p.accEmpty[s], 4); }
+        tc::mbar_init(p.bReady, 1);
     }
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tbase = *p.tslot;
-    uint32_t phases = 0;
+    PassCnt cnt{0, 0, 0, 0};
     unsigned char *bscr = a.scratch + (size_t)blockIdx.x * L.scratch_bytes;
     const size_t sl = (size_t)L.ncap * N;  // float2 per slice of a vector array
     bool ok = true;
@@ -1238,23 +1370,11 @@ __global__ void __launch_bounds__(NT, 1) k_mixed_pass(MixedArgs a, int mode, int
         const int nopen = ((const int *)(jm + L.off_oc))[L.ncap];
         const int npad = max(16, rup(nopen, 16));
         float2 *x = (float2 *)(jm + L.off_x), *rc = (float2 *)(jm + L.off_rc), *d = (float2 *)(jm + L.off_d);
-        if (mode == PASS_X0) {
-            for (int b = 1; b < Nz && ok; ++b)
-                ok = pass_product(L, p, jm, bscr, b, x + (b - 1) * sl, nullptr, x + b * sl, -1.f, nullptr, nopen,
-                                  npad, tbase, phases);
-        } else if (mode == PASS_BACK) {
-            for (int b = Nz - 2; b >= 0 && ok; --b)
-                ok = pass_product(L, p, jm, bscr, b + 1, rc + (b + 1) * sl, nullptr, rc + b * sl, -1.f, rc + b * sl,
-                                  nopen, npad, tbase, phases);
-        } else {
-            // unless this is the last iteration, x(b) += d(b) for b < Nz-1 on the way
-            // (the last slice is kept so that tau is formed from x + d in FP64)
-            float2 *xa = last ? nullptr : x;
-            ok = pass_product(L, p, jm, bscr, 0, rc, nullptr, d, 1.f, nullptr, nopen, npad, tbase, phases,
-                              (Nz > 1 && xa) ? xa : nullptr);
-            for (int b = 1; b < Nz && ok; ++b)
-                ok = pass_product(L, p, jm, bscr, b, rc + b * sl, d + ((b - 1) & 1) * sl, d + (b & 1) * sl, 1.f,
-                                  nullptr, nopen, npad, tbase, phases, (b < Nz - 1 && xa) ? xa + b * sl : nullptr);
+        // unless this is the last iteration, CORR folds d into x(b) for b < Nz-1
+        // on the way (the last slice is kept so that tau is formed from x + d in FP64)
+        ok = pass_run(L, p, jm, bscr, mode, x, rc, d, (mode == PASS_CORR && !last) ? x : nullptr, nopen, npad,
+                      tbase, cnt);
+        if (mode == PASS_CORR) {
             if (ok) {
                 // tau of x0 + d at the last slice, FP64
                 const negf::Geo &g = a.g;
@@ -1330,16 +1450,18 @@ __global__ void __launch_bounds__(NT, 1) k_mixed_pass(MixedArgs a, int mode, int
     if (tid < 32) tc::tmem_dealloc(tbase, ncols);
 }
 
-// FP64 residual of the block-tridiagonal system for x0, one CTA per (slice b,
-// job): r(b) = E_1 delta_b0 - x0(b-1) - D_b x0(b) - x0(b+1), D_b generated in
-// FP64 (negf::d_element) and the product on the FP64 tensor cores (DMMA
+// FP64 residual of the block-tridiagonal system for x0, one CTA per (job,
+// slice b): r(b) = E_1 delta_b0 - x0(b-1) - D_b x0(b) - x0(b+1), D_b in FP64 (the
+// off-diagonal part from the -c2 V(G_i - G_j) table, the diagonal from
+// negf::d_element) and the product on the FP64 tensor cores (DMMA
 // warp tiles of negf::WarpAcc), 64 x 64 output tiles, K in chunks of 16.
 __global__ void __launch_bounds__(NT, 2) k_mixed_residual(MixedArgs a) {
     extern __shared__ __align__(128) unsigned char smem[];
     const MixedLayout &L = a.L;
     const negf::Geo &g = a.g;
     const int N = L.N, Nz = L.Nz, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int b = blockIdx.x, w = blockIdx.y;
+    // jobs fastest: the CTAs in flight share slice b's D table in L2
+    const int w = blockIdx.x, b = blockIdx.y;
     if (a.status[w] != 0) return;
     constexpr int KC = negf::KC, AP = negf::AP, BP = negf::BP;
     double2 *sA = (double2 *)smem;           // [KC][AP]
@@ -1361,6 +1483,7 @@ __global__ void __launch_bounds__(NT, 2) k_mixed_residual(MixedArgs a) {
     const float2 *xb = x + b * sl;
     float2 *out = (float2 *)(jm + L.off_rc) + b * sl;
     const double2 *vs = g.vhat + (size_t)g.W * g.H * b;
+    const double2 *vt = a.voff + (size_t)N * L.ld * b;
     const int wm0 = (warp >> 2) * negf::WM, wn0 = (warp & 3) * negf::WN;
     for (int I0 = 0; I0 < N; I0 += negf::CM) {
         for (int J0 = 0; J0 < npad; J0 += negf::CN) {
@@ -1370,8 +1493,11 @@ __global__ void __launch_bounds__(NT, 2) k_mixed_residual(MixedArgs a) {
             for (int k0 = 0; k0 < N; k0 += KC) {
                 for (int e2 = tid; e2 < KC * negf::CM; e2 += NT) {
                     const int kk = e2 / negf::CM, ii = e2 % negf::CM, i = I0 + ii, k = k0 + kk;
-                    sA[kk * AP + ii] = (i < N && k < N) ? negf::d_element(g, js, vs, b, E, jb.y, i, k, js.nx[k], js.ny[k])
-                                                        : make_double2(0.0, 0.0);
+                    // off-diagonal D_b from the table (coalesced in i), the diagonal generated
+                    sA[kk * AP + ii] = (i < N && k < N)
+                                           ? (i == k ? negf::d_element(g, js, vs, b, E, jb.y, i, k, js.nx[k], js.ny[k])
+                                                     : vt[i + (size_t)L.ld * k])
+                                           : make_double2(0.0, 0.0);
                 }
                 for (int e2 = tid; e2 < KC * negf::CN; e2 += NT) {
                     const int jj = e2 / KC, kk = e2 % KC, j = J0 + jj, k = k0 + kk;
@@ -1673,7 +1799,7 @@ int negf_internal_mixed(negf_ctx *c, const double *h_E, const double *d_E, int n
                 // refinement steps; converged jobs (MIX_DONE) are skipped by the next ones
                 for (int it = 1; it <= pol.max_refinements; ++it) {
                     const int last = it == pol.max_refinements;
-                    k_mixed_residual<<<dim3(Nz, nw), NT, sm_res, st>>>(a);
+                    k_mixed_residual<<<dim3(nw, Nz), NT, sm_res, st>>>(a);
                     CKM(cudaGetLastError());
                     k_mixed_pass<<<nw, NT, sm_pass, st>>>(a, PASS_BACK, it, last);
                     CKM(cudaGetLastError());
