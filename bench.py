@@ -647,7 +647,7 @@ def run_batched(args):
 
     from negftrans_b200 import workloads as W
     from negftrans_b200.negf import Engine, transmission_batch
-    probs = W.batched_uneven()
+    probs = W.batched_uneven(n_range=(180, 260))  # per-k cutoffs: bases of 180-263 plane waves
     engines = [Engine(*p["args"]) for p in probs]
     E_all = np.linspace(0.0, W.MSTAR * 0.030 / 27.211386245988, 1024, endpoint=False)
     # tile shapes by the autotuner: per basis size, time the variants on a full
@@ -662,7 +662,7 @@ def run_batched(args):
             if p["N"] == N:
                 engines[i].set_variant(v)
     perm = np.random.default_rng(2024).permutation(len(E_all))
-    B = args.batch
+    B = args.batch or 32
     batches = [E_all[perm[(s * B + np.arange(B)) % len(E_all)]] for s in range(args.warmup + args.steps)]
     for s in range(args.warmup):
         transmission_batch(engines, batches[s])

@@ -94,19 +94,40 @@ def config(name: str, nz: int | None = None) -> Workload:
     raise KeyError(name)
 
 
-def batched_uneven(nkx=4, nzs=(300, 600, 1200), encut_eV=0.0105288, grid=64, seed=4000):
+def _encut_for_size(n_target, L, kx, ky, hi):
+    """Smallest cutoff (Hartree) whose basis |k+G|^2/2 <= ENCUT at (kx, ky) has
+    at least n_target plane waves (the count is monotone in the cutoff)."""
+    from .grid import PlaneWaveBasis_k
+    lo = 0.0
+    for _ in range(60):
+        mid = 0.5 * (lo + hi)
+        if len(PlaneWaveBasis_k(mid, L, L, kx, ky)[0]) >= n_target:
+            hi = mid
+        else:
+            lo = mid
+    return hi
+
+
+def batched_uneven(nkx=4, nzs=(300, 600, 1200), encut_eV=0.0105288, grid=64, seed=4000, n_range=None):
     """Problems of the uneven batch: one per (device, k-point) of an nkx x nkx
-    Monkhorst-Pack mesh, each with its own basis |k+G| <= G_c (sizes vary with
-    k), devices of N_z slices of 1 nm with seeded V_g ~ U[20, 80] meV and
-    w ~ U[8, 25] nm (+ GaAs scaling).  Returns a list of dicts holding the
-    Engine arguments ('args'), 'N', 'Nz' and the device index."""
+    Monkhorst-Pack mesh, each with its own basis |k+G| <= G_c, devices of N_z
+    slices of 1 nm with seeded V_g ~ U[20, 80] meV and w ~ U[8, 25] nm (+ GaAs
+    scaling).  With one G_c (n_range None) the k shifts change the basis size
+    by a few plane waves only; n_range = (lo, hi) gives k-point i its own cutoff
+    so that the sizes spread evenly over [lo, hi].  Returns a list of dicts
+    holding the Engine arguments ('args'), 'N', 'Nz' and the device index."""
     from .grid import Kpoint_mesh_construction, PlaneWaveBasis_k, V_reciprocal_all
     from .constants import A_0
     rng = np.random.Generator(np.random.PCG64(seed))
     L = 1000.0 / A_0
     enc = encut_eV / HARTREE
     kp = Kpoint_mesh_construction(nkx, nkx, L, L)
-    bases = [PlaneWaveBasis_k(enc, L, L, kx, ky) for kx, ky, _ in kp]
+    if n_range is None:
+        bases = [PlaneWaveBasis_k(enc, L, L, kx, ky) for kx, ky, _ in kp]
+    else:
+        targets = np.rint(np.linspace(n_range[0], n_range[1], len(kp))).astype(int)
+        bases = [PlaneWaveBasis_k(_encut_for_size(int(t), L, kx, ky, 20.0 * enc), L, L, kx, ky)
+                 for t, (kx, ky, _) in zip(targets, kp)]
     nmax = max(int(np.max(np.abs(np.concatenate([b[0], b[1]])))) for b in bases)
     # the reference's NGX (main.f90:94-100), raised so that every pair
     # difference of a shifted basis indexes inside the table; the table keeps

@@ -291,6 +291,30 @@ def test_transmission_batch_uneven(oracle):
         np.testing.assert_allclose(t, ref, rtol=RTOL, atol=1e-12)
 
 
+def test_transmission_batch_uneven_spread(oracle):
+    """The uneven batch of the benchmark's shape at reduced length: per-k
+    cutoffs spreading the bases over 180-263 plane waves (both kernel
+    variants), devices of 4 and 7 slices, one persistent launch per variant,
+    every problem against the oracle."""
+    from negftrans_b200.negf import transmission_batch
+    probs = W.batched_uneven(nkx=2, nzs=(4, 7), n_range=(180, 260))
+    sizes = sorted({p["N"] for p in probs})
+    assert sizes[0] <= 185 and sizes[-1] >= 256 and len(sizes) == 4
+    E = np.linspace(0.0, 0.067 * 0.03 / HARTREE, 5, endpoint=False)
+    engines = [Engine(*p["args"]) for p in probs]
+    try:
+        tau, info, _ = transmission_batch(engines, E)
+    finally:
+        for e in engines:
+            e.close()
+    assert info == 0
+    for p, t in zip(probs, tau):
+        nx, ny, vhat, lx, ly, lz, vl, vr, eta, kp = p["args"]
+        ref, _ = oracle.transmission_jobs(oracle.Problem(nx, ny, vhat, lx, ly, lz, vl, vr, eta, kp), E,
+                                          nthreads=8)
+        np.testing.assert_allclose(t, ref, rtol=RTOL, atol=1e-12)
+
+
 @pytest.mark.parametrize("flat", [True, False])
 def test_lattice_lead_model(oracle, flat):
     """lead_model = 1 (exact lattice surface Green's function of the leads)

@@ -119,6 +119,21 @@ def test_workload_shapes():
         assert np.max(np.abs(pr.nx[:, None] - pr.nx[None, :])) <= pr.NGX
 
 
+def test_uneven_batch_spreads_the_basis_sizes(oracle):
+    """cfg 4 with per-k cutoffs: 16 k-points x 3 devices, bases spread over
+    180-263 plane waves; every per-k basis is the oracle's basis at its own
+    cutoff and k, and the V table covers every pair difference."""
+    probs = W.batched_uneven(n_range=(180, 260))
+    assert len(probs) == 48 and sorted({p["Nz"] for p in probs}) == [300, 600, 1200]
+    sizes = sorted({p["N"] for p in probs})
+    assert len(sizes) == 16 and 180 <= sizes[0] <= 185 and 256 < sizes[-1] <= 270
+    for p in probs[:16]:
+        nx, ny, vhat = p["args"][:3]
+        ngx = (vhat.shape[0] - 1) // 2
+        assert np.max(np.abs(np.subtract.outer(nx, nx))) <= ngx
+        assert np.max(np.abs(np.subtract.outer(ny, ny))) <= (vhat.shape[1] - 1) // 2
+
+
 def test_disorder_statistics():
     V = W.qpc_potential(32, 32, 64, 100.0, 64.0, 0.0, 15.0, 20.0, disorder=0.002, seed=7)
     assert abs(np.sqrt(np.mean(V ** 2)) - 0.002) < 1e-12
