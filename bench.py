@@ -2,13 +2,16 @@
 """Benchmark of the RGF hot path: (E,k) energy-point solves per second,
 mixed precision against FP64 on one B200.
 
-Workload (default): qpc_disorder_n221 -- N = 221 plane waves, N_z = 800
-slices, Gamma point, a QPC with 2 meV / 10 nm disorder, energies from the
-2048-point grid on [0, 40) meV.  `--workload qpc_disorder_n797` is the large
-block case (N = 797, N_z = 400, 1024 energies; a step there takes ~10-20 s).
+Workload (default): qpc_disorder_n797 -- the large-block configuration the
+mixed-vs-FP64 metric is quoted on: N = 797 plane waves (33x33 G grid, circular
+cutoff), N_z = 400 slices of 1 nm, Gamma point, a QPC (V_g = 60 meV, w = 20 nm)
+with 2 meV / 10 nm disorder, energies from the 1024-point grid on [0, 50) meV.
+`--workload qpc_disorder_n221` is the medium case (N = 221, N_z = 800, 2048
+energies on [0, 40) meV).
 
 --precision mixed (default): one step = negf_transmission(NEGF_MIXED) on
-`--batch` energies (default one mixed wave, one job per SM): split-fp16
+`--batch` energies (default: whole mixed waves, about one SM per job; at
+N = 797 device memory bounds a wave to ~61 jobs on two SMs each): split-fp16
 tensor-core factorization, FP64 residual refinement, FP64 re-run of rejected
 jobs -- every job of the step, whatever path it takes.  `value` = jobs / the
 device time of the call (CUDA events on the context's stream); `e2e` = jobs /
@@ -50,9 +53,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="qpc_disorder_n221")
+    ap.add_argument("--workload", default="qpc_disorder_n797")
     ap.add_argument("--batch", type=int, default=0,
-                    help="energies per step and GPU (0: one mixed wave = the SM count, or 2x for fp64)")
+                    help="energies per step and GPU (0: whole mixed waves, about the SM count; 2x the SM count for fp64)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                     help="mixed: NEGF_MIXED headline with the FP64 rate and max|dT| beside it")
     ap.add_argument("--nz", type=int, default=0,
@@ -81,12 +84,6 @@ def host_threads(req, per_job_bytes=0):
     return max(1, t)
 
 
-def oracle_job_bytes(pr):
-    """Peak memory of one oracle F-mode job: H, D, first column and generator_r
-    (four N x N x N_z complex arrays)."""
-    return 4 * 16 * pr.N * pr.N * pr.Nz
-
-
 def flops_per_solve(N, Nz):
     """Flops of one transmission (F-mode) sweep in the reference's algorithm:
     N_z inverses and N_z-1 complex block products at 8 N^3 real flops each
@@ -111,11 +108,6 @@ def executed_flops(N, Nz, n_open):
     """Flops this engine executes per sweep: N_z inverses (8 N^3) and N_z-1
     chain products restricted to the n_open rows the trace reads (8 n N^2)."""
     return 8.0 * N ** 3 * Nz + 8.0 * n_open * N ** 2 * (Nz - 1)
-
-
-def oracle_problem(O, pr):
-    a = pr.atomic
-    return O.Problem(pr.nx, pr.ny, pr.vhat, a.LX, a.LY, a.LZ, a.V_L, a.V_R, a.ETA, pr.kpoint)
 
 
 def oracle_inputs(w):
@@ -148,17 +140,26 @@ def cpu_rate_problem(p, energies, nthreads, reps=1):
     return len(E) / statistics.mean(times), times
 
 
-def cpu_rate(pr, energies, nthreads, reps=1):
-    """Solves/s of the oracle port on `nthreads` host threads (one job each)."""
-    from oracle import oracle as O
-    p = oracle_problem(O, pr)
-    E = np.asarray(energies[:nthreads], np.float64)
-    times = []
-    for _ in range(reps):
-        t0 = time.perf_counter()
-        O.transmission_jobs(p, E, nthreads=nthreads)
-        times.append(time.perf_counter() - t0)
-    return len(E) / statistics.mean(times), times
+# one CPU sweep of a bounded sample should take about this long (seconds per job)
+CPU_SAMPLE_S = 10.0
+
+
+def cpu_sample_nz(N, Nz):
+    """Slices of the CPU sample sweep: the whole device when one oracle sweep
+    takes under ~3 CPU_SAMPLE_S (16 N^3 N_z flop at ~20 GFLOP/s per core, the
+    LAPACK/BLAS rates measured for these block sizes), else a device of the same
+    basis and slice thickness cut to fewer slices.  The oracle's work per slice
+    (one zgetrf+zgetri and one zgemm of N x N) does not depend on the potential,
+    so the full sweep's rate is the sample's times (2 nz - 1) / (2 N_z - 1)."""
+    est = 16.0 * N ** 3 * Nz / 20e9
+    if est <= 3 * CPU_SAMPLE_S:
+        return Nz
+    return max(8, int(Nz * CPU_SAMPLE_S / est))
+
+
+def sweep_scale(nz, Nz):
+    """Work of a sweep of nz slices over one of Nz slices (nz inverses, nz - 1 products)."""
+    return (2.0 * nz - 1.0) / (2.0 * Nz - 1.0)
 
 
 class ClockSampler:
@@ -233,13 +234,41 @@ def fp64_peak_tflops(torch, dev):
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
+def sample_problem(name, nz_full):
+    """The oracle's problem for the CPU sample of workload `name`: the whole
+    device, or (cpu_sample_nz) the same basis and slice thickness over fewer
+    slices; its inputs come from the oracle's own set-up."""
+    from negftrans_b200 import workloads as W
+    w = W.config(name)
+    p, E = oracle_inputs(w)
+    nz = cpu_sample_nz(p.N, nz_full)
+    if nz != nz_full:
+        p, E = oracle_inputs(W.config(name, nz=nz))
+    return w, p, E
+
+
+def cpu_baseline(args, N, Nz):
+    """cpu_baseline of this implementation's line: the oracle port on every host
+    core (one sweep per thread) over the bounded sample of sample_problem."""
+    _, p, E = sample_problem(args.workload, Nz)
+    nth = host_threads(args.cpu_threads, 4 * 16 * p.N * p.N * p.Nz)
+    r, t = cpu_rate_problem(p, E[::7], nth)
+    rate = r * sweep_scale(p.Nz, Nz)
+    what = "sweeps of this workload" if p.Nz == Nz else \
+        f"sweeps over {p.Nz} of the {Nz} slices (same basis, blocks and slice thickness; the rate is scaled by the work per sweep)"
+    return {"value": rate, "unit": UNIT, "cores": nth, "kind": "port",
+            "sample": f"{nth} {what}, one per thread, {t[0]:.1f} s"}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     from negftrans_b200 import workloads as W
     w = W.config(args.workload)
-    p, E = oracle_inputs(w)
+    Nz_full = w.V_eV.shape[2]
+    w, p, E = sample_problem(args.workload, Nz_full)
+    scale = sweep_scale(p.Nz, Nz_full)
     nth = host_threads(args.cpu_threads, 4 * 16 * p.N * p.N * p.Nz)
     for _ in range(args.warmup):
         cpu_rate_problem(p, E, nth)
@@ -248,14 +277,19 @@ def run_reference(args):
         sample = np.roll(E, -s * nth)
         r, t = cpu_rate_problem(p, sample, nth)
         times.append(t[0])
-    ms = 1e3 * statistics.mean(times)
+    # a step is nth full sweeps; with a shortened device its time is the sample's / scale
+    ms = 1e3 * statistics.mean(times) / scale
     value = nth / (ms * 1e-3)
-    sample = f"{nth} (E,k) sweeps per step, one per host thread (N={p.N}, Nz={p.Nz})"
+    if p.Nz == Nz_full:
+        sample = f"{nth} (E,k) sweeps per step, one per host thread (N={p.N}, Nz={p.Nz})"
+    else:
+        sample = (f"{nth} (E,k) sweeps per step, one per host thread, each over {p.Nz} of the {Nz_full} slices "
+                  f"(N={p.N}, same slice thickness; time scaled by the work per sweep, {scale:.4f})")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-        "config": workload_config(args.workload, p.N, p.Nz, w.n_energy, len(p.kpt)),
+        "config": workload_config(args.workload, p.N, Nz_full, w.n_energy, len(p.kpt)),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": nth, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference (Fortran+MPI+FFTW+LAPACK) cannot be built on this image; its "
@@ -403,10 +437,7 @@ def run_ours_fp64(args):
             line["e2e_matches_device"] = bool(np.allclose(tau_h, tau_dev, rtol=1e-12, atol=1e-14))
 
     if rank == 0 and not args.no_cpu_baseline and world == 1:
-        nth = host_threads(args.cpu_threads, oracle_job_bytes(pr))
-        r, t = cpu_rate(pr, E_all[::7], nth)
-        line["cpu_baseline"] = {"value": r, "unit": UNIT, "cores": nth, "kind": "port",
-                                "sample": f"{nth} sweeps of this workload, one per thread, {t[0]:.1f} s"}
+        line["cpu_baseline"] = cpu_baseline(args, pr.N, pr.Nz)
     if args.density:
         # the density path (D mode + contour, negf.f90:9-113) on the same device, as
         # information beside the headline: contour jobs per second
@@ -502,9 +533,12 @@ def run_ours(args):
     nk = len(pr.kpoint)
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
     eng = Engine(*pr.engine_args(), device=local)
-    # one mixed wave holds at most one job per SM (fewer when device memory is short)
-    eng.transmission(E_all[:8], precision=NEGF_MIXED)  # set-up call (allocations)
-    B = args.batch or sms
+    # set-up call (allocations) on one SM count of energies; it also reports how
+    # many jobs a mixed wave holds on this device (one job per SM, or fewer on two
+    # SMs each when device memory bounds the wave), so a step is whole waves
+    eng.transmission(E_all[:sms], precision=NEGF_MIXED)
+    wave = max(1, eng.mixed_stats()["jobs_per_wave"])
+    B = args.batch or wave * max(1, round(sms / wave))
     n_steps = args.warmup + args.steps
     perm = np.random.default_rng(2024).permutation(len(E_all))
     # a step is B energies per GPU: every rank holds the step's whole batch and the
@@ -561,7 +595,7 @@ def run_ours(args):
         timed_E, timed_tau = timed_E[lo:hi], timed_tau[lo:hi]
     F = 2 * sms
     fp_ms, fp_jobs, tau64 = [], [], np.zeros_like(timed_tau)
-    eng.transmission(timed_E[:F], precision=NEGF_FP64)  # warm-up
+    eng.transmission(timed_E[:8], precision=NEGF_FP64)  # warm-up (kernel variant chosen, workspace)
     for c0 in range(0, len(timed_E), F):
         chunk = timed_E[c0:c0 + F]
         t64, _ = eng.transmission(chunk, precision=NEGF_FP64)
@@ -605,7 +639,8 @@ def run_ours(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64 (split-fp16 tensor products, f32 accumulate) + f64 refinement",
             "data": "synthetic",
             "config": workload_config(args.workload, N, Nz, w.n_energy, nk),
-            "step": {"energies_per_gpu": B, "precision": "mixed (NEGF_MIXED)",
+            "step": {"energies_per_gpu": B, "jobs_per_wave": wave,
+                     "ctas_per_job": stats[-1].get("ctas_per_job"), "precision": "mixed (NEGF_MIXED)",
                      "parallelism": f"energy-sharded x{world}",
                      "l2": f"per-job factor storage ~{8 * N * N * Nz / 1e6:.0f} MB > L2 (inputs larger than L2)"},
             "fp64_value": fp64_value,
@@ -628,10 +663,7 @@ def run_ours(args):
             "singular_jobs": int(sum(1 for i in infos if i)),
         }
     if rank == 0 and not args.no_cpu_baseline and world == 1:
-        nth = host_threads(args.cpu_threads, oracle_job_bytes(pr))
-        r, t = cpu_rate(pr, E_all[::7], nth)
-        line["cpu_baseline"] = {"value": r, "unit": UNIT, "cores": nth, "kind": "port",
-                                "sample": f"{nth} sweeps of this workload, one per thread, {t[0]:.1f} s"}
+        line["cpu_baseline"] = cpu_baseline(args, pr.N, pr.Nz)
     if rank == 0:
         print(json.dumps(line), flush=True)
     eng.close()

@@ -82,7 +82,10 @@ typedef struct negf_mixed_policy {
                               * after more).  Default 1e-7.                             */
     int32_t max_refinements; /* refinement steps before a job that has not met the
                               * tolerance is re-run in FP64 (1..8, default 5)           */
-    int32_t pad;
+    int32_t ctas_per_job;    /* CTAs that sweep one job: 1, 2 (a thread-block cluster
+                              * on two SMs), or 0 = automatic (2 when one CTA per job
+                              * would leave at least half of the SMs idle, e.g. when
+                              * the factor storage bounds the wave)                    */
 } negf_mixed_policy;
 
 typedef struct negf_mixed_stats {
@@ -91,7 +94,7 @@ typedef struct negf_mixed_stats {
     int32_t n_fp64_policy;   /* sent to FP64 by the policy                              */
     int32_t n_fp64_rejected; /* refined, rejected by the check and re-run in FP64       */
     int32_t jobs_per_wave;   /* mixed jobs resident at once (device memory bound)       */
-    int32_t pad;
+    int32_t ctas_per_job;    /* CTAs per job of the sweep in the last call             */
     double max_correction;   /* largest |d| / |x| among accepted jobs                   */
     double mixed_ms;         /* device time of the mixed part (CUDA events)             */
     double fp64_ms;          /* device time of the FP64 re-runs                         */

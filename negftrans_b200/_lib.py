@@ -49,16 +49,16 @@ class Problem(C.Structure):
 
 class MixedPolicy(C.Structure):
     _fields_ = [("threshold_window", C.c_double), ("eta_fp64_below", C.c_double), ("tau_tolerance", C.c_double),
-                ("max_refinements", C.c_int32), ("pad", C.c_int32)]
+                ("max_refinements", C.c_int32), ("ctas_per_job", C.c_int32)]
 
 
 class MixedStats(C.Structure):
     _fields_ = [("n_jobs", C.c_int32), ("n_mixed", C.c_int32), ("n_fp64_policy", C.c_int32),
-                ("n_fp64_rejected", C.c_int32), ("jobs_per_wave", C.c_int32), ("pad", C.c_int32),
+                ("n_fp64_rejected", C.c_int32), ("jobs_per_wave", C.c_int32), ("ctas_per_job", C.c_int32),
                 ("max_correction", C.c_double), ("mixed_ms", C.c_double), ("fp64_ms", C.c_double)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class Stats(C.Structure):

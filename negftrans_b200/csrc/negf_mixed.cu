@@ -70,6 +70,55 @@ __device__ inline void gj_identity(const GjSmem &s, int N) {
     for (int i = threadIdx.x; i < N; i += NT) { s.prow[i] = i; s.iprow[i] = i; }
 }
 
+// ------------------------------------------------------------ job teams
+// The CTAs that share one job: a thread-block cluster of n = 1 or 2 CTAs.
+// With n = 2 the rows of every per-row phase and the output tiles of every
+// trailing update are split between the two, and the phases are separated
+// by cluster barriers (release / acquire at cluster scope, so the global
+// writes of one CTA are visible to the other after it).  Loads of the shared
+// working matrix go through L2 (ld.global.cg): its lines may have been
+// rewritten by the other SM since this SM's L1 last held them.
+struct Team {
+    int rank, n;
+    int *gx;        // per-job global exponents (n > 1): rexpW [ntr * TM], then cexpB [ntc * PTN]
+    int *slot;      // shared [2]: this CTA's contribution to team_or, by call parity
+    uint32_t par;
+};
+__device__ __forceinline__ void cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n"
+                 "barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void team_sync(const Team &t) {
+    if (t.n > 1) cluster_sync();
+    else __syncthreads();
+}
+// OR of a CTA-uniform flag over the team; every thread of both CTAs calls it
+// at the same point and gets the same result.  The slot of a parity is
+// rewritten two calls later, after the peer has passed the barrier between.
+__device__ inline int team_or(Team &t, int v) {
+    if (t.n == 1) return v;
+    int *sl = t.slot + (t.par & 1u);
+    if (threadIdx.x == 0) *sl = v;
+    cluster_sync();
+    int r = 0;
+    for (int q = 0; q < t.n; ++q) {
+        uint32_t ra;
+        int x;
+        asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(ra) : "r"(tc::smem_u32(sl)), "r"(q));
+        asm volatile("ld.shared::cluster.s32 %0, [%1];\n" : "=r"(x) : "r"(ra) : "memory");
+        r |= x;
+    }
+    t.par++;
+    return r;
+}
+// [lo, hi) of this CTA's share of `count` items in units of `gran`
+__device__ __forceinline__ int2 team_range(const Team &t, int count, int gran) {
+    const int units = (count + gran - 1) / gran;
+    const int u0 = units * t.rank / t.n, u1 = units * (t.rank + 1) / t.n;
+    return make_int2(min(count, u0 * gran), min(count, u1 * gran));
+}
+__device__ __forceinline__ float2 ldcg2(const float2 *p) { return __ldcg(p); }
+
 // ------------------------------------------------ diagonal-block inverse
 // Sortable 32-bit key: |re|+|im| bits (non-negative floats order as
 // unsigned integers) with the low 10 bits replaced by 1023 - row, so the
@@ -97,7 +146,7 @@ __device__ inline int invert_diag_warp(const float2 *__restrict__ A, int ld, int
     float2 R[32];
 #pragma unroll
     for (int j = 0; j < 32; ++j)
-        R[j] = (valid && j < m) ? A[(k0 + lane) + (size_t)ld * (k0 + j)]
+        R[j] = (valid && j < m) ? ldcg2(A + (k0 + lane) + (size_t)ld * (k0 + j))
                                 : make_float2((!valid && j == lane) ? 1.0f : 0.0f, 0.0f);
     int *spr = s.spr;
     bool used = false;
@@ -343,11 +392,13 @@ __device__ inline void issue_split_mma(uint32_t a0, uint32_t b0, int n, uint32_t
 // row; the row's panel values are staged in the pipe's C buffers (idle
 // between trailing updates) so that the k loop stays rolled.  Tile rows
 // N .. ntr*TM-1 are zero.
+// Rows [rlo, rhi) of the ntr * TM tile rows; with gexp the row exponents
+// also go to global memory for the other CTA of the team.
 __device__ inline void panel_w(const Pipe &P, const GjSmem &s, float2 *__restrict__ A, int ld, int N, int k0,
-                               int m) {
-    const int ntr = (N + TM - 1) / TM, tid = threadIdx.x;
+                               int m, int rlo, int rhi, int *gexp) {
+    const int tid = threadIdx.x;
     float2 *xs = (float2 *)P.sC;  // [32][NT]: 64 KB of the three contiguous C buffers
-    for (int row = tid; row < ntr * TM; row += NT) {
+    for (int row = rlo + tid; row < rhi; row += NT) {
         float2 w[32];
         const int rk = row - k0;
         if (row >= N) {
@@ -363,7 +414,7 @@ __device__ inline void panel_w(const Pipe &P, const GjSmem &s, float2 *__restric
         } else {
             // all 32 loads in flight before the first staging store
 #pragma unroll
-            for (int k = 0; k < 32; ++k) w[k] = (k < m) ? A[row + (size_t)ld * (k0 + k)] : make_float2(0.f, 0.f);
+            for (int k = 0; k < 32; ++k) w[k] = (k < m) ? ldcg2(A + row + (size_t)ld * (k0 + k)) : make_float2(0.f, 0.f);
 #pragma unroll
             for (int k = 0; k < 32; ++k) xs[k * NT + tid] = w[k];
 #pragma unroll
@@ -391,6 +442,7 @@ __device__ inline void panel_w(const Pipe &P, const GjSmem &s, float2 *__restric
         const int e = tc::scale_exponent(mx);
         const float sc = tc::exp2i(-e);
         P.rexpW[row] = e;
+        if (gexp) gexp[row] = e;
         unsigned char *tile = P.wt + (size_t)(row / TM) * WTILE;
 #pragma unroll
         for (int g = 0; g < 4; ++g) {
@@ -410,10 +462,13 @@ __device__ inline void panel_w(const Pipe &P, const GjSmem &s, float2 *__restric
 }
 // B tiles: rest column jr (the columns outside the panel, in order) with the
 // K values A(k0 + kk, col(jr)) of the panel's rows; four threads per column.
-__device__ inline void convert_b(const Pipe &P, const float2 *__restrict__ A, int ld, int N, int k0, int nbt) {
+// Rest columns [clo, chi) (multiples of 8); with gexp the column exponents
+// also go to global memory for the other CTA of the team.
+__device__ inline void convert_b(const Pipe &P, const float2 *__restrict__ A, int ld, int N, int k0, int nbt,
+                                 int clo, int chi, int *gexp) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane & 3;
-    const int nrest = N - nbt, ntc = (nrest + PTN - 1) / PTN;
-    for (int c0 = warp * 8; c0 < ntc * PTN; c0 += NWARP * 8) {
+    const int nrest = N - nbt;
+    for (int c0 = clo + warp * 8; c0 < chi; c0 += NWARP * 8) {
         const int jr = c0 + (lane >> 2);
         const bool cv = jr < nrest;
         const int col = jr < k0 ? jr : jr + nbt;
@@ -422,14 +477,17 @@ __device__ inline void convert_b(const Pipe &P, const float2 *__restrict__ A, in
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
             const int kk = 8 * g + q;
-            v[q] = (cv && kk < nbt) ? A[k0 + kk + (size_t)ld * col] : make_float2(0.f, 0.f);
+            v[q] = (cv && kk < nbt) ? ldcg2(A + k0 + kk + (size_t)ld * col) : make_float2(0.f, 0.f);
             m = fmaxf(m, fmaxf(fabsf(v[q].x), fabsf(v[q].y)));
         }
         m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 1));
         m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 2));
         const int e = tc::scale_exponent(m);
         const float sc = tc::exp2i(-e);
-        if (g == 0) P.cexpB[jr] = e;
+        if (g == 0) {
+            P.cexpB[jr] = e;
+            if (gexp) gexp[jr] = e;
+        }
         __align__(16) __half rh[8], rl[8], ih[8], il[8];
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
@@ -447,10 +505,12 @@ __device__ inline void convert_b(const Pipe &P, const float2 *__restrict__ A, in
 
 // A(:, rest) += W * B for the panel [k0, k0+nbt) (W and B tiles already in
 // the CTA's global scratch), pipelined (see above); the C tiles of matrix cm
-// move by TMA.  Returns false if a wait timed out (uniform).
-__device__ inline bool trailing_pipe(Pipe &P, int N, int k0, int nbt, const CMat &cm) {
+// move by TMA.  Output tiles [t0, t1) of the ntr x ntc tiles (row tile major),
+// so that the CTAs of a team share the update.  Returns false if a wait timed
+// out (uniform over the CTA).
+__device__ inline bool trailing_pipe(Pipe &P, int N, int k0, int nbt, const CMat &cm, int t0, int t1) {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int nrest = N - nbt, ntr = (N + TM - 1) / TM, ntc = (nrest + PTN - 1) / PTN, T = ntr * ntc;
+    const int nrest = N - nbt, ntc = (nrest + PTN - 1) / PTN, T = t1 - t0;
     // generic stores (W/B tiles in global, the staging in the C buffers) before
     // the bulk copies and TMA tiles that read or overwrite them
     asm volatile("fence.proxy.async;\n" ::: "memory");
@@ -463,25 +523,30 @@ __device__ inline bool trailing_pipe(Pipe &P, int N, int k0, int nbt, const CMat
         const int jr = (t % ntc) * PTN;
         return jr < k0 ? jr : jr + nbt;
     };
+    // the W tile changes at the first local tile and at every row-tile start
+    auto w_first = [&](int v) -> bool { return v == 0 || (t0 + v) % ntc == 0; };
+    auto w_last = [&](int v) -> bool { return v == T - 1 || (t0 + v) % ntc == ntc - 1; };
+    auto w_index = [&](int v) -> uint32_t { return bW + (uint32_t)((t0 + v) / ntc - t0 / ntc); };
     if (warp == 0) {
         // ------------------------------------------------------ producer
         if (lane == 0) {
             auto load = [&](int u) -> bool {
-                if (u % ntc == 0) {
-                    const uint32_t iw = bW + u / ntc;
+                const int t = t0 + u;
+                if (w_first(u)) {
+                    const uint32_t iw = w_index(u);
                     if (iw >= 1 && !tc::mbar_wait(P.emptyW, (iw - 1) & 1u, WAIT_LIMIT)) return false;
                     expect_bytes(P.fullW, WTILE);
-                    bulk_copy(P.sW, P.wt + (size_t)(u / ntc) * WTILE, WTILE, P.fullW);
+                    bulk_copy(P.sW, P.wt + (size_t)(t / ntc) * WTILE, WTILE, P.fullW);
                 }
                 const uint32_t ib = bB + u, ic = bT + u;
                 if (ib >= NBB && !tc::mbar_wait(&P.emptyB[ib % NBB], ((ib - NBB) / NBB) & 1u, WAIT_LIMIT))
                     return false;
                 expect_bytes(&P.fullB[ib % NBB], BTILE);
-                bulk_copy(P.sB + (ib % NBB) * BTILE, P.bt + (size_t)(u % ntc) * BTILE, BTILE, &P.fullB[ib % NBB]);
+                bulk_copy(P.sB + (ib % NBB) * BTILE, P.bt + (size_t)(t % ntc) * BTILE, BTILE, &P.fullB[ib % NBB]);
                 // the C buffer last held tile u - NCB, whose store this thread issued
                 bulk_wait_read0();
                 expect_bytes(&P.fullC[ic % NCB], CTILE);  // the whole box, out-of-range elements zero-filled
-                tma_load4(P.sC + (ic % NCB) * CTILE, cm.tm, (u / ntc) * TM, tile_col0(u), cm.z, cm.w, &P.fullC[ic % NCB]);
+                tma_load4(P.sC + (ic % NCB) * CTILE, cm.tm, (t / ntc) * TM, tile_col0(t), cm.z, cm.w, &P.fullC[ic % NCB]);
                 return true;
             };
             for (int u = 0; u < NCB && u < T && !err; ++u)
@@ -489,7 +554,7 @@ __device__ inline bool trailing_pipe(Pipe &P, int N, int k0, int nbt, const CMat
             for (int v = 0; v < T && !err; ++v) {
                 const uint32_t ic = bT + v;
                 if (!tc::mbar_wait(&P.doneC[ic % NCB], (ic / NCB) & 1u, WAIT_LIMIT)) { err = 1; break; }
-                tma_store4(cm.tm, (v / ntc) * TM, tile_col0(v), cm.z, cm.w, P.sC + (ic % NCB) * CTILE);  // clipped
+                tma_store4(cm.tm, ((t0 + v) / ntc) * TM, tile_col0(t0 + v), cm.z, cm.w, P.sC + (ic % NCB) * CTILE);  // clipped
                 bulk_commit();
                 if (v + NCB < T && !load(v + NCB)) err = 1;
             }
@@ -503,13 +568,13 @@ __device__ inline bool trailing_pipe(Pipe &P, int N, int k0, int nbt, const CMat
             for (int t = 0; t < T; ++t) {
                 const uint32_t ic = bT + t, ib = bB + t, a = ic & 1u;
                 if (ic >= 2 && !tc::mbar_wait(&P.accEmpty[a], ((ic >> 1) & 1u) ^ 1u, WAIT_LIMIT)) { err = 1; break; }
-                if (t % ntc == 0 && !tc::mbar_wait(P.fullW, (bW + t / ntc) & 1u, WAIT_LIMIT)) { err = 1; break; }
+                if (w_first(t) && !tc::mbar_wait(P.fullW, w_index(t) & 1u, WAIT_LIMIT)) { err = 1; break; }
                 if (!tc::mbar_wait(&P.fullB[ib % NBB], (ib / NBB) & 1u, WAIT_LIMIT)) { err = 1; break; }
                 tc::fence_after_sync();
                 issue_split_mma(tc::smem_u32(P.sW), tc::smem_u32(P.sB + (ib % NBB) * BTILE), PTN, P.tbase + a * (2 * PTN), true);
                 tc::mma_commit(&P.accFull[a]);
                 tc::mma_commit(&P.emptyB[ib % NBB]);
-                if (t % ntc == ntc - 1) tc::mma_commit(P.emptyW);
+                if (w_last(t)) tc::mma_commit(P.emptyW);
             }
         }
         __syncwarp();
@@ -523,7 +588,7 @@ __device__ inline bool trailing_pipe(Pipe &P, int N, int k0, int nbt, const CMat
             if (!tc::mbar_wait(&P.fullC[cb], (ic / NCB) & 1u, WAIT_LIMIT)) err = 1;
             if (__any_sync(0xffffffffu, err)) { err = 1; break; }
             tc::fence_after_sync();
-            const int it = t / ntc, jt = t % ntc, i = it * TM + r;
+            const int it = (t0 + t) / ntc, jt = (t0 + t) % ntc, i = it * TM + r;
             const bool rv = i < N;
             const int er = rv ? P.rexpW[i] : 0;
             float2 *cs = (float2 *)(P.sC + cb * CTILE);
@@ -559,7 +624,7 @@ __device__ inline bool trailing_pipe(Pipe &P, int N, int k0, int nbt, const CMat
         }
     }
     if (__syncthreads_or(err)) return false;
-    P.nW += ntr;
+    if (T > 0) P.nW += (uint32_t)((t1 - 1) / ntc - t0 / ntc + 1);
     P.nB += T;
     P.nT += T;
     return true;
@@ -576,24 +641,40 @@ __device__ inline bool trailing_pipe(Pipe &P, int N, int k0, int nbt, const CMat
 // Returns (on warp 0) the 1-based column of the first zero pivot, 0 if none;
 // *err = 1 if a tensor-core wait timed out.
 __device__ int gj_invert(float2 *__restrict__ A, int N, int ld, const GjSmem &s, Pipe &P, const CMat &cm,
-                         int *err) {
+                         int *err, Team &tm) {
     int info = 0;
+    const int ntr = (N + TM - 1) / TM;
+    const int2 rr = team_range(tm, ntr * TM, 8);  // this CTA's rows of the panel products
     for (int k0 = 0; k0 < N; k0 += KB) {
         const int nbt = min(KB, N - k0);
+        // every CTA of the team inverts the diagonal block (the same values)
         if (threadIdx.x < 32) {
             const int r = invert_diag_warp(A, ld, k0, nbt, s);
             if (r && !info) info = k0 + r;
         }
         __syncthreads();
-        panel_w(P, s, A, ld, N, k0, nbt);
+        panel_w(P, s, A, ld, N, k0, nbt, rr.x, rr.y, tm.n > 1 ? tm.gx : nullptr);
         if (nbt < N) {
-            convert_b(P, A, ld, N, k0, nbt);
-            if (!trailing_pipe(P, N, k0, nbt, cm)) {
+            const int nrest = N - nbt, ntc = (nrest + PTN - 1) / PTN;
+            const int2 cr = team_range(tm, ntc * PTN, 8);
+            int *gc = tm.n > 1 ? tm.gx + ntr * TM : nullptr;
+            convert_b(P, A, ld, N, k0, nbt, cr.x, cr.y, gc);
+            if (tm.n > 1) {
+                // the W and B tiles of both CTAs (read by bulk copies) and their exponents
+                asm volatile("fence.proxy.async;\n" ::: "memory");
+                cluster_sync();
+                for (int i = threadIdx.x; i < ntr * TM; i += NT) P.rexpW[i] = __ldcg(tm.gx + i);
+                for (int j = threadIdx.x; j < ntc * PTN; j += NT) P.cexpB[j] = __ldcg(gc + j);
+            }
+            const int2 tr = team_range(tm, ntr * ntc, 1);
+            const bool ok = trailing_pipe(P, N, k0, nbt, cm, tr.x, tr.y);
+            // every C tile of both CTAs stored before the next panel reads A
+            if (team_or(tm, !ok)) {
                 *err = 1;
                 return info;
             }
         } else {
-            __syncthreads();
+            team_sync(tm);
         }
     }
     return info;
@@ -677,7 +758,8 @@ __global__ void __launch_bounds__(NT, 1)
     int err = 0;
     float2 *A = work + (size_t)blockIdx.x * ld * N;
     const CMat cm{&tm, 0, (int)blockIdx.x};
-    const int inf = gj_invert(A, N, ld, s, P, cm, &err);
+    Team team{0, 1, nullptr, nullptr, 0};
+    const int inf = gj_invert(A, N, ld, s, P, cm, &err, team);
     if (!err) {
         float2 *o = out + (size_t)blockIdx.x * N * N;
         for (int j = 0; j < N; ++j)
@@ -710,7 +792,8 @@ struct MixedLayout {
     int N, Nz, ld, ntr, nkc, ncap;
     size_t mat_bytes;  // one matrix in split tiles
     size_t off_tiles, off_prow, off_rexp, off_x, off_rc, off_d, off_oc, job_bytes;
-    size_t scratch_bytes;  // per CTA
+    size_t off_gx;         // in a wave slot's scratch: the team's exponent exchange
+    size_t scratch_bytes;  // per wave slot (the CTAs of one job)
 };
 constexpr size_t TILE_BYTES = 4 * (size_t)TM * KB * 2;  // 32 KB
 inline size_t align256(size_t x) { return (x + 255) / 256 * 256; }
@@ -729,8 +812,11 @@ MixedLayout make_layout(int N, int Nz, int ld, int ncap) {
     L.off_d = o; o = align256(o + (size_t)2 * ncap * N * 8);
     L.off_oc = o; o = align256(o + (size_t)(ncap + 4) * 4);
     L.job_bytes = o;
-    // sweep: two working matrices; passes: the B operand of one product in split tiles
-    L.scratch_bytes = align256(std::max((size_t)2 * N * ld * 8 + pipe_scratch_bytes(N), (size_t)L.nkc * ncap * 256));
+    // sweep: two working matrices, the panel tiles and the exponents exchanged
+    // by a team; passes: the B operand of one product in split tiles
+    L.off_gx = align256((size_t)2 * N * ld * 8 + pipe_scratch_bytes(N));
+    const size_t gx_bytes = 4 * ((size_t)L.ntr * TM + (size_t)((N + PTN - 1) / PTN) * PTN);
+    L.scratch_bytes = align256(std::max(L.off_gx + gx_bytes, (size_t)L.nkc * ncap * 256));
     return L;
 }
 
@@ -741,6 +827,7 @@ struct MixedArgs {
     const double *E;       // energies
     const int2 *jobs;      // per wave slot: (energy index, k-point)
     int njobs;
+    int cpj;               // CTAs (one cluster) per job in the sweep: 1 or 2
     unsigned char *jobmem; // njobs job regions
     unsigned char *scratch;
     double *tau, *dnorm, *xnorm, *dprev;
@@ -800,17 +887,17 @@ __device__ inline negf::Smem carve_job(unsigned char *base, int N) {
 // M = round32(D_k - inv(prev)) in FP64: the off-diagonal part of D_k
 // (-c2 V(G_i - G_j), the same for every energy and k-point) streams from the
 // precomputed table, the diagonal is generated (negf::d_element,
-// grid.f90:236-333).  Thread t owns row t: coalesced loads of the table and of
+// grid.f90:236-333).  Rows [rlo, rhi); thread t owns row rlo + t: coalesced loads of the table and of
 // the previous inverse R, coalesced stores; four columns per pass keep eight
 // loads in flight per thread.
 __device__ inline void form_mixed(float2 *__restrict__ M, const negf::Geo &g, const negf::Smem &js,
                                   const double2 *__restrict__ voff, int k, double2 E, int ik,
-                                  const float2 *__restrict__ R) {
+                                  const float2 *__restrict__ R, int rlo, int rhi) {
     const int N = g.N, ld = g.ld;
     const double2 *vs = g.vhat + (size_t)g.W * g.H * k;
     const double2 *vk = voff + (size_t)N * ld * k;
     for (int j0 = 0; j0 < N; j0 += 4) {
-        for (int t = threadIdx.x; t < N; t += NT) {
+        for (int t = rlo + threadIdx.x; t < rhi; t += NT) {
             double2 d[4];
             float2 r[4];
 #pragma unroll
@@ -820,7 +907,7 @@ __device__ inline void form_mixed(float2 *__restrict__ M, const negf::Geo &g, co
                 r[q] = make_float2(0.f, 0.f);
                 if (j < N) {
                     d[q] = vk[t + (size_t)ld * j];
-                    if (R) r[q] = R[t + (size_t)ld * j];
+                    if (R) r[q] = ldcg2(R + t + (size_t)ld * j);
                 }
             }
 #pragma unroll
@@ -856,16 +943,17 @@ __global__ void __launch_bounds__(NT) k_voff(negf::Geo g, double2 *__restrict__ 
 // Stores the raw inverse R (working layout) as the split tiles of slot b,
 // with its pivot rows and row exponents.
 __device__ inline void store_factor(const float2 *__restrict__ R, const MixedLayout &L, const GjSmem &s,
-                                    int *rexpN, unsigned char *jm, int b) {
+                                    int *rexpN, unsigned char *jm, int b, const Team &tm) {
     const int N = L.N, ld = L.ld, tid = threadIdx.x;
     int *prow_g = (int *)(jm + L.off_prow) + (size_t)b * N;
     int *rexp_g = (int *)(jm + L.off_rexp) + (size_t)b * N;
     unsigned char *tiles = jm + L.off_tiles + (size_t)b * L.mat_bytes;
-    for (int t = tid; t < N; t += NT) {
+    const int2 rr = team_range(tm, N, 8);
+    for (int t = rr.x + tid; t < rr.y; t += NT) {
         float m = 0.0f;
 #pragma unroll 8
         for (int j = 0; j < N; ++j) {
-            const float2 v = R[t + (size_t)ld * j];
+            const float2 v = ldcg2(R + t + (size_t)ld * j);
             m = fmaxf(m, fmaxf(fabsf(v.x), fabsf(v.y)));
         }
         const int e = tc::scale_exponent(m);
@@ -873,35 +961,40 @@ __device__ inline void store_factor(const float2 *__restrict__ R, const MixedLay
         rexp_g[t] = e;
         prow_g[t] = s.prow[t];
     }
-    __syncthreads();
+    team_sync(tm);
+    if (tm.n > 1) {
+        for (int t = tid; t < N; t += NT) rexpN[t] = __ldcg(rexp_g + t);
+        __syncthreads();
+    }
+    // this CTA's tiles (row tile major)
+    const int2 ur = team_range(tm, L.ntr * L.nkc, 1);
     const int r = tid % TM, h = tid / TM;
-    for (int rt = 0; rt < L.ntr; ++rt) {
+    for (int u = ur.x; u < ur.y; ++u) {
+        const int rt = u / L.nkc, kc = u % L.nkc;
         const int row = rt * TM + r;
         const float sc = tc::exp2i(row < N ? -rexpN[row] : 0);
-        for (int kc = 0; kc < L.nkc; ++kc) {
-            unsigned char *tile = tiles + ((size_t)rt * L.nkc + kc) * TILE_BYTES;
+        unsigned char *tile = tiles + (size_t)u * TILE_BYTES;
 #pragma unroll
-            for (int g2 = 0; g2 < 2; ++g2) {
-                const int kg = 2 * h + g2;
-                float2 v[8];
+        for (int g2 = 0; g2 < 2; ++g2) {
+            const int kg = 2 * h + g2;
+            float2 v[8];
 #pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    const int col = kc * KB + 8 * kg + q;
-                    float2 x = (row < N && col < N) ? R[row + (size_t)ld * col] : make_float2(0.f, 0.f);
-                    v[q] = make_float2(x.x * sc, x.y * sc);
-                }
-                __align__(16) __half rh[8], rl[8], ih[8], il[8];
-#pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    const tc::Split2 a = tc::split_fp16(v[q].x), bb = tc::split_fp16(v[q].y);
-                    rh[q] = a.hi; rl[q] = a.lo; ih[q] = bb.hi; il[q] = bb.lo;
-                }
-                const uint32_t off = tc::kmajor_offset(r, 8 * kg, KB);
-                *(uint4 *)(tile + 0 * (TM * KB * 2) + off) = *(const uint4 *)rh;
-                *(uint4 *)(tile + 1 * (TM * KB * 2) + off) = *(const uint4 *)rl;
-                *(uint4 *)(tile + 2 * (TM * KB * 2) + off) = *(const uint4 *)ih;
-                *(uint4 *)(tile + 3 * (TM * KB * 2) + off) = *(const uint4 *)il;
+            for (int q = 0; q < 8; ++q) {
+                const int col = kc * KB + 8 * kg + q;
+                float2 x = (row < N && col < N) ? ldcg2(R + row + (size_t)ld * col) : make_float2(0.f, 0.f);
+                v[q] = make_float2(x.x * sc, x.y * sc);
             }
+            __align__(16) __half rh[8], rl[8], ih[8], il[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const tc::Split2 a = tc::split_fp16(v[q].x), bb = tc::split_fp16(v[q].y);
+                rh[q] = a.hi; rl[q] = a.lo; ih[q] = bb.hi; il[q] = bb.lo;
+            }
+            const uint32_t off = tc::kmajor_offset(r, 8 * kg, KB);
+            *(uint4 *)(tile + 0 * (TM * KB * 2) + off) = *(const uint4 *)rh;
+            *(uint4 *)(tile + 1 * (TM * KB * 2) + off) = *(const uint4 *)rl;
+            *(uint4 *)(tile + 2 * (TM * KB * 2) + off) = *(const uint4 *)ih;
+            *(uint4 *)(tile + 3 * (TM * KB * 2) + off) = *(const uint4 *)il;
         }
     }
     __syncthreads();
@@ -917,20 +1010,26 @@ __global__ void __launch_bounds__(NT, 1) k_mixed_sweep(MixedArgs a, const __grid
     const MixedLayout &L = a.L;
     const negf::Geo &g = a.g;
     const int N = L.N, Nz = L.Nz, ld = L.ld, tid = threadIdx.x;
+    // a.cpj CTAs (one cluster) per job; slot = the job's wave slot in the scratch
+    const int slot = blockIdx.x / a.cpj, nslot = gridDim.x / a.cpj;
     GjSmem s = carve_gj(smem, N);
     size_t off = gj_smem_bytes(N);
     unsigned char *pipe_smem = smem + off;
     off += (pipe_smem_bytes(N) + 127) / 128 * 128;
-    float2 *W0 = (float2 *)(a.scratch + (size_t)blockIdx.x * L.scratch_bytes);
+    unsigned char *jscr = a.scratch + (size_t)slot * L.scratch_bytes;
+    float2 *W0 = (float2 *)jscr;
     float2 *W1 = W0 + (size_t)N * ld;
     Pipe P = carve_pipe(pipe_smem, N, (unsigned char *)(W1 + (size_t)N * ld));
     negf::Smem js = carve_job_slim(smem + off, N, P.sC);
     off += job_smem_bytes_slim(N);
     int *rexpN = (int *)(smem + off);
+    off += (size_t)rup(N, 4) * 4;
+    Team tm{(int)(blockIdx.x % a.cpj), a.cpj, (int *)(jscr + L.off_gx), (int *)(smem + off), 0u};
     for (int i = tid; i < N; i += NT) { js.nx[i] = g.nx[i]; js.ny[i] = g.ny[i]; }
     gj_identity(s, N);
     pipe_setup(P);
-    for (int w = blockIdx.x; w < a.njobs; w += gridDim.x) {
+    const int2 fr = team_range(tm, N, 8);  // this CTA's rows of the formation and of x0
+    for (int w = slot; w < a.njobs; w += nslot) {
         const int2 jb = a.jobs[w];
         const double e = a.E[jb.x];
         const double2 E = make_double2(e, g.eta);
@@ -939,41 +1038,46 @@ __global__ void __launch_bounds__(NT, 1) k_mixed_sweep(MixedArgs a, const __grid
         __syncthreads();
         negf::open_cols(N, js, js.gR);
         __syncthreads();
-        const int nopen = *js.nrows;
+        const int nopen = *js.nrows;  // the same in every CTA of the team
         int *oc = (int *)(jm + L.off_oc);
         if (nopen > L.ncap) {
-            if (tid == 0) a.status[w] = -1;
+            if (tid == 0 && tm.rank == 0) a.status[w] = -1;
             __syncthreads();
             continue;
         }
-        for (int j = tid; j < nopen; j += NT) oc[j] = js.rows[j];
-        if (tid == 0) oc[L.ncap] = nopen;
+        if (tm.rank == 0) {
+            for (int j = tid; j < nopen; j += NT) oc[j] = js.rows[j];
+            if (tid == 0) oc[L.ncap] = nopen;
+        }
         float2 *cur = W0, *oth = W1;
         int zc = 0, info = 0, err = 0;
         for (int b = Nz - 1; b >= 0; --b) {
-            form_mixed(oth, g, js, a.voff, b, E, jb.y, b < Nz - 1 ? cur : nullptr);
-            __syncthreads();
+            form_mixed(oth, g, js, a.voff, b, E, jb.y, b < Nz - 1 ? cur : nullptr, fr.x, fr.y);
+            team_sync(tm);
             float2 *tt = cur; cur = oth; oth = tt;
             zc ^= 1;
-            const CMat cm{&tmC, zc, (int)blockIdx.x};
-            const int r = gj_invert(cur, N, ld, s, P, cm, &err);
+            const CMat cm{&tmC, zc, slot};
+            const int r = gj_invert(cur, N, ld, s, P, cm, &err, tm);
             if (r && !info) info = r;
-            if (err) break;  // uniform: set from __syncthreads_or
-            store_factor(cur, L, s, rexpN, jm, b);
+            if (err) break;  // uniform over the team (team_or)
+            store_factor(cur, L, s, rexpN, jm, b, tm);
         }
         if (!err) {
             float2 *x0 = (float2 *)(jm + L.off_x);  // slice 0
             for (int j = 0; j < L.ncap; ++j) {
-                const int jc = j < nopen ? s.iprow[oc[j]] : -1;
-                for (int r = tid; r < N; r += NT)
-                    x0[r + (size_t)N * j] = jc >= 0 ? cur[s.prow[r] + (size_t)ld * jc] : make_float2(0.f, 0.f);
+                const int jc = j < nopen ? s.iprow[js.rows[j]] : -1;
+                for (int r = fr.x + tid; r < fr.y; r += NT)
+                    x0[r + (size_t)N * j] = jc >= 0 ? ldcg2(cur + s.prow[r] + (size_t)ld * jc) : make_float2(0.f, 0.f);
             }
         }
-        if (tid == 0) a.status[w] = err ? -2 : info;
-        __syncthreads();
+        if (tid == 0 && tm.rank == 0) a.status[w] = err ? -2 : info;
+        // the next job's formation overwrites the working matrices that x0 read
+        team_sync(tm);
         if (err) break;
     }
     pipe_teardown(P);
+    // no CTA leaves while the other may still read its shared memory (team_or)
+    if (tm.n > 1) cluster_sync();
 }
 
 // ======================================================= refinement passes
@@ -1451,10 +1555,15 @@ __global__ void __launch_bounds__(NT, 1) k_mixed_pass(MixedArgs a, int mode, int
 }
 
 // FP64 residual of the block-tridiagonal system for x0, one CTA per (job,
-// slice b): r(b) = E_1 delta_b0 - x0(b-1) - D_b x0(b) - x0(b+1), D_b in FP64 (the
-// off-diagonal part from the -c2 V(G_i - G_j) table, the diagonal from
-// negf::d_element) and the product on the FP64 tensor cores (DMMA
-// warp tiles of negf::WarpAcc), 64 x 64 output tiles, K in chunks of 16.
+// slice b): r(b) = E_1 delta_b0 - x0(b-1) - D_b x0(b) - x0(b+1), D_b in FP64
+// and the product on the FP64 tensor cores (DMMA warp tiles of
+// negf::WarpAcc), 64 x 64 output tiles, K in chunks of 16, two stages: the
+// table chunk of the next stage streams in by cp.async and the next x0 chunk
+// (FP32) is loaded into registers while the current chunk is multiplied,
+// then widened to FP64 into the other stage.  The product uses the
+// -c2 V(G_i - G_j) table as it is, diagonal included; the epilogue replaces
+// its diagonal term by the generated one (negf::d_element):
+// D_b x = T_b x + (d_ii - T_b(i,i)) x_i.
 __global__ void __launch_bounds__(NT, 2) k_mixed_residual(MixedArgs a) {
     extern __shared__ __align__(128) unsigned char smem[];
     const MixedLayout &L = a.L;
@@ -1463,10 +1572,10 @@ __global__ void __launch_bounds__(NT, 2) k_mixed_residual(MixedArgs a) {
     // jobs fastest: the CTAs in flight share slice b's D table in L2
     const int w = blockIdx.x, b = blockIdx.y;
     if (a.status[w] != 0) return;
-    constexpr int KC = negf::KC, AP = negf::AP, BP = negf::BP;
-    double2 *sA = (double2 *)smem;           // [KC][AP]
-    double2 *sB = sA + KC * AP;              // [KC][BP]
-    negf::Smem js = carve_job(smem + (size_t)KC * (AP + BP) * 16, N);
+    constexpr int KC = negf::KC, AP = negf::AP, BP = negf::BP, CM = negf::CM, CN = negf::CN;
+    double2 *sA = (double2 *)smem;           // [2][KC][AP]
+    double2 *sB = sA + 2 * KC * AP;          // [2][KC][BP]
+    negf::Smem js = carve_job(smem + (size_t)2 * KC * (AP + BP) * 16, N);
     unsigned char *jm = a.jobmem + (size_t)w * L.job_bytes;
     const int *oc = (const int *)(jm + L.off_oc);
     const int nopen = oc[L.ncap];
@@ -1485,36 +1594,71 @@ __global__ void __launch_bounds__(NT, 2) k_mixed_residual(MixedArgs a) {
     const double2 *vs = g.vhat + (size_t)g.W * g.H * b;
     const double2 *vt = a.voff + (size_t)N * L.ld * b;
     const int wm0 = (warp >> 2) * negf::WM, wn0 = (warp & 3) * negf::WN;
-    for (int I0 = 0; I0 < N; I0 += negf::CM) {
-        for (int J0 = 0; J0 < npad; J0 += negf::CN) {
+    const int nkc = (N + KC - 1) / KC;
+    constexpr int BQ = (KC * CN) / NT;  // x0 values per thread per chunk
+    for (int J0 = 0; J0 < npad; J0 += CN) {
+        for (int I0 = 0; I0 < N; I0 += CM) {
             const bool active = (I0 + wm0 < N) && (J0 + wn0 < npad);
             negf::WarpAcc acc;
             acc.zero();
-            for (int k0 = 0; k0 < N; k0 += KC) {
-                for (int e2 = tid; e2 < KC * negf::CM; e2 += NT) {
-                    const int kk = e2 / negf::CM, ii = e2 % negf::CM, i = I0 + ii, k = k0 + kk;
-                    // off-diagonal D_b from the table (coalesced in i), the diagonal generated
-                    sA[kk * AP + ii] = (i < N && k < N)
-                                           ? (i == k ? negf::d_element(g, js, vs, b, E, jb.y, i, k, js.nx[k], js.ny[k])
-                                                     : vt[i + (size_t)L.ld * k])
-                                           : make_double2(0.0, 0.0);
-                }
-                for (int e2 = tid; e2 < KC * negf::CN; e2 += NT) {
-                    const int jj = e2 / KC, kk = e2 % KC, j = J0 + jj, k = k0 + kk;
-                    float2 v = (j < nopen && k < N) ? xb[k + (size_t)N * j] : make_float2(0.f, 0.f);
-                    sB[kk * BP + jj] = make_double2(v.x, v.y);
-                }
-                __syncthreads();
-                if (active) {
+            float2 xr[BQ];
+            auto load_a = [&](int st, int k0) {
+                double2 *dA = sA + st * KC * AP;
 #pragma unroll
-                    for (int kb = 0; kb < KC; kb += 4) acc.step(sA, AP, wm0, sB, BP, wn0, kb, lane);
+                for (int q = 0; q < (KC * CM) / NT; ++q) {
+                    const int e2 = tid + NT * q, kk = e2 / CM, ii = e2 % CM, k = k0 + kk, i = I0 + ii;
+                    const bool v = k < N && i < N;
+                    negf::cp_async16(dA + kk * AP + ii, vt + (v ? (i + (size_t)L.ld * k) : 0), v);
                 }
+                negf::cp_async_commit();
+            };
+            auto load_x = [&](int k0) {
+#pragma unroll
+                for (int q = 0; q < BQ; ++q) {
+                    const int e2 = tid + NT * q, jj = e2 / KC, kk = e2 % KC, j = J0 + jj, k = k0 + kk;
+                    xr[q] = (j < nopen && k < N) ? xb[k + (size_t)N * j] : make_float2(0.f, 0.f);
+                }
+            };
+            auto store_x = [&](int st) {
+                double2 *dB = sB + st * KC * BP;
+#pragma unroll
+                for (int q = 0; q < BQ; ++q) {
+                    const int e2 = tid + NT * q, jj = e2 / KC, kk = e2 % KC;
+                    dB[kk * BP + jj] = make_double2(xr[q].x, xr[q].y);
+                }
+            };
+            load_a(0, 0);
+            load_x(0);
+            store_x(0);
+            for (int c = 0; c < nkc; ++c) {
+                negf::cp_async_wait<0>();
+                // chunk c is in stage c & 1, and every warp has finished chunk c - 1,
+                // so stage (c + 1) & 1 may be refilled
                 __syncthreads();
+                if (c + 1 < nkc) {
+                    load_a((c + 1) & 1, (c + 1) * KC);
+                    load_x((c + 1) * KC);
+                }
+                if (active) {
+                    const double2 *cA = sA + (c & 1) * KC * AP;
+                    const double2 *cB = sB + (c & 1) * KC * BP;
+#pragma unroll
+                    for (int kb = 0; kb < KC; kb += 4) acc.step(cA, AP, wm0, cB, BP, wn0, kb, lane);
+                }
+                if (c + 1 < nkc) store_x((c + 1) & 1);
             }
+            // every warp is done with both stages before the next tile refills them
+            __syncthreads();
             if (active) {
 #pragma unroll
                 for (int m = 0; m < 4; ++m) {
                     const int i = I0 + wm0 + 8 * m + (lane >> 2);
+                    double2 dfix = make_double2(0.0, 0.0);
+                    if (i < N) {
+                        const double2 dii = negf::d_element(g, js, vs, b, E, jb.y, i, i, js.nx[i], js.ny[i]);
+                        const double2 tii = vt[i + (size_t)L.ld * i];
+                        dfix = make_double2(dii.x - tii.x, dii.y - tii.y);
+                    }
 #pragma unroll
                     for (int n = 0; n < 2; ++n)
 #pragma unroll
@@ -1523,8 +1667,11 @@ __global__ void __launch_bounds__(NT, 2) k_mixed_residual(MixedArgs a) {
                             if (i < N && j < L.ncap) {
                                 double rx = 0.0, ry = 0.0;
                                 if (j < nopen) {
-                                    rx = -acc.re[m][n][e3];
-                                    ry = -acc.im[m][n][e3];
+                                    const float2 xi = xb[i + (size_t)N * j];
+                                    const double ax = acc.re[m][n][e3] + (dfix.x * xi.x - dfix.y * xi.y);
+                                    const double ay = acc.im[m][n][e3] + (dfix.x * xi.y + dfix.y * xi.x);
+                                    rx = -ax;
+                                    ry = -ay;
                                     if (b > 0) { const float2 v = x[(b - 1) * sl + i + (size_t)N * j]; rx -= v.x; ry -= v.y; }
                                     if (b + 1 < Nz) { const float2 v = x[(b + 1) * sl + i + (size_t)N * j]; rx -= v.x; ry -= v.y; }
                                     if (b == 0 && i == oc[j]) rx += 1.0;
@@ -1739,7 +1886,33 @@ int negf_internal_mixed(negf_ctx *c, const double *h_E, const double *d_E, int n
         const size_t fp64_ws = (size_t)c->num_sms * 4 * c->ld * N * 16;
         const size_t avail = free_b + c->mixed_bytes;
         const size_t budget = avail > fp64_ws + ((size_t)4 << 30) ? (size_t)(0.92 * (avail - fp64_ws)) - ((size_t)2 << 30) : 0;
-        int W = (int)std::min<size_t>({(size_t)m_jobs.size(), (size_t)c->num_sms, budget / (per_job + small_per_job)});
+        const size_t mem_jobs = budget / (per_job + small_per_job);
+        int W = (int)std::min<size_t>({(size_t)m_jobs.size(), (size_t)c->num_sms, mem_jobs});
+        // Two CTAs (one cluster) per job when a wave of single-CTA jobs would
+        // leave at least half of the SMs idle (few jobs, or factor storage
+        // bounding the wave): the job then sweeps on two SMs.
+        int cpj = pol.ctas_per_job;
+        if (cpj == 0) cpj = (2 * (size_t)W <= (size_t)c->num_sms) ? 2 : 1;
+        const size_t sm_sweep = gj_smem_bytes(N) + (pipe_smem_bytes(N) + 127) / 128 * 128 +
+                                job_smem_bytes_slim(N) + (size_t)rup(N, 4) * 4 + 16;
+        if (cpj == 2 && W >= 1) {
+            CKM(cudaFuncSetAttribute(k_mixed_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_sweep));
+            cudaLaunchConfig_t qc = {};
+            cudaLaunchAttribute qa[1];
+            qa[0].id = cudaLaunchAttributeClusterDimension;
+            qa[0].val.clusterDim.x = 2;
+            qa[0].val.clusterDim.y = 1;
+            qa[0].val.clusterDim.z = 1;
+            qc.gridDim = dim3(2 * W);
+            qc.blockDim = dim3(NT);
+            qc.dynamicSmemBytes = sm_sweep;
+            qc.attrs = qa;
+            qc.numAttrs = 1;
+            int nclu = 0;
+            CKM(cudaOccupancyMaxActiveClusters(&nclu, k_mixed_sweep, &qc));
+            if (nclu < 1) cpj = 1;
+            else W = std::min(W, nclu);
+        }
         if (W < 1) {
             // not enough device memory for one job: everything in FP64
             for (int q : m_jobs) { f_ie.push_back(q % nE); f_ik.push_back(q / nE); }
@@ -1755,6 +1928,7 @@ int negf_internal_mixed(negf_ctx *c, const double *h_E, const double *d_E, int n
                 c->mixed_bytes = need;
             }
             stats.jobs_per_wave = W;
+            stats.ctas_per_job = cpj;
             unsigned char *base = (unsigned char *)c->d_mixed;
             MixedArgs a;
             a.g = mixed_geo(c);
@@ -1772,10 +1946,9 @@ int negf_internal_mixed(negf_ctx *c, const double *h_E, const double *d_E, int n
             a.dprev = a.xnorm + W;
             a.status = (int *)(a.dprev + W);
             a.tol = pol.tau_tolerance;
-            const size_t sm_sweep = gj_smem_bytes(N) + (pipe_smem_bytes(N) + 127) / 128 * 128 +
-                                    job_smem_bytes_slim(N) + (size_t)rup(N, 4) * 4;
+            a.cpj = cpj;
             const size_t sm_pass = pass_smem_bytes(N, ncap);
-            const size_t sm_res = (size_t)negf::KC * (negf::AP + negf::BP) * 16 + job_smem_bytes(N);
+            const size_t sm_res = (size_t)2 * negf::KC * (negf::AP + negf::BP) * 16 + job_smem_bytes(N);
             rc = set_smem(k_mixed_sweep, sm_sweep);
             if (!rc) rc = set_smem(k_mixed_pass, sm_pass);
             if (!rc) rc = set_smem(k_mixed_residual, sm_res);
@@ -1792,8 +1965,21 @@ int negf_internal_mixed(negf_ctx *c, const double *h_E, const double *d_E, int n
                 a.njobs = nw;
                 CKM(cudaMemcpyAsync(d_jobs, wj.data(), sizeof(int2) * nw, cudaMemcpyHostToDevice, st));
                 CKM(cudaEventRecord(c->ev0, st));
-                k_mixed_sweep<<<nw, NT, sm_sweep, st>>>(a, tmC);
-                CKM(cudaGetLastError());
+                {
+                    cudaLaunchConfig_t lc = {};
+                    cudaLaunchAttribute la[1];
+                    la[0].id = cudaLaunchAttributeClusterDimension;
+                    la[0].val.clusterDim.x = cpj;
+                    la[0].val.clusterDim.y = 1;
+                    la[0].val.clusterDim.z = 1;
+                    lc.gridDim = dim3(nw * cpj);
+                    lc.blockDim = dim3(NT);
+                    lc.dynamicSmemBytes = sm_sweep;
+                    lc.stream = st;
+                    lc.attrs = la;
+                    lc.numAttrs = 1;
+                    CKM(cudaLaunchKernelEx(&lc, k_mixed_sweep, a, tmC));
+                }
                 k_mixed_pass<<<nw, NT, sm_pass, st>>>(a, PASS_X0, 0, 0);
                 CKM(cudaGetLastError());
                 // refinement steps; converged jobs (MIX_DONE) are skipped by the next ones

@@ -93,11 +93,12 @@ class Engine:
         return tau, rc
 
     def set_mixed_policy(self, threshold_window=None, eta_fp64_below=None, tau_tolerance=None,
-                         max_refinements=None):
+                         max_refinements=None, ctas_per_job=None):
         """Policy of the NEGF_MIXED path (Hartree): energies within threshold_window of a
         lead subband threshold run in FP64; eta below eta_fp64_below sends every job to
         FP64; a refined job is accepted when its estimated remaining |dtau| is below
         tau_tolerance after at most max_refinements steps (else it is re-run in FP64).
+        ctas_per_job: 1 or 2 CTAs sweep one job (0 = automatic).
         Unset arguments keep their current values."""
         p = MixedPolicy()
         check("negf_get_mixed_policy", lib().negf_get_mixed_policy(self._ctx, C.byref(p)))
@@ -109,13 +110,15 @@ class Engine:
             p.tau_tolerance = float(tau_tolerance)
         if max_refinements is not None:
             p.max_refinements = int(max_refinements)
+        if ctas_per_job is not None:
+            p.ctas_per_job = int(ctas_per_job)
         check("negf_set_mixed_policy", lib().negf_set_mixed_policy(self._ctx, C.byref(p)))
 
     def mixed_policy(self):
         """The current NEGF_MIXED policy (dict)."""
         p = MixedPolicy()
         check("negf_get_mixed_policy", lib().negf_get_mixed_policy(self._ctx, C.byref(p)))
-        return {k: getattr(p, k) for k, _ in p._fields_ if k != "pad"}
+        return {k: getattr(p, k) for k, _ in p._fields_}
 
     def mixed_stats(self):
         """Counts and device times of the last NEGF_MIXED call (dict)."""

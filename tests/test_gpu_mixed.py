@@ -168,3 +168,28 @@ def test_mixed_policy_routes_jobs_to_fp64():
     near = sum(bool(np.any(np.abs(e - th) < 1e-3 * 0.067 / 27.211386245988)) for e in E)
     assert st["n_fp64_policy"] == near
     assert np.max(np.abs(tm - t64)) <= TOL_MIXED
+
+
+@pytest.mark.parametrize("name,nz,ne", [("qpc_n69", 40, 24), ("qpc_disorder_n221", 48, 12), ("qpc_disorder_n797", 12, 4)])
+def test_mixed_one_and_two_ctas_per_job(name, nz, ne):
+    """The sweep on one CTA per job and on a two-CTA cluster per job (rows,
+    panel products and trailing tiles split between two SMs) both meet the
+    bar against the oracle, and the call reports which one ran."""
+    from negftrans_b200 import prepare as P
+    from negftrans_b200._lib import NEGF_MIXED
+    from negftrans_b200.negf import Engine
+    w, pr = _prepared(name, nz=nz)
+    grid = P.transmission_energies(pr.atomic, w.n_energy)
+    E = np.ascontiguousarray(grid[:: max(1, len(grid) // ne)][:ne])
+    ref = _oracle(pr, E)
+    out = {}
+    with Engine(*pr.engine_args()) as eng:
+        for cpj in (1, 2):
+            eng.set_mixed_policy(ctas_per_job=cpj)
+            tau, info = eng.transmission(E, precision=NEGF_MIXED)
+            st = eng.mixed_stats()
+            assert info == 0
+            assert st["ctas_per_job"] == cpj, st
+            assert np.max(np.abs(tau - ref)) <= TOL_MIXED, (cpj, np.abs(tau - ref), st)
+            out[cpj] = tau
+    assert np.max(np.abs(out[1] - out[2])) <= TOL_MIXED
