@@ -236,14 +236,15 @@ __device__ inline void stage_w(const TileSmem &t, const GjSmem &s, const float2 
 // N..ld-1 are never touched).
 constexpr int PTN = 32;                         // columns of an output tile
 constexpr int NCB = 3;                          // C buffers
-constexpr int NBB = 3;                          // B buffers
+constexpr int NBB = 2;                          // B buffers
+constexpr int NKB = 2;                          // K chunks of KB in one update at most (rank 64)
 constexpr uint32_t WTILE = 4u * TM * KB * 2;     // 32 KB
 constexpr uint32_t BTILE = 4u * PTN * KB * 2;    // 8 KB
 constexpr uint32_t CTILE = (uint32_t)TM * PTN * 8;  // 32 KB: PTN columns of TM float2
 static_assert(NCB * CTILE >= 32u * NT * 8, "panel_w stages 32 values per thread in the C buffers");
 struct Pipe {
-    unsigned char *sW;
-    unsigned char *sB;               // NBB buffers of BTILE bytes (no arrays of pointers, so the
+    unsigned char *sW;               // NKB chunks of WTILE bytes: the W tile of one row tile
+    unsigned char *sB;               // NBB buffers of NKB * BTILE bytes (no arrays of pointers, so the
     unsigned char *sC;               // struct stays in registers): NCB buffers of CTILE bytes
     uint64_t *fullW, *emptyW;        // [1], [1]
     uint64_t *fullB, *emptyB;        // [NBB]
@@ -253,28 +254,29 @@ struct Pipe {
     int *rexpW;                      // [ntr * TM] row exponents of W
     int *cexpB;                      // [ntc * PTN] column exponents of the pivot rows
     uint32_t *tslot;
-    unsigned char *wt, *bt;          // global: W tiles, B tiles
+    unsigned char *wt, *bt;          // global: W tiles (NKB * WTILE per row tile), B tiles (NKB * BTILE
+                                     // per column tile; an update of one K chunk uses the first)
     uint32_t tbase;
     uint32_t nW, nB, nT;             // W tiles, B tiles and output tiles so far (phase counters)
 };
 constexpr int PIPE_BARS = 2 + 2 * NBB + 2 * NCB + 4 + 1;
 __host__ __device__ inline size_t pipe_smem_bytes(int N) {
     const int ntr = (N + TM - 1) / TM, ntc = (N + PTN - 1) / PTN;
-    return (size_t)WTILE + NBB * (size_t)BTILE + NCB * (size_t)CTILE + PIPE_BARS * 8 + 8 + 4 * (size_t)ntr * TM +
+    return (size_t)NKB * WTILE + NBB * (size_t)NKB * BTILE + NCB * (size_t)CTILE + PIPE_BARS * 8 + 8 + 4 * (size_t)ntr * TM +
            4 * (size_t)ntc * PTN + 16;
 }
 // global scratch of one CTA for the panel tiles
 __host__ __device__ inline size_t pipe_scratch_bytes(int N) {
     const int ntr = (N + TM - 1) / TM, ntc = (N + PTN - 1) / PTN;
-    return (size_t)ntr * WTILE + (size_t)ntc * BTILE;
+    return (size_t)ntr * NKB * WTILE + (size_t)ntc * NKB * BTILE;
 }
 __device__ inline Pipe carve_pipe(unsigned char *base, int N, unsigned char *gscratch) {
     Pipe P;
     const int ntr = (N + TM - 1) / TM, ntc = (N + PTN - 1) / PTN;
     unsigned char *q = base;
-    P.sW = q; q += WTILE;
+    P.sW = q; q += NKB * WTILE;
     P.sC = q; q += NCB * CTILE;
-    P.sB = q; q += NBB * BTILE;
+    P.sB = q; q += NBB * NKB * BTILE;
     uint64_t *bar = (uint64_t *)q;
     P.fullW = bar; P.emptyW = bar + 1;
     P.fullB = bar + 2; P.emptyB = P.fullB + NBB;
@@ -286,7 +288,7 @@ __device__ inline Pipe carve_pipe(unsigned char *base, int N, unsigned char *gsc
     P.cexpB = (int *)q; q += 4 * (size_t)ntc * PTN;
     P.tslot = (uint32_t *)q;
     P.wt = gscratch;
-    P.bt = gscratch + (size_t)ntr * WTILE;
+    P.bt = gscratch + (size_t)ntr * NKB * WTILE;
     P.nW = P.nB = P.nT = 0;
     return P;
 }
@@ -443,7 +445,7 @@ __device__ inline void panel_w(const Pipe &P, const GjSmem &s, float2 *__restric
         const float sc = tc::exp2i(-e);
         P.rexpW[row] = e;
         if (gexp) gexp[row] = e;
-        unsigned char *tile = P.wt + (size_t)(row / TM) * WTILE;
+        unsigned char *tile = P.wt + (size_t)(row / TM) * NKB * WTILE;
 #pragma unroll
         for (int g = 0; g < 4; ++g) {
             __align__(16) __half rh[8], rl[8], ih[8], il[8];
@@ -460,57 +462,141 @@ __device__ inline void panel_w(const Pipe &P, const GjSmem &s, float2 *__restric
         }
     }
 }
-// B tiles: rest column jr (the columns outside the panel, in order) with the
-// K values A(k0 + kk, col(jr)) of the panel's rows; four threads per column.
-// Rest columns [clo, chi) (multiples of 8); with gexp the column exponents
-// also go to global memory for the other CTA of the team.
-__device__ inline void convert_b(const Pipe &P, const float2 *__restrict__ A, int ld, int N, int k0, int nbt,
-                                 int clo, int chi, int *gexp) {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane & 3;
-    const int nrest = N - nbt;
-    for (int c0 = clo + warp * 8; c0 < chi; c0 += NWARP * 8) {
-        const int jr = c0 + (lane >> 2);
-        const bool cv = jr < nrest;
-        const int col = jr < k0 ? jr : jr + nbt;
-        float2 v[8];
-        float m = 0.0f;
+// W of a 64-column panel [k0, k0+64) whose columns already hold their final
+// Gauss-Jordan values: W = A(:, K) - E_K (the identity on the panel's rows),
+// so that A(:, J) += W A_old(K, J) eliminates the whole panel from every other
+// column J.  Two K chunks per row tile, one exponent per row over all 64
+// values.  Rows [rlo, rhi) of the ntr * TM tile rows (rows N.. are zero);
+// with gexp the row exponents also go to global memory.
+__device__ __noinline__ void panel_w64(const Pipe &P, const float2 *__restrict__ A, int ld, int N, int k0, int rlo,
+                                 int rhi, int *gexp) {
+    for (int row = rlo + threadIdx.x; row < rhi; row += NT) {
+        const int rk = row - k0;
+        auto ld8 = [&](int c0, float2 (&v)[8]) {
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const int kk = 8 * g + q;
-            v[q] = (cv && kk < nbt) ? ldcg2(A + k0 + kk + (size_t)ld * col) : make_float2(0.f, 0.f);
-            m = fmaxf(m, fmaxf(fabsf(v[q].x), fabsf(v[q].y)));
+            for (int q = 0; q < 8; ++q) {
+                float2 x = row < N ? ldcg2(A + row + (size_t)ld * (k0 + c0 + q)) : make_float2(0.f, 0.f);
+                if (c0 + q == rk) x.x -= 1.0f;
+                v[q] = x;
+            }
+        };
+        // the row maximum first (16 loads in flight), then the values again, eight at a time
+        float mx = 0.0f;
+#pragma unroll 1
+        for (int c0 = 0; c0 < 64; c0 += 16) {
+            float2 a[8], b[8];
+            ld8(c0, a);
+            ld8(c0 + 8, b);
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                mx = fmaxf(mx, fmaxf(fmaxf(fabsf(a[q].x), fabsf(a[q].y)), fmaxf(fabsf(b[q].x), fabsf(b[q].y))));
         }
-        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 1));
-        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 2));
-        const int e = tc::scale_exponent(m);
+        const int e = tc::scale_exponent(mx);
         const float sc = tc::exp2i(-e);
-        if (g == 0) {
-            P.cexpB[jr] = e;
-            if (gexp) gexp[jr] = e;
-        }
-        __align__(16) __half rh[8], rl[8], ih[8], il[8];
+        P.rexpW[row] = e;
+        if (gexp) gexp[row] = e;
+        unsigned char *tile = P.wt + (size_t)(row / TM) * NKB * WTILE;
+#pragma unroll 1
+        for (int g = 0; g < 8; ++g) {
+            float2 w[8];
+            ld8(8 * g, w);
+            __align__(16) __half rh[8], rl[8], ih[8], il[8];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const tc::Split2 a = tc::split_fp16(v[q].x * sc), b = tc::split_fp16(v[q].y * sc);
-            rh[q] = a.hi; rl[q] = a.lo; ih[q] = b.hi; il[q] = b.lo;
+            for (int q = 0; q < 8; ++q) {
+                const tc::Split2 u = tc::split_fp16(w[q].x * sc), v = tc::split_fp16(w[q].y * sc);
+                rh[q] = u.hi; rl[q] = u.lo; ih[q] = v.hi; il[q] = v.lo;
+            }
+            unsigned char *t = tile + (size_t)(g / 4) * WTILE;
+            const uint32_t off = tc::kmajor_offset(row % TM, 8 * (g % 4), KB);
+            *(uint4 *)(t + 0 * (TM * KB * 2) + off) = *(const uint4 *)rh;
+            *(uint4 *)(t + 1 * (TM * KB * 2) + off) = *(const uint4 *)rl;
+            *(uint4 *)(t + 2 * (TM * KB * 2) + off) = *(const uint4 *)ih;
+            *(uint4 *)(t + 3 * (TM * KB * 2) + off) = *(const uint4 *)il;
         }
-        unsigned char *tile = P.bt + (size_t)(jr / PTN) * BTILE;
-        const uint32_t off = tc::kmajor_offset(jr % PTN, 8 * g, KB);
-        *(uint4 *)(tile + 0 * (PTN * KB * 2) + off) = *(const uint4 *)rh;
-        *(uint4 *)(tile + 1 * (PTN * KB * 2) + off) = *(const uint4 *)rl;
-        *(uint4 *)(tile + 2 * (PTN * KB * 2) + off) = *(const uint4 *)ih;
-        *(uint4 *)(tile + 3 * (PTN * KB * 2) + off) = *(const uint4 *)il;
     }
 }
 
-// A(:, rest) += W * B for the panel [k0, k0+nbt) (W and B tiles already in
-// the CTA's global scratch), pipelined (see above); the C tiles of matrix cm
-// move by TMA.  Output tiles [t0, t1) of the ntr x ntc tiles (row tile major),
-// so that the CTAs of a team share the update.  Returns false if a wait timed
-// out (uniform over the CTA).
-__device__ inline bool trailing_pipe(Pipe &P, int N, int k0, int nbt, const CMat &cm, int t0, int t1) {
+// Which matrix columns the B tiles and output tiles of an update cover:
+// either the rest columns of a panel (column tile jt holds rest columns jr =
+// jt*PTN.., matrix column jr < skip0 ? jr : jr + nskip) or one column tile at
+// cfix (cfix >= 0).  nrest = valid rest columns.
+struct ColMap {
+    int skip0, nskip, cfix, nrest;
+    __device__ __forceinline__ int col(int jr) const { return cfix >= 0 ? cfix + jr : (jr < skip0 ? jr : jr + nskip); }
+    __device__ __forceinline__ int ntc() const { return (nrest + PTN - 1) / PTN; }
+};
+
+// B tiles: rest column jr with the K values A(krow0 + kk, col(jr)), kk <
+// nkr <= 32 * NKBT (the rows of the panel, old values), one exponent per
+// column over all of them; four threads per column.  Rest columns [clo, chi)
+// (multiples of 8); with gexp the column exponents also go to global memory
+// for the other CTA of the team.  A single K chunk takes two groups of eight
+// columns per warp and round (sixteen loads in flight).
+// (not inlined: a separate register allocation keeps the sweep kernel's spills low)
+template <int NKBT>
+__device__ __noinline__ void convert_b(const Pipe &P, const float2 *__restrict__ A, int ld, int krow0, int nkr,
+                                 const ColMap &cmap, int clo, int chi, int *gexp) {
+    constexpr int GR = NKBT == 1 ? 2 : 1;  // column groups per warp and round
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane & 3;
+    for (int c00 = clo + warp * 8; c00 < chi; c00 += GR * NWARP * 8) {
+        float2 v[GR][8 * NKBT];
+#pragma unroll
+        for (int h = 0; h < GR; ++h) {
+            const int jr = c00 + h * NWARP * 8 + (lane >> 2);
+            const bool cv = jr < cmap.nrest && jr < chi;
+            const int col = cmap.col(jr);
+#pragma unroll
+            for (int c = 0; c < NKBT; ++c)
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const int kk = 32 * c + 8 * g + q;
+                    v[h][8 * c + q] = (cv && kk < nkr) ? ldcg2(A + krow0 + kk + (size_t)ld * col) : make_float2(0.f, 0.f);
+                }
+        }
+#pragma unroll
+        for (int h = 0; h < GR; ++h) {
+            const int c0 = c00 + h * NWARP * 8;
+            if (c0 >= chi) break;  // uniform over the warp
+            const int jr = c0 + (lane >> 2);
+            float m = 0.0f;
+#pragma unroll
+            for (int q = 0; q < 8 * NKBT; ++q) m = fmaxf(m, fmaxf(fabsf(v[h][q].x), fabsf(v[h][q].y)));
+            m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 1));
+            m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 2));
+            const int e = tc::scale_exponent(m);
+            const float sc = tc::exp2i(-e);
+            if (g == 0) {
+                P.cexpB[jr] = e;
+                if (gexp) gexp[jr] = e;
+            }
+#pragma unroll
+            for (int c = 0; c < NKBT; ++c) {
+                __align__(16) __half rh[8], rl[8], ih[8], il[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const tc::Split2 a = tc::split_fp16(v[h][8 * c + q].x * sc), b = tc::split_fp16(v[h][8 * c + q].y * sc);
+                    rh[q] = a.hi; rl[q] = a.lo; ih[q] = b.hi; il[q] = b.lo;
+                }
+                unsigned char *tile = P.bt + (size_t)(jr / PTN) * NKB * BTILE + (size_t)c * BTILE;
+                const uint32_t off = tc::kmajor_offset(jr % PTN, 8 * g, KB);
+                *(uint4 *)(tile + 0 * (PTN * KB * 2) + off) = *(const uint4 *)rh;
+                *(uint4 *)(tile + 1 * (PTN * KB * 2) + off) = *(const uint4 *)rl;
+                *(uint4 *)(tile + 2 * (PTN * KB * 2) + off) = *(const uint4 *)ih;
+                *(uint4 *)(tile + 3 * (PTN * KB * 2) + off) = *(const uint4 *)il;
+            }
+        }
+    }
+}
+
+// A(:, cols) += W * B (N rows) with nkb K chunks (W and B tiles already in the CTA's
+// global scratch), pipelined (see above); the C tiles of matrix cm move by
+// TMA, the columns as cmap says.  Output tiles [t0, t1) of the ntr x ntc
+// tiles (row tile major), so that the CTAs of a team share the update.
+// Returns false if a wait timed out (uniform over the CTA).
+__device__ inline bool trailing_pipe(Pipe &P, int N, const CMat &cm, const ColMap &cmap, int nkb, int t0, int t1) {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int nrest = N - nbt, ntc = (nrest + PTN - 1) / PTN, T = t1 - t0;
+    const int nrest = cmap.nrest, ntc = cmap.ntc(), T = t1 - t0;
+    const uint32_t wbytes = (uint32_t)nkb * WTILE, bbytes = (uint32_t)nkb * BTILE;
     // generic stores (W/B tiles in global, the staging in the C buffers) before
     // the bulk copies and TMA tiles that read or overwrite them
     asm volatile("fence.proxy.async;\n" ::: "memory");
@@ -518,11 +604,8 @@ __device__ inline bool trailing_pipe(Pipe &P, int N, int k0, int nbt, const CMat
     const uint32_t bW = P.nW, bB = P.nB, bT = P.nT;
     int err = 0;
     // first matrix column of tile t: the rest columns of a tile are contiguous
-    // (k0 and the tile width are multiples of 32)
-    auto tile_col0 = [&](int t) -> int {
-        const int jr = (t % ntc) * PTN;
-        return jr < k0 ? jr : jr + nbt;
-    };
+    // (the panel start and width are multiples of 32)
+    auto tile_col0 = [&](int t) -> int { return cmap.col((t % ntc) * PTN); };
     // the W tile changes at the first local tile and at every row-tile start
     auto w_first = [&](int v) -> bool { return v == 0 || (t0 + v) % ntc == 0; };
     auto w_last = [&](int v) -> bool { return v == T - 1 || (t0 + v) % ntc == ntc - 1; };
@@ -535,14 +618,15 @@ __device__ inline bool trailing_pipe(Pipe &P, int N, int k0, int nbt, const CMat
                 if (w_first(u)) {
                     const uint32_t iw = w_index(u);
                     if (iw >= 1 && !tc::mbar_wait(P.emptyW, (iw - 1) & 1u, WAIT_LIMIT)) return false;
-                    expect_bytes(P.fullW, WTILE);
-                    bulk_copy(P.sW, P.wt + (size_t)(t / ntc) * WTILE, WTILE, P.fullW);
+                    expect_bytes(P.fullW, wbytes);
+                    bulk_copy(P.sW, P.wt + (size_t)(t / ntc) * NKB * WTILE, wbytes, P.fullW);
                 }
                 const uint32_t ib = bB + u, ic = bT + u;
                 if (ib >= NBB && !tc::mbar_wait(&P.emptyB[ib % NBB], ((ib - NBB) / NBB) & 1u, WAIT_LIMIT))
                     return false;
-                expect_bytes(&P.fullB[ib % NBB], BTILE);
-                bulk_copy(P.sB + (ib % NBB) * BTILE, P.bt + (size_t)(t % ntc) * BTILE, BTILE, &P.fullB[ib % NBB]);
+                expect_bytes(&P.fullB[ib % NBB], bbytes);
+                bulk_copy(P.sB + (ib % NBB) * NKB * BTILE, P.bt + (size_t)(t % ntc) * NKB * BTILE, bbytes,
+                          &P.fullB[ib % NBB]);
                 // the C buffer last held tile u - NCB, whose store this thread issued
                 bulk_wait_read0();
                 expect_bytes(&P.fullC[ic % NCB], CTILE);  // the whole box, out-of-range elements zero-filled
@@ -571,7 +655,9 @@ __device__ inline bool trailing_pipe(Pipe &P, int N, int k0, int nbt, const CMat
                 if (w_first(t) && !tc::mbar_wait(P.fullW, w_index(t) & 1u, WAIT_LIMIT)) { err = 1; break; }
                 if (!tc::mbar_wait(&P.fullB[ib % NBB], (ib / NBB) & 1u, WAIT_LIMIT)) { err = 1; break; }
                 tc::fence_after_sync();
-                issue_split_mma(tc::smem_u32(P.sW), tc::smem_u32(P.sB + (ib % NBB) * BTILE), PTN, P.tbase + a * (2 * PTN), true);
+                for (int c = 0; c < nkb; ++c)
+                    issue_split_mma(tc::smem_u32(P.sW + c * WTILE), tc::smem_u32(P.sB + (ib % NBB) * NKB * BTILE + c * BTILE),
+                                    PTN, P.tbase + a * (2 * PTN), c == 0);
                 tc::mma_commit(&P.accFull[a]);
                 tc::mma_commit(&P.emptyB[ib % NBB]);
                 if (w_last(t)) tc::mma_commit(P.emptyW);
@@ -645,36 +731,66 @@ __device__ int gj_invert(float2 *__restrict__ A, int N, int ld, const GjSmem &s,
     int info = 0;
     const int ntr = (N + TM - 1) / TM;
     const int2 rr = team_range(tm, ntr * TM, 8);  // this CTA's rows of the panel products
-    for (int k0 = 0; k0 < N; k0 += KB) {
-        const int nbt = min(KB, N - k0);
-        // every CTA of the team inverts the diagonal block (the same values)
+    int *gr = tm.n > 1 ? tm.gx : nullptr, *gc = tm.n > 1 ? tm.gx + ntr * TM : nullptr;
+    // every CTA of the team inverts the diagonal block (the same values)
+    auto diag = [&](int k0, int m) {
         if (threadIdx.x < 32) {
-            const int r = invert_diag_warp(A, ld, k0, nbt, s);
+            const int r = invert_diag_warp(A, ld, k0, m, s);
             if (r && !info) info = k0 + r;
         }
         __syncthreads();
-        panel_w(P, s, A, ld, N, k0, nbt, rr.x, rr.y, tm.n > 1 ? tm.gx : nullptr);
-        if (nbt < N) {
-            const int nrest = N - nbt, ntc = (nrest + PTN - 1) / PTN;
-            const int2 cr = team_range(tm, ntc * PTN, 8);
-            int *gc = tm.n > 1 ? tm.gx + ntr * TM : nullptr;
-            convert_b(P, A, ld, N, k0, nbt, cr.x, cr.y, gc);
-            if (tm.n > 1) {
-                // the W and B tiles of both CTAs (read by bulk copies) and their exponents
-                asm volatile("fence.proxy.async;\n" ::: "memory");
-                cluster_sync();
-                for (int i = threadIdx.x; i < ntr * TM; i += NT) P.rexpW[i] = __ldcg(tm.gx + i);
-                for (int j = threadIdx.x; j < ntc * PTN; j += NT) P.cexpB[j] = __ldcg(gc + j);
+    };
+    // B tiles of the K rows [krow0, krow0 + nkr) for the columns of cmap, then
+    // A(:, cols) += W B; every C tile of both CTAs is stored before it returns
+    auto update = [&](const ColMap &cmap, int krow0, int nkr) -> bool {
+        const int ntc = cmap.ntc();
+        const int2 cr = team_range(tm, ntc * PTN, 8);
+        if (nkr > KB) convert_b<2>(P, A, ld, krow0, nkr, cmap, cr.x, cr.y, gc);
+        else convert_b<1>(P, A, ld, krow0, nkr, cmap, cr.x, cr.y, gc);
+        if (tm.n > 1) {
+            // the W and B tiles of both CTAs (read by bulk copies) and their exponents
+            asm volatile("fence.proxy.async;\n" ::: "memory");
+            cluster_sync();
+            for (int i = threadIdx.x; i < ntr * TM; i += NT) P.rexpW[i] = __ldcg(gr + i);
+            for (int j = threadIdx.x; j < ntc * PTN; j += NT) P.cexpB[j] = __ldcg(gc + j);
+        }
+        const int2 tr = team_range(tm, ntr * ntc, 1);
+        const bool ok = trailing_pipe(P, N, cm, cmap, nkr > KB ? 2 : 1, tr.x, tr.y);
+        return !team_or(tm, !ok);
+    };
+    // 64-column panels once the working matrices of a wave no longer stay in
+    // L2 (their rank-32 updates then stream from HBM); 32-column panels below
+    const bool pairs = N > 256;
+    int k0 = 0;
+    while (k0 < N) {
+        if (pairs && N - k0 >= 2 * KB) {
+            // A 64-column panel K1 | K2: two 32-column steps on the panel's own
+            // columns (K1 eliminated from K2, K2 from K1, each a one-column-tile
+            // update), then W = A(:, K) - E_K and one rank-64 update of every
+            // other column: half the passes over the working matrix of two
+            // rank-32 updates, the same elimination.
+            const int k1 = k0 + KB;
+            diag(k0, KB);
+            panel_w(P, s, A, ld, N, k0, KB, rr.x, rr.y, gr);
+            if (!update(ColMap{0, 0, k1, KB}, k0, KB)) { *err = 1; return info; }
+            diag(k1, KB);
+            panel_w(P, s, A, ld, N, k1, KB, rr.x, rr.y, gr);
+            if (!update(ColMap{0, 0, k0, KB}, k1, KB)) { *err = 1; return info; }
+            if (N > k0 + 2 * KB) {
+                panel_w64(P, A, ld, N, k0, rr.x, rr.y, gr);
+                if (!update(ColMap{k0, 2 * KB, -1, N - 2 * KB}, k0, 2 * KB)) { *err = 1; return info; }
             }
-            const int2 tr = team_range(tm, ntr * ntc, 1);
-            const bool ok = trailing_pipe(P, N, k0, nbt, cm, tr.x, tr.y);
-            // every C tile of both CTAs stored before the next panel reads A
-            if (team_or(tm, !ok)) {
-                *err = 1;
-                return info;
-            }
+            k0 += 2 * KB;
         } else {
-            team_sync(tm);
+            const int nbt = min(KB, N - k0);
+            diag(k0, nbt);
+            panel_w(P, s, A, ld, N, k0, nbt, rr.x, rr.y, gr);
+            if (nbt < N) {
+                if (!update(ColMap{k0, nbt, -1, N - nbt}, k0, nbt)) { *err = 1; return info; }
+            } else {
+                team_sync(tm);
+            }
+            k0 += nbt;
         }
     }
     return info;
@@ -788,11 +904,21 @@ __global__ void __launch_bounds__(NT, 1)
 //   d      [2][ncap][N] the correction, two slices at a time
 //   oc     [ncap] open channels of the right lead, then n_open
 // complex FP32 everywhere (column j of a slice at j * N).
+// The sweep's job vectors in shared memory, and the lead self-energies in
+// global memory (see carve_job_slim).
+__host__ __device__ inline size_t job_smem_bytes_slim(int N) {
+    const int n4 = rup(N, 4);
+    const size_t b = 3 * (size_t)n4 * 4 + 16;
+    return (b + 127) / 128 * 128;
+}
+__host__ __device__ inline size_t job_sig_bytes(int N) { return 2 * (size_t)rup(N, 2) * 16; }
+
 struct MixedLayout {
     int N, Nz, ld, ntr, nkc, ncap;
     size_t mat_bytes;  // one matrix in split tiles
     size_t off_tiles, off_prow, off_rexp, off_x, off_rc, off_d, off_oc, job_bytes;
     size_t off_gx;         // in a wave slot's scratch: the team's exponent exchange
+    size_t off_sig;        // ... then the lead self-energies of each CTA of the team
     size_t scratch_bytes;  // per wave slot (the CTAs of one job)
 };
 constexpr size_t TILE_BYTES = 4 * (size_t)TM * KB * 2;  // 32 KB
@@ -816,8 +942,15 @@ MixedLayout make_layout(int N, int Nz, int ld, int ncap) {
     // by a team; passes: the B operand of one product in split tiles
     L.off_gx = align256((size_t)2 * N * ld * 8 + pipe_scratch_bytes(N));
     const size_t gx_bytes = 4 * ((size_t)L.ntr * TM + (size_t)((N + PTN - 1) / PTN) * PTN);
-    L.scratch_bytes = align256(std::max(L.off_gx + gx_bytes, (size_t)L.nkc * ncap * 256));
+    L.off_sig = align256(L.off_gx + gx_bytes);
+    L.scratch_bytes = align256(std::max(L.off_sig + 2 * job_sig_bytes(N), (size_t)L.nkc * ncap * 256));
     return L;
+}
+
+// shared memory of k_mixed_sweep: Gauss-Jordan state, the update pipeline,
+// the job's index vectors and the team's exchange slots
+inline size_t sweep_smem_bytes(int N) {
+    return gj_smem_bytes(N) + (pipe_smem_bytes(N) + 127) / 128 * 128 + job_smem_bytes_slim(N) + 16;
 }
 
 struct MixedArgs {
@@ -828,6 +961,7 @@ struct MixedArgs {
     const int2 *jobs;      // per wave slot: (energy index, k-point)
     int njobs;
     int cpj;               // CTAs (one cluster) per job in the sweep: 1 or 2
+    int pa;                // factor ring stages of the passes
     unsigned char *jobmem; // njobs job regions
     unsigned char *scratch;
     double *tau, *dnorm, *xnorm, *dprev;
@@ -845,25 +979,18 @@ __host__ __device__ inline size_t job_smem_bytes(int N) {
     b += 2 * (size_t)n2 * 16 + 2 * (size_t)n2 * 8;
     return (b + 127) / 128 * 128;
 }
-// The sweep's variant: only nx, ny, the open-channel list and the lead
-// self-energies in its own space; gamma_L / gamma_R (needed only while the
-// open channels are listed at the start of a job) at gscr.
-__host__ __device__ inline size_t job_smem_bytes_slim(int N) {
-    const int n4 = rup(N, 4), n2 = rup(N, 2);
-    size_t b = 3 * (size_t)n4 * 4 + 16;
-    b = (b + 15) / 16 * 16;
-    b += 2 * (size_t)n2 * 16;
-    return (b + 127) / 128 * 128;
-}
-__device__ inline negf::Smem carve_job_slim(unsigned char *base, int N, unsigned char *gscr) {
+// The sweep's variant: only nx, ny and the open-channel list in its own
+// space; gamma_L / gamma_R (needed only while the open channels are listed at
+// the start of a job) at gscr, the lead self-energies (read only by the
+// diagonal of the end slices) in global memory at gsig.
+__device__ inline negf::Smem carve_job_slim(unsigned char *base, int N, unsigned char *gscr, unsigned char *gsig) {
     negf::Smem s{};
     const int n4 = rup(N, 4), n2 = rup(N, 2);
     s.nx = (int *)base;
     s.ny = s.nx + n4;
     s.rows = s.ny + n4;
     s.nrows = s.rows + n4;
-    size_t off = ((size_t)3 * n4 * 4 + 16 + 15) / 16 * 16;
-    s.sigL = (double2 *)(base + off);
+    s.sigL = (double2 *)gsig;
     s.sigR = s.sigL + n2;
     s.gL = (double *)gscr;
     s.gR = s.gL + n2;
@@ -887,36 +1014,37 @@ __device__ inline negf::Smem carve_job(unsigned char *base, int N) {
 // M = round32(D_k - inv(prev)) in FP64: the off-diagonal part of D_k
 // (-c2 V(G_i - G_j), the same for every energy and k-point) streams from the
 // precomputed table, the diagonal is generated (negf::d_element,
-// grid.f90:236-333).  Rows [rlo, rhi); thread t owns row rlo + t: coalesced loads of the table and of
-// the previous inverse R, coalesced stores; four columns per pass keep eight
-// loads in flight per thread.
+// grid.f90:236-333), rows [rlo, rhi).
 __device__ inline void form_mixed(float2 *__restrict__ M, const negf::Geo &g, const negf::Smem &js,
                                   const double2 *__restrict__ voff, int k, double2 E, int ik,
                                   const float2 *__restrict__ R, int rlo, int rhi) {
     const int N = g.N, ld = g.ld;
     const double2 *vs = g.vhat + (size_t)g.W * g.H * k;
     const double2 *vk = voff + (size_t)N * ld * k;
-    for (int j0 = 0; j0 < N; j0 += 4) {
-        for (int t = rlo + threadIdx.x; t < rhi; t += NT) {
-            double2 d[4];
-            float2 r[4];
+    // work items (row, 8-column chunk), rows fastest: every thread busy, loads
+    // coalesced along the rows, sixteen loads in flight per item
+    constexpr int CH = 8;
+    const int nrows = rhi - rlo, nch = (N + CH - 1) / CH, nitem = nrows * nch;
+    for (int it = threadIdx.x; it < nitem; it += NT) {
+        const int t = rlo + it % nrows, j0 = (it / nrows) * CH;
+        double2 d[CH];
+        float2 r[CH];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int j = j0 + q;
-                d[q] = make_double2(0.0, 0.0);
-                r[q] = make_float2(0.f, 0.f);
-                if (j < N) {
-                    d[q] = vk[t + (size_t)ld * j];
-                    if (R) r[q] = ldcg2(R + t + (size_t)ld * j);
-                }
+        for (int q = 0; q < CH; ++q) {
+            const int j = j0 + q;
+            d[q] = make_double2(0.0, 0.0);
+            r[q] = make_float2(0.f, 0.f);
+            if (j < N) {
+                d[q] = __ldg(vk + t + (size_t)ld * j);
+                if (R) r[q] = ldcg2(R + t + (size_t)ld * j);
             }
+        }
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int j = j0 + q;
-                if (j == t) d[q] = negf::d_element(g, js, vs, k, E, ik, t, t, js.nx[t], js.ny[t]);
-                if (j < N) M[t + (size_t)ld * j] = make_float2((float)(d[q].x - (double)r[q].x),
-                                                               (float)(d[q].y - (double)r[q].y));
-            }
+        for (int q = 0; q < CH; ++q) {
+            const int j = j0 + q;
+            if (j == t) d[q] = negf::d_element(g, js, vs, k, E, ik, t, t, js.nx[t], js.ny[t]);
+            if (j < N) M[t + (size_t)ld * j] = make_float2((float)(d[q].x - (double)r[q].x),
+                                                           (float)(d[q].y - (double)r[q].y));
         }
     }
 }
@@ -1020,11 +1148,11 @@ __global__ void __launch_bounds__(NT, 1) k_mixed_sweep(MixedArgs a, const __grid
     float2 *W0 = (float2 *)jscr;
     float2 *W1 = W0 + (size_t)N * ld;
     Pipe P = carve_pipe(pipe_smem, N, (unsigned char *)(W1 + (size_t)N * ld));
-    negf::Smem js = carve_job_slim(smem + off, N, P.sC);
+    const int rank = (int)(blockIdx.x % a.cpj);
+    negf::Smem js = carve_job_slim(smem + off, N, P.sC, jscr + L.off_sig + (size_t)rank * job_sig_bytes(N));
     off += job_smem_bytes_slim(N);
-    int *rexpN = (int *)(smem + off);
-    off += (size_t)rup(N, 4) * 4;
-    Team tm{(int)(blockIdx.x % a.cpj), a.cpj, (int *)(jscr + L.off_gx), (int *)(smem + off), 0u};
+    int *rexpN = P.rexpW;  // free while a factor is stored
+    Team tm{rank, a.cpj, (int *)(jscr + L.off_gx), (int *)(smem + off), 0u};
     for (int i = tid; i < N; i += NT) { js.nx[i] = g.nx[i]; js.ny[i] = g.ny[i]; }
     gj_identity(s, N);
     pipe_setup(P);
@@ -1086,14 +1214,16 @@ __global__ void __launch_bounds__(NT, 1) k_mixed_sweep(MixedArgs a, const __grid
 // z = R v_p, y(iprow[t]) = alpha z(t) + wadd(iprow[t]).  v = v1 - v2 (v2 may be
 // null).  The B operand v_p is converted once per product into split tiles
 // (one exponent per column over all N rows) in the CTA's scratch; then for
-// each 128-row tile of R the K chunks stream through a 3-stage pipeline of
-// bulk copies (A: one 32 KB tile, B: one chunk) into tcgen05 MMAs.
+// each 128-row tile of R the K chunks stream through a pipeline of bulk
+// copies (A: a ring of pa 32 KB factor tiles, as deep as shared memory allows
+// for the vector block's width; B: one chunk) into tcgen05 MMAs.
 enum PassMode { PASS_X0 = 0, PASS_BACK = 1, PASS_CORR = 2 };
-constexpr int PA = 3;  // A ring stages (one 32 KB factor tile each)
-constexpr int PB = 3;  // B ring stages (one K chunk of the vector block each)
+constexpr int PA_MIN = 3, PA_MAX = 6;  // A ring stages (one 32 KB factor tile each)
+constexpr int PB = 3;                  // B ring stages (one K chunk of the vector block each)
 
 struct PassSmem {
-    unsigned char *stA;   // PA x TILE_BYTES
+    int pa;               // A ring stages
+    unsigned char *stA;   // pa x TILE_BYTES
     unsigned char *stB;   // PB x (ncap * 256)
     int *cexp;            // [ncap] column exponents of the current product's v
     unsigned *cmax;       // [ncap] column maxima (float bits) of the next product's v
@@ -1101,24 +1231,25 @@ struct PassSmem {
     uint32_t *tslot;
     double *red;          // [2 * NWARP]
 };
-constexpr int PASS_BARS = 2 * PA + 2 * PB + 2 + 2 + 1;
-__host__ __device__ inline size_t pass_smem_bytes(int N, int ncap) {
-    size_t b = PA * TILE_BYTES + PB * (size_t)ncap * 256;
+constexpr int PASS_BARS = 2 * PA_MAX + 2 * PB + 2 + 2 + 1;
+__host__ __device__ inline size_t pass_smem_bytes(int N, int ncap, int pa) {
+    size_t b = pa * TILE_BYTES + PB * (size_t)ncap * 256;
     b += 2 * (size_t)ncap * 4 + PASS_BARS * 8 + 16 + 2 * NWARP * 8;
     (void)N;
     return (b + 127) / 128 * 128;
 }
-__device__ inline PassSmem carve_pass(unsigned char *base, int ncap) {
+__device__ inline PassSmem carve_pass(unsigned char *base, int ncap, int pa) {
     PassSmem p;
     unsigned char *q = base;
-    p.stA = q; q += PA * TILE_BYTES;
+    p.pa = pa;
+    p.stA = q; q += pa * TILE_BYTES;
     p.stB = q; q += PB * (size_t)ncap * 256;
     p.cexp = (int *)q; q += (size_t)ncap * 4;
     p.cmax = (unsigned *)q; q += (size_t)ncap * 4;
     q = (unsigned char *)(((uintptr_t)q + 15) & ~(uintptr_t)15);
     uint64_t *bar = (uint64_t *)q;
-    p.fullA = bar; p.emptyA = bar + PA;
-    p.fullB = bar + 2 * PA; p.emptyB = p.fullB + PB;
+    p.fullA = bar; p.emptyA = bar + PA_MAX;
+    p.fullB = bar + 2 * PA_MAX; p.emptyB = p.fullB + PB;
     p.accFull = p.emptyB + PB; p.accEmpty = p.accFull + 2;
     p.bReady = p.accEmpty + 2;
     q += PASS_BARS * 8;
@@ -1318,8 +1449,8 @@ __device__ bool pass_run(const MixedLayout &L, const PassSmem &p, unsigned char 
                 const Prod q = pass_prod(mode, s, Nz, sl, x, rc, d, xa);
                 const unsigned char *tiles = jm + L.off_tiles + (size_t)q.slot * L.mat_bytes;
                 for (int t = 0; t < ntr * nkc && !err; ++t, ++ia) {
-                    const uint32_t st = ia % PA;
-                    if (ia >= PA && !tc::mbar_wait(&p.emptyA[st], ((ia / PA) - 1) & 1u, WAIT_LIMIT)) { err = 1; break; }
+                    const uint32_t st = ia % (uint32_t)p.pa;
+                    if (ia >= (uint32_t)p.pa && !tc::mbar_wait(&p.emptyA[st], ((ia / p.pa) - 1) & 1u, WAIT_LIMIT)) { err = 1; break; }
                     mbar_expect_tx(&p.fullA[st], (uint32_t)TILE_BYTES);
                     bulk_g2s(p.stA + st * TILE_BYTES, tiles + (size_t)t * TILE_BYTES, (uint32_t)TILE_BYTES,
                              &p.fullA[st]);
@@ -1351,8 +1482,8 @@ __device__ bool pass_run(const MixedLayout &L, const PassSmem &p, unsigned char 
                     const uint32_t buf = iu & 1u, dacc = tbase + buf * (2 * L.ncap);
                     if (iu >= 2 && !tc::mbar_wait(&p.accEmpty[buf], ((iu >> 1) - 1) & 1u, WAIT_LIMIT)) { err = 1; break; }
                     for (int kc = 0; kc < nkc; ++kc, ++ia, ++ib) {
-                        const uint32_t sa = ia % PA, sb = ib % PB;
-                        if (!tc::mbar_wait(&p.fullA[sa], (ia / PA) & 1u, WAIT_LIMIT) ||
+                        const uint32_t sa = ia % (uint32_t)p.pa, sb = ib % PB;
+                        if (!tc::mbar_wait(&p.fullA[sa], (ia / p.pa) & 1u, WAIT_LIMIT) ||
                             !tc::mbar_wait(&p.fullB[sb], (ib / PB) & 1u, WAIT_LIMIT)) { err = 1; break; }
                         tc::fence_after_sync();
                         issue_pass_chunk(p.stA + sa * TILE_BYTES, p.stB + sb * bst, npad, dacc, kc == 0);
@@ -1448,14 +1579,14 @@ __global__ void __launch_bounds__(NT, 1) k_mixed_pass(MixedArgs a, int mode, int
     extern __shared__ __align__(128) unsigned char smem[];
     const MixedLayout &L = a.L;
     const int N = L.N, Nz = L.Nz, tid = threadIdx.x;
-    PassSmem p = carve_pass(smem, L.ncap);
+    PassSmem p = carve_pass(smem, L.ncap, a.pa);
     // the job vectors of the tau step live in the A ring, idle by then
     negf::Smem js = carve_job(p.stA, N);
     uint32_t ncols = 32;
     while (ncols < 4u * L.ncap) ncols <<= 1;  // two accumulators of 2 ncap columns
     if (tid < 32) tc::tmem_alloc(p.tslot, ncols);
     if (tid == 0) {
-        for (int s = 0; s < PA; ++s) { tc::mbar_init(&p.fullA[s], 1); tc::mbar_init(&p.emptyA[s], 1); }
+        for (int s = 0; s < p.pa; ++s) { tc::mbar_init(&p.fullA[s], 1); tc::mbar_init(&p.emptyA[s], 1); }
         for (int s = 0; s < PB; ++s) { tc::mbar_init(&p.fullB[s], 1); tc::mbar_init(&p.emptyB[s], 1); }
         for (int s = 0; s < 2; ++s) { tc::mbar_init(&p.accFull[s], 1); tc::mbar_init(&p.accEmpty[s], 4); }
         tc::mbar_init(p.bReady, 1);
@@ -1804,6 +1935,7 @@ negf::Geo mixed_geo(const negf_ctx *c) {
 }
 
 constexpr double PI_M = 3.141592653589793;  // global.f90:28
+constexpr int FP64_KEEP = 32;                // FP64 re-runs whose workspace fits beside the mixed buffers
 
 // |k+G_i|^2 / 2 for mode i at k-point ik (grid.f90:258)
 double kinetic(const negf_ctx *c, int ik, int i) {
@@ -1882,10 +2014,14 @@ int negf_internal_mixed(negf_ctx *c, const double *h_E, const double *d_E, int n
         }
         size_t free_b = 0, total_b = 0;
         cudaMemGetInfo(&free_b, &total_b);
-        // the FP64 re-runs keep their own workspace (4 blocks per CTA)
-        const size_t fp64_ws = (size_t)c->num_sms * 4 * c->ld * N * 16;
+        // the FP64 re-runs keep their own workspace (4 blocks per CTA): room is
+        // kept for FP64_KEEP of them beside the mixed buffers (beyond that the
+        // mixed buffers are released before the re-runs), less what the
+        // context already holds
+        const size_t fp64_ws = (size_t)std::min(c->num_sms, FP64_KEEP) * 4 * c->ld * N * 16;
+        const size_t fp64_more = fp64_ws > c->ws_bytes ? fp64_ws - c->ws_bytes : 0;
         const size_t avail = free_b + c->mixed_bytes;
-        const size_t budget = avail > fp64_ws + ((size_t)4 << 30) ? (size_t)(0.92 * (avail - fp64_ws)) - ((size_t)2 << 30) : 0;
+        const size_t budget = avail > fp64_more + ((size_t)2 << 30) ? (size_t)(0.95 * (avail - fp64_more)) - ((size_t)1 << 30) : 0;
         const size_t mem_jobs = budget / (per_job + small_per_job);
         int W = (int)std::min<size_t>({(size_t)m_jobs.size(), (size_t)c->num_sms, mem_jobs});
         // Two CTAs (one cluster) per job when a wave of single-CTA jobs would
@@ -1893,8 +2029,15 @@ int negf_internal_mixed(negf_ctx *c, const double *h_E, const double *d_E, int n
         // bounding the wave): the job then sweeps on two SMs.
         int cpj = pol.ctas_per_job;
         if (cpj == 0) cpj = (2 * (size_t)W <= (size_t)c->num_sms) ? 2 : 1;
-        const size_t sm_sweep = gj_smem_bytes(N) + (pipe_smem_bytes(N) + 127) / 128 * 128 +
-                                job_smem_bytes_slim(N) + (size_t)rup(N, 4) * 4 + 16;
+        const size_t sm_sweep = sweep_smem_bytes(N);
+        int smem_optin = 0;
+        CKM(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
+        // a basis whose sweep state does not fit one SM's shared memory (about
+        // N > 900) runs in FP64 like a job that does not fit device memory
+        // the deepest factor ring of the passes that shared memory allows
+        int pa = PA_MAX;
+        while (pa > PA_MIN && pass_smem_bytes(N, ncap, pa) > (size_t)smem_optin) --pa;
+        if (sm_sweep > (size_t)smem_optin || pass_smem_bytes(N, ncap, pa) > (size_t)smem_optin) W = 0;
         if (cpj == 2 && W >= 1) {
             CKM(cudaFuncSetAttribute(k_mixed_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_sweep));
             cudaLaunchConfig_t qc = {};
@@ -1914,7 +2057,7 @@ int negf_internal_mixed(negf_ctx *c, const double *h_E, const double *d_E, int n
             else W = std::min(W, nclu);
         }
         if (W < 1) {
-            // not enough device memory for one job: everything in FP64
+            // not enough device memory (or shared memory) for one job: everything in FP64
             for (int q : m_jobs) { f_ie.push_back(q % nE); f_ik.push_back(q / nE); }
             stats.n_fp64_policy += (int)m_jobs.size();
             m_jobs.clear();
@@ -1947,7 +2090,8 @@ int negf_internal_mixed(negf_ctx *c, const double *h_E, const double *d_E, int n
             a.status = (int *)(a.dprev + W);
             a.tol = pol.tau_tolerance;
             a.cpj = cpj;
-            const size_t sm_pass = pass_smem_bytes(N, ncap);
+            const size_t sm_pass = pass_smem_bytes(N, ncap, pa);
+            a.pa = pa;
             const size_t sm_res = (size_t)2 * negf::KC * (negf::AP + negf::BP) * 16 + job_smem_bytes(N);
             rc = set_smem(k_mixed_sweep, sm_sweep);
             if (!rc) rc = set_smem(k_mixed_pass, sm_pass);
@@ -2021,6 +2165,12 @@ int negf_internal_mixed(negf_ctx *c, const double *h_E, const double *d_E, int n
     }
     // ---- FP64 re-runs
     float ms64 = 0.f;
+    if ((int)f_ie.size() > FP64_KEEP && c->d_mixed) {
+        // more re-runs than the room kept for them: the mixed buffers go first
+        cudaFree(c->d_mixed);
+        c->d_mixed = nullptr;
+        c->mixed_bytes = 0;
+    }
     if (!f_ie.empty()) {
         std::vector<double> t64(f_ie.size());
         std::vector<int> i64(f_ie.size());
