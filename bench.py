@@ -533,12 +533,13 @@ def run_ours(args):
     nk = len(pr.kpoint)
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
     eng = Engine(*pr.engine_args(), device=local)
-    # set-up call (allocations) on one SM count of energies spread over the grid;
-    # it also reports how many jobs a mixed wave holds on this device (one job per
-    # SM, or fewer on two SMs each when device memory bounds the wave: a wave's
-    # memory grows with the open channels of its highest energy), so a step is
-    # whole waves
-    eng.transmission(np.ascontiguousarray(E_all[:: max(1, len(E_all) // sms)][:sms]), precision=NEGF_MIXED)
+    # set-up call (allocations) on one SM count of energies spread over the grid,
+    # its last point included; it also reports how many jobs a mixed wave holds on
+    # this device (one job per SM, or fewer on two SMs each when device memory
+    # bounds the wave: a wave's memory grows with the open channels of its highest
+    # energy), so a step is whole waves
+    E_setup = E_all[np.linspace(0, len(E_all) - 1, min(sms, len(E_all))).round().astype(int)]
+    eng.transmission(np.ascontiguousarray(E_setup), precision=NEGF_MIXED)
     wave = max(1, eng.mixed_stats()["jobs_per_wave"])
     B = args.batch or wave * max(1, round(sms / wave))
     n_steps = args.warmup + args.steps

@@ -916,6 +916,8 @@ __host__ __device__ inline size_t job_sig_bytes(int N) { return 2 * (size_t)rup(
 struct MixedLayout {
     int N, Nz, ld, ntr, nkc, ncap;
     size_t mat_bytes;  // one matrix in split tiles
+    int last_rows;     // rows stored of the last row tile (the valid ones, rounded up to 8)
+    uint32_t last_plane;  // bytes of one plane of a last-row-tile tile (last_rows / 8 core-matrix rows)
     size_t off_tiles, off_prow, off_rexp, off_x, off_rc, off_d, off_oc, job_bytes;
     size_t off_gx;         // in a wave slot's scratch: the team's exponent exchange
     size_t off_sig;        // ... then the lead self-energies of each CTA of the team
@@ -928,7 +930,12 @@ MixedLayout make_layout(int N, int Nz, int ld, int ncap) {
     L.N = N; L.Nz = Nz; L.ld = ld; L.ncap = ncap;
     L.ntr = (N + TM - 1) / TM;
     L.nkc = (N + KB - 1) / KB;
-    L.mat_bytes = (size_t)L.ntr * L.nkc * TILE_BYTES;
+    // the last row tile keeps only its valid rows: a plane of it is the first
+    // last_rows / 8 core-matrix rows of a full plane (up to 11 % of the factor
+    // storage at N = 797, so more jobs fit a wave)
+    L.last_rows = ((N - (L.ntr - 1) * TM) + 7) / 8 * 8;
+    L.last_plane = (uint32_t)(L.last_rows / 8) * (KB / 8) * 128;
+    L.mat_bytes = (size_t)(L.ntr - 1) * L.nkc * TILE_BYTES + (size_t)L.nkc * 4 * L.last_plane;
     size_t o = 0;
     L.off_tiles = o; o = align256(o + (size_t)Nz * L.mat_bytes);
     L.off_prow = o; o = align256(o + (size_t)Nz * N * 4);
@@ -951,6 +958,15 @@ MixedLayout make_layout(int N, int Nz, int ld, int ncap) {
 // the job's index vectors and the team's exchange slots
 inline size_t sweep_smem_bytes(int N) {
     return gj_smem_bytes(N) + (pipe_smem_bytes(N) + 127) / 128 * 128 + job_smem_bytes_slim(N) + 16;
+}
+
+// Byte offset of factor tile (rt, kc) in a stored matrix, and its plane stride.
+__host__ __device__ inline size_t factor_tile_off(const MixedLayout &L, int rt, int kc) {
+    return rt < L.ntr - 1 ? ((size_t)rt * L.nkc + kc) * TILE_BYTES
+                          : (size_t)(L.ntr - 1) * L.nkc * TILE_BYTES + (size_t)kc * 4 * L.last_plane;
+}
+__host__ __device__ inline uint32_t factor_plane(const MixedLayout &L, int rt) {
+    return rt < L.ntr - 1 ? (uint32_t)(TM * KB * 2) : L.last_plane;
 }
 
 struct MixedArgs {
@@ -1100,8 +1116,10 @@ __device__ inline void store_factor(const float2 *__restrict__ R, const MixedLay
     for (int u = ur.x; u < ur.y; ++u) {
         const int rt = u / L.nkc, kc = u % L.nkc;
         const int row = rt * TM + r;
+        if (rt == L.ntr - 1 && r >= L.last_rows) continue;  // not stored
         const float sc = tc::exp2i(row < N ? -rexpN[row] : 0);
-        unsigned char *tile = tiles + (size_t)u * TILE_BYTES;
+        unsigned char *tile = tiles + factor_tile_off(L, rt, kc);
+        const uint32_t pl = factor_plane(L, rt);
 #pragma unroll
         for (int g2 = 0; g2 < 2; ++g2) {
             const int kg = 2 * h + g2;
@@ -1119,10 +1137,10 @@ __device__ inline void store_factor(const float2 *__restrict__ R, const MixedLay
                 rh[q] = a.hi; rl[q] = a.lo; ih[q] = bb.hi; il[q] = bb.lo;
             }
             const uint32_t off = tc::kmajor_offset(r, 8 * kg, KB);
-            *(uint4 *)(tile + 0 * (TM * KB * 2) + off) = *(const uint4 *)rh;
-            *(uint4 *)(tile + 1 * (TM * KB * 2) + off) = *(const uint4 *)rl;
-            *(uint4 *)(tile + 2 * (TM * KB * 2) + off) = *(const uint4 *)ih;
-            *(uint4 *)(tile + 3 * (TM * KB * 2) + off) = *(const uint4 *)il;
+            *(uint4 *)(tile + 0 * pl + off) = *(const uint4 *)rh;
+            *(uint4 *)(tile + 1 * pl + off) = *(const uint4 *)rl;
+            *(uint4 *)(tile + 2 * pl + off) = *(const uint4 *)ih;
+            *(uint4 *)(tile + 3 * pl + off) = *(const uint4 *)il;
         }
     }
     __syncthreads();
@@ -1451,9 +1469,19 @@ __device__ bool pass_run(const MixedLayout &L, const PassSmem &p, unsigned char 
                 for (int t = 0; t < ntr * nkc && !err; ++t, ++ia) {
                     const uint32_t st = ia % (uint32_t)p.pa;
                     if (ia >= (uint32_t)p.pa && !tc::mbar_wait(&p.emptyA[st], ((ia / p.pa) - 1) & 1u, WAIT_LIMIT)) { err = 1; break; }
-                    mbar_expect_tx(&p.fullA[st], (uint32_t)TILE_BYTES);
-                    bulk_g2s(p.stA + st * TILE_BYTES, tiles + (size_t)t * TILE_BYTES, (uint32_t)TILE_BYTES,
-                             &p.fullA[st]);
+                    const int rt = t / nkc, kc = t % nkc;
+                    const unsigned char *src = tiles + factor_tile_off(L, rt, kc);
+                    if (rt < ntr - 1) {
+                        mbar_expect_tx(&p.fullA[st], (uint32_t)TILE_BYTES);
+                        bulk_g2s(p.stA + st * TILE_BYTES, src, (uint32_t)TILE_BYTES, &p.fullA[st]);
+                    } else {
+                        // a last-row-tile tile: each plane to the start of its full-size
+                        // plane in the stage (the rows past it are never read back)
+                        mbar_expect_tx(&p.fullA[st], 4 * L.last_plane);
+                        for (int pl = 0; pl < 4; ++pl)
+                            bulk_g2s(p.stA + st * TILE_BYTES + (size_t)pl * (TM * KB * 2), src + (size_t)pl * L.last_plane,
+                                     L.last_plane, &p.fullA[st]);
+                    }
                 }
             }
         }
