@@ -140,7 +140,7 @@ __device__ __forceinline__ uint32_t pivot_key32(float v, int row) {
 // P(r, c) = R(pr[r], ipr[c]) (pr[k] the pivot lane of step k), with the
 // identity on the padding.  Returns the 1-based step of the first zero pivot
 // (0 if none).
-__device__ inline int invert_diag_warp(const float2 *__restrict__ A, int ld, int k0, int m, const GjSmem &s) {
+__device__ __noinline__ int invert_diag_warp(const float2 *__restrict__ A, int ld, int k0, int m, const GjSmem &s) {
     const int lane = threadIdx.x & 31;
     const bool valid = lane < m;
     float2 R[32];
@@ -251,15 +251,16 @@ struct Pipe {
     uint64_t *fullC, *doneC;         // [NCB]: C loaded / C updated by the epilogue
     uint64_t *accFull, *accEmpty;    // [2]
     uint64_t *drain;                 // [1] completion of every MMA before tensor memory is freed
+    uint64_t *laReady;               // [1] the look-ahead tile is stored (next diagonal block final)
     int *rexpW;                      // [ntr * TM] row exponents of W
     int *cexpB;                      // [ntc * PTN] column exponents of the pivot rows
     uint32_t *tslot;
     unsigned char *wt, *bt;          // global: W tiles (NKB * WTILE per row tile), B tiles (NKB * BTILE
                                      // per column tile; an update of one K chunk uses the first)
     uint32_t tbase;
-    uint32_t nW, nB, nT;             // W tiles, B tiles and output tiles so far (phase counters)
+    uint32_t nW, nB, nT, nLA;        // W tiles, B tiles, output tiles, look-aheads so far (phase counters)
 };
-constexpr int PIPE_BARS = 2 + 2 * NBB + 2 * NCB + 4 + 1;
+constexpr int PIPE_BARS = 2 + 2 * NBB + 2 * NCB + 4 + 1 + 1;
 __host__ __device__ inline size_t pipe_smem_bytes(int N) {
     const int ntr = (N + TM - 1) / TM, ntc = (N + PTN - 1) / PTN;
     return (size_t)NKB * WTILE + NBB * (size_t)NKB * BTILE + NCB * (size_t)CTILE + PIPE_BARS * 8 + 8 + 4 * (size_t)ntr * TM +
@@ -283,13 +284,14 @@ __device__ inline Pipe carve_pipe(unsigned char *base, int N, unsigned char *gsc
     P.fullC = P.emptyB + NBB; P.doneC = P.fullC + NCB;
     P.accFull = P.doneC + NCB; P.accEmpty = P.accFull + 2;
     P.drain = P.accEmpty + 2;
+    P.laReady = P.drain + 1;
     q += PIPE_BARS * 8 + 8;
     P.rexpW = (int *)q; q += 4 * (size_t)ntr * TM;
     P.cexpB = (int *)q; q += 4 * (size_t)ntc * PTN;
     P.tslot = (uint32_t *)q;
     P.wt = gscratch;
     P.bt = gscratch + (size_t)ntr * NKB * WTILE;
-    P.nW = P.nB = P.nT = 0;
+    P.nW = P.nB = P.nT = P.nLA = 0;
     return P;
 }
 // 128 tensor-memory columns: two accumulators of PTN complex columns (re, im)
@@ -302,6 +304,7 @@ __device__ inline void pipe_setup(Pipe &P) {
         for (int i = 0; i < NCB; ++i) { tc::mbar_init(&P.fullC[i], 1); tc::mbar_init(&P.doneC[i], 4); }
         for (int i = 0; i < 2; ++i) { tc::mbar_init(&P.accFull[i], 1); tc::mbar_init(&P.accEmpty[i], 4); }
         tc::mbar_init(P.drain, 1);
+        tc::mbar_init(P.laReady, 1);
     }
     tc::fence_before_sync();
     __syncthreads();
@@ -588,38 +591,59 @@ __device__ __noinline__ void convert_b(const Pipe &P, const float2 *__restrict__
     }
 }
 
+// Look-ahead of a trailing update: the output tile that holds the next
+// panel's diagonal block goes first; once it is stored, warp 2 (idle during
+// the update) inverts that block into s.sP while the other tiles run.
+struct LookAhead {
+    int tile;                  // output tile index, -1: none
+    const float2 *A;
+    int ld, k0, m;             // the block A(k0:k0+m, k0:k0+m)
+    int *info;                 // shared: its zero-pivot step (1-based), 0 if none
+};
+
 // A(:, cols) += W * B (N rows) with nkb K chunks (W and B tiles already in the CTA's
 // global scratch), pipelined (see above); the C tiles of matrix cm move by
 // TMA, the columns as cmap says.  Output tiles [t0, t1) of the ntr x ntc
-// tiles (row tile major), so that the CTAs of a team share the update.
-// Returns false if a wait timed out (uniform over the CTA).
-__device__ inline bool trailing_pipe(Pipe &P, int N, const CMat &cm, const ColMap &cmap, int nkb, int t0, int t1) {
+// tiles (row tile major; the look-ahead tile first), so that the CTAs of a
+// team share the update.  Returns false if a wait timed out (uniform over
+// the CTA).
+__device__ inline bool trailing_pipe(Pipe &P, int N, const CMat &cm, const ColMap &cmap, int nkb, int t0, int t1,
+                                     const GjSmem &s, const LookAhead &la) {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nrest = cmap.nrest, ntc = cmap.ntc(), T = t1 - t0;
     const uint32_t wbytes = (uint32_t)nkb * WTILE, bbytes = (uint32_t)nkb * BTILE;
+    const bool lad = la.tile >= t0 && la.tile < t1;
     // generic stores (W/B tiles in global, the staging in the C buffers) before
     // the bulk copies and TMA tiles that read or overwrite them
     asm volatile("fence.proxy.async;\n" ::: "memory");
     __syncthreads();
     const uint32_t bW = P.nW, bB = P.nB, bT = P.nT;
     int err = 0;
+    // tile of local step v: the look-ahead tile, then the others in order
+    auto tile_of = [&](int v) -> int {
+        if (!lad) return t0 + v;
+        if (v == 0) return la.tile;
+        return t0 + v - 1 < la.tile ? t0 + v - 1 : t0 + v;
+    };
     // first matrix column of tile t: the rest columns of a tile are contiguous
     // (the panel start and width are multiples of 32)
     auto tile_col0 = [&](int t) -> int { return cmap.col((t % ntc) * PTN); };
-    // the W tile changes at the first local tile and at every row-tile start
-    auto w_first = [&](int v) -> bool { return v == 0 || (t0 + v) % ntc == 0; };
-    auto w_last = [&](int v) -> bool { return v == T - 1 || (t0 + v) % ntc == ntc - 1; };
-    auto w_index = [&](int v) -> uint32_t { return bW + (uint32_t)((t0 + v) / ntc - t0 / ntc); };
+    // the W tile changes at the first step and wherever the row tile changes
+    auto w_first = [&](int v) -> bool { return v == 0 || tile_of(v) / ntc != tile_of(v - 1) / ntc; };
+    auto w_last = [&](int v) -> bool { return v == T - 1 || tile_of(v) / ntc != tile_of(v + 1) / ntc; };
+    int nwl = 0;  // W loads of this update
+    for (int v = 0; v < T; ++v) nwl += w_first(v);
     if (warp == 0) {
         // ------------------------------------------------------ producer
         if (lane == 0) {
+            uint32_t iw = bW;  // next W load
             auto load = [&](int u) -> bool {
-                const int t = t0 + u;
+                const int t = tile_of(u);
                 if (w_first(u)) {
-                    const uint32_t iw = w_index(u);
                     if (iw >= 1 && !tc::mbar_wait(P.emptyW, (iw - 1) & 1u, WAIT_LIMIT)) return false;
                     expect_bytes(P.fullW, wbytes);
                     bulk_copy(P.sW, P.wt + (size_t)(t / ntc) * NKB * WTILE, wbytes, P.fullW);
+                    ++iw;
                 }
                 const uint32_t ib = bB + u, ic = bT + u;
                 if (ib >= NBB && !tc::mbar_wait(&P.emptyB[ib % NBB], ((ib - NBB) / NBB) & 1u, WAIT_LIMIT))
@@ -637,11 +661,19 @@ __device__ inline bool trailing_pipe(Pipe &P, int N, const CMat &cm, const ColMa
                 if (!load(u)) err = 1;
             for (int v = 0; v < T && !err; ++v) {
                 const uint32_t ic = bT + v;
+                const int t = tile_of(v);
                 if (!tc::mbar_wait(&P.doneC[ic % NCB], (ic / NCB) & 1u, WAIT_LIMIT)) { err = 1; break; }
-                tma_store4(cm.tm, ((t0 + v) / ntc) * TM, tile_col0(t0 + v), cm.z, cm.w, P.sC + (ic % NCB) * CTILE);  // clipped
+                tma_store4(cm.tm, (t / ntc) * TM, tile_col0(t), cm.z, cm.w, P.sC + (ic % NCB) * CTILE);  // clipped
                 bulk_commit();
+                if (lad && v == 0) {
+                    // the next diagonal block is final in global memory
+                    bulk_wait0();
+                    asm volatile("fence.proxy.async.global;\n" ::: "memory");
+                    mbar_arrive(P.laReady);
+                }
                 if (v + NCB < T && !load(v + NCB)) err = 1;
             }
+            if (lad && err && T > 0) mbar_arrive(P.laReady);  // release the look-ahead warp (its result is discarded)
             bulk_wait0();
             asm volatile("fence.proxy.async.global;\n" ::: "memory");
         }
@@ -649,10 +681,14 @@ __device__ inline bool trailing_pipe(Pipe &P, int N, const CMat &cm, const ColMa
     } else if (warp == 1) {
         // --------------------------------------------------- MMA issuer
         if (lane == 0) {
+            uint32_t iw = bW;  // next W use
             for (int t = 0; t < T; ++t) {
                 const uint32_t ic = bT + t, ib = bB + t, a = ic & 1u;
                 if (ic >= 2 && !tc::mbar_wait(&P.accEmpty[a], ((ic >> 1) & 1u) ^ 1u, WAIT_LIMIT)) { err = 1; break; }
-                if (w_first(t) && !tc::mbar_wait(P.fullW, w_index(t) & 1u, WAIT_LIMIT)) { err = 1; break; }
+                if (w_first(t)) {
+                    if (!tc::mbar_wait(P.fullW, iw & 1u, WAIT_LIMIT)) { err = 1; break; }
+                    ++iw;
+                }
                 if (!tc::mbar_wait(&P.fullB[ib % NBB], (ib / NBB) & 1u, WAIT_LIMIT)) { err = 1; break; }
                 tc::fence_after_sync();
                 for (int c = 0; c < nkb; ++c)
@@ -664,6 +700,18 @@ __device__ inline bool trailing_pipe(Pipe &P, int N, const CMat &cm, const ColMa
             }
         }
         __syncwarp();
+    } else if (warp == 2) {
+        // ---------------------------------------------- look-ahead inverse
+        if (lad) {
+            int ok = 1;
+            if (lane == 0) ok = tc::mbar_wait(P.laReady, P.nLA & 1u, WAIT_LIMIT) ? 1 : 0;
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            if (!ok) err = 1;
+            else {
+                const int r = invert_diag_warp(la.A, la.ld, la.k0, la.m, s);
+                if (lane == 0) *la.info = r;
+            }
+        }
     } else if (warp >= 4) {
         // ------------------------------------------------------ epilogue
         const int q4 = warp & 3, r = 32 * q4 + lane;
@@ -674,7 +722,8 @@ __device__ inline bool trailing_pipe(Pipe &P, int N, const CMat &cm, const ColMa
             if (!tc::mbar_wait(&P.fullC[cb], (ic / NCB) & 1u, WAIT_LIMIT)) err = 1;
             if (__any_sync(0xffffffffu, err)) { err = 1; break; }
             tc::fence_after_sync();
-            const int it = (t0 + t) / ntc, jt = (t0 + t) % ntc, i = it * TM + r;
+            const int tt = tile_of(t);
+            const int it = tt / ntc, jt = tt % ntc, i = it * TM + r;
             const bool rv = i < N;
             const int er = rv ? P.rexpW[i] : 0;
             float2 *cs = (float2 *)(P.sC + cb * CTILE);
@@ -710,9 +759,10 @@ __device__ inline bool trailing_pipe(Pipe &P, int N, const CMat &cm, const ColMa
         }
     }
     if (__syncthreads_or(err)) return false;
-    if (T > 0) P.nW += (uint32_t)((t1 - 1) / ntc - t0 / ntc + 1);
+    P.nW += nwl;
     P.nB += T;
     P.nT += T;
+    if (lad) P.nLA++;
     return true;
 }
 
@@ -742,7 +792,7 @@ __device__ int gj_invert(float2 *__restrict__ A, int N, int ld, const GjSmem &s,
     };
     // B tiles of the K rows [krow0, krow0 + nkr) for the columns of cmap, then
     // A(:, cols) += W B; every C tile of both CTAs is stored before it returns
-    auto update = [&](const ColMap &cmap, int krow0, int nkr) -> bool {
+    auto update = [&](const ColMap &cmap, int krow0, int nkr, const LookAhead &la) -> bool {
         const int ntc = cmap.ntc();
         const int2 cr = team_range(tm, ntc * PTN, 8);
         if (nkr > KB) convert_b<2>(P, A, ld, krow0, nkr, cmap, cr.x, cr.y, gc);
@@ -755,12 +805,15 @@ __device__ int gj_invert(float2 *__restrict__ A, int N, int ld, const GjSmem &s,
             for (int j = threadIdx.x; j < ntc * PTN; j += NT) P.cexpB[j] = __ldcg(gc + j);
         }
         const int2 tr = team_range(tm, ntr * ntc, 1);
-        const bool ok = trailing_pipe(P, N, cm, cmap, nkr > KB ? 2 : 1, tr.x, tr.y);
+        const bool ok = trailing_pipe(P, N, cm, cmap, nkr > KB ? 2 : 1, tr.x, tr.y, s, la);
         return !team_or(tm, !ok);
     };
     // 64-column panels once the working matrices of a wave no longer stay in
     // L2 (their rank-32 updates then stream from HBM); 32-column panels below
     const bool pairs = N > 256;
+    const LookAhead none{-1, nullptr, 0, 0, 0, nullptr};
+    int *la_info = tm.slot + 2;  // shared int after the team's two exchange slots
+    bool have_next = false;      // the next diagonal block was inverted during the last update
     int k0 = 0;
     while (k0 < N) {
         if (pairs && N - k0 >= 2 * KB) {
@@ -772,21 +825,38 @@ __device__ int gj_invert(float2 *__restrict__ A, int N, int ld, const GjSmem &s,
             const int k1 = k0 + KB;
             diag(k0, KB);
             panel_w(P, s, A, ld, N, k0, KB, rr.x, rr.y, gr);
-            if (!update(ColMap{0, 0, k1, KB}, k0, KB)) { *err = 1; return info; }
+            if (!update(ColMap{0, 0, k1, KB}, k0, KB, none)) { *err = 1; return info; }
             diag(k1, KB);
             panel_w(P, s, A, ld, N, k1, KB, rr.x, rr.y, gr);
-            if (!update(ColMap{0, 0, k0, KB}, k1, KB)) { *err = 1; return info; }
+            if (!update(ColMap{0, 0, k0, KB}, k1, KB, none)) { *err = 1; return info; }
             if (N > k0 + 2 * KB) {
                 panel_w64(P, A, ld, N, k0, rr.x, rr.y, gr);
-                if (!update(ColMap{k0, 2 * KB, -1, N - 2 * KB}, k0, 2 * KB)) { *err = 1; return info; }
+                if (!update(ColMap{k0, 2 * KB, -1, N - 2 * KB}, k0, 2 * KB, none)) { *err = 1; return info; }
             }
             k0 += 2 * KB;
         } else {
             const int nbt = min(KB, N - k0);
-            diag(k0, nbt);
+            if (have_next) {
+                // inverted during the previous update (s.sP, s.spr), its status in la_info
+                const int r = *la_info;
+                if (r && !info) info = k0 + r;
+                have_next = false;
+            } else {
+                diag(k0, nbt);
+            }
             panel_w(P, s, A, ld, N, k0, nbt, rr.x, rr.y, gr);
             if (nbt < N) {
-                if (!update(ColMap{k0, nbt, -1, N - nbt}, k0, nbt)) { *err = 1; return info; }
+                // one CTA per job: the next panel's diagonal block (rows and columns
+                // kn.., in row tile kn / TM and rest-column tile k0 / PTN) is
+                // inverted by warp 2 while this update runs
+                const int kn = k0 + nbt;
+                LookAhead la = none;
+                if (tm.n == 1 && kn < N) {
+                    const int ntc = (N - nbt + PTN - 1) / PTN;
+                    la = LookAhead{(kn / TM) * ntc + k0 / PTN, A, ld, kn, min(KB, N - kn), la_info};
+                }
+                if (!update(ColMap{k0, nbt, -1, N - nbt}, k0, nbt, la)) { *err = 1; return info; }
+                have_next = la.tile >= 0;
             } else {
                 team_sync(tm);
             }
@@ -874,7 +944,8 @@ __global__ void __launch_bounds__(NT, 1)
     int err = 0;
     float2 *A = work + (size_t)blockIdx.x * ld * N;
     const CMat cm{&tm, 0, (int)blockIdx.x};
-    Team team{0, 1, nullptr, nullptr, 0};
+    __shared__ int team_slots[4];
+    Team team{0, 1, nullptr, team_slots, 0};
     const int inf = gj_invert(A, N, ld, s, P, cm, &err, team);
     if (!err) {
         float2 *o = out + (size_t)blockIdx.x * N * N;
