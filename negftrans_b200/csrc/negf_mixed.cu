@@ -599,7 +599,25 @@ struct LookAhead {
     const float2 *A;
     int ld, k0, m;             // the block A(k0:k0+m, k0:k0+m)
     int *info;                 // shared: its zero-pivot step (1-based), 0 if none
+    int peer;                  // team of two: the other CTA's rank (it receives the result), else -1
 };
+
+// Copies P, the pivot lanes and the status of a diagonal-block inverse into
+// the same shared-memory places of CTA `peer` of the cluster (one warp).
+__device__ inline void send_diag(const GjSmem &s, int *info, int peer) {
+    const int lane = threadIdx.x & 31;
+    auto remote = [&](const void *p) -> uint32_t {
+        uint32_t r;
+        asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(r) : "r"(tc::smem_u32(p)), "r"(peer));
+        return r;
+    };
+    for (int e = lane; e < 32 * 32; e += 32) {
+        const float2 v = s.sP[e];
+        asm volatile("st.shared::cluster.v2.f32 [%0], {%1, %2};\n" ::"r"(remote(s.sP + e)), "f"(v.x), "f"(v.y) : "memory");
+    }
+    asm volatile("st.shared::cluster.s32 [%0], %1;\n" ::"r"(remote(s.spr + lane)), "r"(s.spr[lane]) : "memory");
+    if (lane == 0) asm volatile("st.shared::cluster.s32 [%0], %1;\n" ::"r"(remote(info)), "r"(*info) : "memory");
+}
 
 // A(:, cols) += W * B (N rows) with nkb K chunks (W and B tiles already in the CTA's
 // global scratch), pipelined (see above); the C tiles of matrix cm move by
@@ -710,6 +728,10 @@ __device__ inline bool trailing_pipe(Pipe &P, int N, const CMat &cm, const ColMa
             else {
                 const int r = invert_diag_warp(la.A, la.ld, la.k0, la.m, s);
                 if (lane == 0) *la.info = r;
+                __syncwarp();
+                // the team's other CTA gets the same inverse (visible after the
+                // cluster barrier that ends the update)
+                if (la.peer >= 0) send_diag(s, la.info, la.peer);
             }
         }
     } else if (warp >= 4) {
@@ -811,7 +833,8 @@ __device__ int gj_invert(float2 *__restrict__ A, int N, int ld, const GjSmem &s,
     // 64-column panels once the working matrices of a wave no longer stay in
     // L2 (their rank-32 updates then stream from HBM); 32-column panels below
     const bool pairs = N > 256;
-    const LookAhead none{-1, nullptr, 0, 0, 0, nullptr};
+    const LookAhead none{-1, nullptr, 0, 0, 0, nullptr, -1};
+    const int peer = tm.n > 1 ? 1 - tm.rank : -1;
     int *la_info = tm.slot + 2;  // shared int after the team's two exchange slots
     bool have_next = false;      // the next diagonal block was inverted during the last update
     int k0 = 0;
@@ -823,15 +846,31 @@ __device__ int gj_invert(float2 *__restrict__ A, int N, int ld, const GjSmem &s,
             // other column: half the passes over the working matrix of two
             // rank-32 updates, the same elimination.
             const int k1 = k0 + KB;
-            diag(k0, KB);
+            if (have_next) {
+                const int r = *la_info;
+                if (r && !info) info = k0 + r;
+                have_next = false;
+            } else {
+                diag(k0, KB);
+            }
             panel_w(P, s, A, ld, N, k0, KB, rr.x, rr.y, gr);
-            if (!update(ColMap{0, 0, k1, KB}, k0, KB, none)) { *err = 1; return info; }
-            diag(k1, KB);
+            // the update of K2's columns first finishes K2's diagonal block (row
+            // tile k1 / TM of its one column tile), inverted while the rest runs
+            const LookAhead la1{k1 / TM, A, ld, k1, KB, la_info, peer};
+            if (!update(ColMap{0, 0, k1, KB}, k0, KB, la1)) { *err = 1; return info; }
+            {
+                const int r = *la_info;
+                if (r && !info) info = k1 + r;
+            }
             panel_w(P, s, A, ld, N, k1, KB, rr.x, rr.y, gr);
             if (!update(ColMap{0, 0, k0, KB}, k1, KB, none)) { *err = 1; return info; }
             if (N > k0 + 2 * KB) {
                 panel_w64(P, A, ld, N, k0, rr.x, rr.y, gr);
-                if (!update(ColMap{k0, 2 * KB, -1, N - 2 * KB}, k0, 2 * KB, none)) { *err = 1; return info; }
+                // the next panel's diagonal block: row tile kn / TM, rest-column tile k0 / PTN
+                const int kn = k0 + 2 * KB, ntc = (N - 2 * KB + PTN - 1) / PTN;
+                const LookAhead la2{(kn / TM) * ntc + k0 / PTN, A, ld, kn, min(KB, N - kn), la_info, peer};
+                if (!update(ColMap{k0, 2 * KB, -1, N - 2 * KB}, k0, 2 * KB, la2)) { *err = 1; return info; }
+                have_next = true;
             }
             k0 += 2 * KB;
         } else {
@@ -846,14 +885,14 @@ __device__ int gj_invert(float2 *__restrict__ A, int N, int ld, const GjSmem &s,
             }
             panel_w(P, s, A, ld, N, k0, nbt, rr.x, rr.y, gr);
             if (nbt < N) {
-                // one CTA per job: the next panel's diagonal block (rows and columns
-                // kn.., in row tile kn / TM and rest-column tile k0 / PTN) is
-                // inverted by warp 2 while this update runs
+                // the next panel's diagonal block (rows and columns kn.., in row tile
+                // kn / TM and rest-column tile k0 / PTN) is inverted by warp 2 of the
+                // CTA that updates that tile while this update runs
                 const int kn = k0 + nbt;
                 LookAhead la = none;
-                if (tm.n == 1 && kn < N) {
+                if (kn < N) {
                     const int ntc = (N - nbt + PTN - 1) / PTN;
-                    la = LookAhead{(kn / TM) * ntc + k0 / PTN, A, ld, kn, min(KB, N - kn), la_info};
+                    la = LookAhead{(kn / TM) * ntc + k0 / PTN, A, ld, kn, min(KB, N - kn), la_info, peer};
                 }
                 if (!update(ColMap{k0, nbt, -1, N - nbt}, k0, nbt, la)) { *err = 1; return info; }
                 have_next = la.tile >= 0;
