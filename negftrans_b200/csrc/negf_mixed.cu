@@ -1355,14 +1355,17 @@ struct PassSmem {
     unsigned char *stB;   // PB x (ncap * 256)
     int *cexp;            // [ncap] column exponents of the current product's v
     unsigned *cmax;       // [ncap] column maxima (float bits) of the next product's v
+    unsigned *cmaxPeer;   // [2][ncap] the team's other CTA's maxima, by exchange parity
     uint64_t *fullA, *emptyA, *fullB, *emptyB, *accFull, *accEmpty, *bReady;
+    uint64_t *maxReady;   // the other CTA's maxima have arrived
+    uint64_t *convReady;  // the other CTA has converted its chunks of the next v
     uint32_t *tslot;
     double *red;          // [2 * NWARP]
 };
-constexpr int PASS_BARS = 2 * PA_MAX + 2 * PB + 2 + 2 + 1;
+constexpr int PASS_BARS = 2 * PA_MAX + 2 * PB + 2 + 2 + 1 + 2;
 __host__ __device__ inline size_t pass_smem_bytes(int N, int ncap, int pa) {
     size_t b = pa * TILE_BYTES + PB * (size_t)ncap * 256;
-    b += 2 * (size_t)ncap * 4 + PASS_BARS * 8 + 16 + 2 * NWARP * 8;
+    b += 4 * (size_t)ncap * 4 + PASS_BARS * 8 + 16 + 2 * NWARP * 8;
     (void)N;
     return (b + 127) / 128 * 128;
 }
@@ -1374,12 +1377,15 @@ __device__ inline PassSmem carve_pass(unsigned char *base, int ncap, int pa) {
     p.stB = q; q += PB * (size_t)ncap * 256;
     p.cexp = (int *)q; q += (size_t)ncap * 4;
     p.cmax = (unsigned *)q; q += (size_t)ncap * 4;
+    p.cmaxPeer = (unsigned *)q; q += 2 * (size_t)ncap * 4;
     q = (unsigned char *)(((uintptr_t)q + 15) & ~(uintptr_t)15);
     uint64_t *bar = (uint64_t *)q;
     p.fullA = bar; p.emptyA = bar + PA_MAX;
     p.fullB = bar + 2 * PA_MAX; p.emptyB = p.fullB + PB;
     p.accFull = p.emptyB + PB; p.accEmpty = p.accFull + 2;
     p.bReady = p.accEmpty + 2;
+    p.maxReady = p.bReady + 1;
+    p.convReady = p.maxReady + 1;
     q += PASS_BARS * 8;
     p.tslot = (uint32_t *)q; q += 16;
     p.red = (double *)q;
@@ -1472,13 +1478,37 @@ __device__ inline Prod pass_prod(int mode, int s, int Nz, size_t sl, float2 *x, 
     return q;
 }
 
+// Arrival on the barrier at the same shared-memory place of CTA `peer` of the
+// cluster, releasing this thread's (and, through the barrier before it, its
+// warps') earlier writes at cluster scope.
+__device__ __forceinline__ void mbar_arrive_peer(uint64_t *bar, int peer) {
+    uint32_t ra;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(ra) : "r"(tc::smem_u32(bar)), "r"(peer));
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];\n" ::"r"(ra) : "memory");
+}
+// mbar_wait with acquire at cluster scope (the arrival came from the other CTA)
+__device__ __forceinline__ bool mbar_wait_cluster(uint64_t *bar, uint32_t parity, uint32_t limit) {
+    const uint32_t a = tc::smem_u32(bar);
+    for (uint32_t it = 0; it < limit; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
+            " selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
 // The epilogue warps' conversion of v = v1 - v2 into the split-fp16 B chunks
 // (chunk kc at kc * npad * 256 B of bscr, planes of npad * KB fp16), one
 // exponent per column.  First, if cmax is null, the column maxima by a pass
 // over v; else the maxima the previous epilogue accumulated in cmax.
 __device__ inline void pass_convert(const MixedLayout &L, const PassSmem &p, const float2 *__restrict__ v1,
                                     const float2 *__restrict__ v2, int nopen, int npad, unsigned char *bscr,
-                                    bool from_cmax) {
+                                    bool from_cmax, int kc0, int kc1) {
     const int N = L.N, et = threadIdx.x - 128, ew = et >> 5, lane = et & 31;
     if (!from_cmax) {
         for (int j = ew; j < npad; j += 4) {
@@ -1498,14 +1528,14 @@ __device__ inline void pass_convert(const MixedLayout &L, const PassSmem &p, con
     epi_bar();
     for (int j = et; j < npad; j += 128) p.cmax[j] = 0u;
     const uint32_t bplane = npad * KB * 2;
-    const int nitem = L.nkc * npad * 4;
+    const int nitem = (kc1 - kc0) * npad * 4;  // this CTA's chunks [kc0, kc1)
     // two items per thread per round: all 32 loads in flight before the first use
     for (int i0 = et; i0 < nitem; i0 += 256) {
         float2 x1[2][8], x2[2][8];
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int item = i0 + 128 * h;
-            const int g4 = item & 3, j = (item >> 2) % npad, kc = (item >> 2) / npad;
+            const int g4 = item & 3, j = (item >> 2) % npad, kc = kc0 + (item >> 2) / npad;
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
                 const int k = kc * KB + 8 * g4 + q;
@@ -1518,7 +1548,7 @@ __device__ inline void pass_convert(const MixedLayout &L, const PassSmem &p, con
         for (int h = 0; h < 2; ++h) {
             const int item = i0 + 128 * h;
             if (item >= nitem) break;
-            const int g4 = item & 3, j = (item >> 2) % npad, kc = (item >> 2) / npad;
+            const int g4 = item & 3, j = (item >> 2) % npad, kc = kc0 + (item >> 2) / npad;
             const float sc = tc::exp2i(-p.cexp[j]);
             __align__(16) __half rh[8], rl[8], ih[8], il[8];
 #pragma unroll
@@ -1541,7 +1571,14 @@ __device__ inline void pass_convert(const MixedLayout &L, const PassSmem &p, con
 
 // Pipeline counters of the roles, carried across the jobs of a CTA.
 struct PassCnt {
-    uint32_t a, b, u, r;  // A stages, B stages, accumulators, products
+    uint32_t a, b, u, r, x;  // A stages, B stages, accumulators, products, maxima exchanges
+};
+// The row tiles [rt0, rt1) a CTA computes; with a team of two (peer >= 0)
+// the other CTA computes the rest, and per product the two exchange their
+// column maxima (DSMEM) and convert the K chunks of their own rows of the
+// next vector into the job's shared B scratch.
+struct PassPart {
+    int rt0, rt1, kc0, kc1, peer;
 };
 
 // All products of one pass of one job through the warp-specialised pipeline:
@@ -1563,9 +1600,10 @@ struct PassCnt {
 // Returns false if a wait timed out (uniform over the CTA).
 __device__ bool pass_run(const MixedLayout &L, const PassSmem &p, unsigned char *jm, unsigned char *bscr, int mode,
                          float2 *x, float2 *rc, float2 *d, float2 *xa, int nopen, int npad, uint32_t tbase,
-                         PassCnt &cnt) {
+                         PassCnt &cnt, const PassPart &pt) {
     const int N = L.N, Nz = L.Nz, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nprod = pass_nprod(mode, Nz), ntr = L.ntr, nkc = L.nkc;
+    const int nrt = pt.rt1 - pt.rt0;  // this CTA's row tiles
     const size_t sl = (size_t)L.ncap * N;
     const uint32_t bbytes = (uint32_t)npad * 256, bst = (uint32_t)L.ncap * 256;
     int err = 0;
@@ -1576,10 +1614,10 @@ __device__ bool pass_run(const MixedLayout &L, const PassSmem &p, unsigned char 
             for (int s = 0; s < nprod && !err; ++s) {
                 const Prod q = pass_prod(mode, s, Nz, sl, x, rc, d, xa);
                 const unsigned char *tiles = jm + L.off_tiles + (size_t)q.slot * L.mat_bytes;
-                for (int t = 0; t < ntr * nkc && !err; ++t, ++ia) {
+                for (int t = 0; t < nrt * nkc && !err; ++t, ++ia) {
                     const uint32_t st = ia % (uint32_t)p.pa;
                     if (ia >= (uint32_t)p.pa && !tc::mbar_wait(&p.emptyA[st], ((ia / p.pa) - 1) & 1u, WAIT_LIMIT)) { err = 1; break; }
-                    const int rt = t / nkc, kc = t % nkc;
+                    const int rt = pt.rt0 + t / nkc, kc = t % nkc;
                     const unsigned char *src = tiles + factor_tile_off(L, rt, kc);
                     if (rt < ntr - 1) {
                         mbar_expect_tx(&p.fullA[st], (uint32_t)TILE_BYTES);
@@ -1602,7 +1640,9 @@ __device__ bool pass_run(const MixedLayout &L, const PassSmem &p, unsigned char 
             uint32_t ib = cnt.b;
             for (int s = 0; s < nprod && !err; ++s) {
                 if (!tc::mbar_wait(p.bReady, (cnt.r + s) & 1u, WAIT_LIMIT)) { err = 1; break; }
-                for (int t = 0; t < ntr * nkc && !err; ++t, ++ib) {
+                // ... and the other CTA's chunks of the same vector
+                if (pt.peer >= 0 && !mbar_wait_cluster(p.convReady, (cnt.r + s) & 1u, WAIT_LIMIT)) { err = 1; break; }
+                for (int t = 0; t < nrt * nkc && !err; ++t, ++ib) {
                     const uint32_t st = ib % PB;
                     if (ib >= PB && !tc::mbar_wait(&p.emptyB[st], ((ib / PB) - 1) & 1u, WAIT_LIMIT)) { err = 1; break; }
                     mbar_expect_tx(&p.fullB[st], bbytes);
@@ -1616,7 +1656,7 @@ __device__ bool pass_run(const MixedLayout &L, const PassSmem &p, unsigned char 
         if (lane == 0) {
             uint32_t ia = cnt.a, ib = cnt.b, iu = cnt.u;
             for (int s = 0; s < nprod && !err; ++s) {
-                for (int rt = 0; rt < ntr && !err; ++rt, ++iu) {
+                for (int rt = pt.rt0; rt < pt.rt1 && !err; ++rt, ++iu) {
                     const uint32_t buf = iu & 1u, dacc = tbase + buf * (2 * L.ncap);
                     if (iu >= 2 && !tc::mbar_wait(&p.accEmpty[buf], ((iu >> 1) - 1) & 1u, WAIT_LIMIT)) { err = 1; break; }
                     for (int kc = 0; kc < nkc; ++kc, ++ia, ++ib) {
@@ -1640,13 +1680,16 @@ __device__ bool pass_run(const MixedLayout &L, const PassSmem &p, unsigned char 
         uint32_t iu = cnt.u;
         {
             const Prod q0 = pass_prod(mode, 0, Nz, sl, x, rc, d, xa);
-            pass_convert(L, p, q0.v1, q0.v2, nopen, npad, bscr, false);
-            if (tid == 128) mbar_arrive(p.bReady);
+            pass_convert(L, p, q0.v1, q0.v2, nopen, npad, bscr, false, pt.kc0, pt.kc1);
+            if (tid == 128) {
+                mbar_arrive(p.bReady);
+                if (pt.peer >= 0) mbar_arrive_peer(p.convReady, pt.peer);
+            }
         }
         for (int s = 0; s < nprod && !err; ++s) {
             const Prod q = pass_prod(mode, s, Nz, sl, x, rc, d, xa);
             const int *rexp_g = (const int *)(jm + L.off_rexp) + (size_t)q.slot * N;
-            for (int rt = 0; rt < ntr; ++rt, ++iu) {
+            for (int rt = pt.rt0; rt < pt.rt1; ++rt, ++iu) {
                 const uint32_t buf = iu & 1u, dacc = tbase + lb + buf * (2 * L.ncap);
                 const int r = 32 * q4 + lane, i = rt * TM + r;
                 const bool rv = i < N;
@@ -1694,17 +1737,37 @@ __device__ bool pass_run(const MixedLayout &L, const PassSmem &p, unsigned char 
             if (err) break;
             if (s + 1 < nprod) {
                 epi_bar();  // every store of y and every column maximum of this product
+                if (pt.peer >= 0) {
+                    // column maxima of the next v over both CTAs' rows
+                    const int et = tid - 128;
+                    const uint32_t px = cnt.x + (uint32_t)s;
+                    unsigned *dst = p.cmaxPeer + (px & 1u) * L.ncap;
+                    for (int j = et; j < npad; j += 128) {
+                        uint32_t ra;
+                        asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(ra) : "r"(tc::smem_u32(dst + j)), "r"(pt.peer));
+                        asm volatile("st.shared::cluster.u32 [%0], %1;\n" ::"r"(ra), "r"(p.cmax[j]) : "memory");
+                    }
+                    epi_bar();
+                    if (tid == 128) mbar_arrive_peer(p.maxReady, pt.peer);
+                    if (epi_any(!mbar_wait_cluster(p.maxReady, px & 1u, WAIT_LIMIT))) { err = 1; break; }
+                    for (int j = et; j < npad; j += 128) p.cmax[j] = max(p.cmax[j], dst[j]);
+                    epi_bar();
+                }
                 const Prod qn = pass_prod(mode, s + 1, Nz, sl, x, rc, d, xa);
-                pass_convert(L, p, qn.v1, qn.v2, nopen, npad, bscr, true);
-                if (tid == 128) mbar_arrive(p.bReady);
+                pass_convert(L, p, qn.v1, qn.v2, nopen, npad, bscr, true, pt.kc0, pt.kc1);
+                if (tid == 128) {
+                    mbar_arrive(p.bReady);
+                    if (pt.peer >= 0) mbar_arrive_peer(p.convReady, pt.peer);
+                }
             }
         }
     }
     if (__syncthreads_or(err)) return false;
-    cnt.a += (uint32_t)(nprod * ntr * nkc);
-    cnt.b += (uint32_t)(nprod * ntr * nkc);
-    cnt.u += (uint32_t)(nprod * ntr);
+    cnt.a += (uint32_t)(nprod * nrt * nkc);
+    cnt.b += (uint32_t)(nprod * nrt * nkc);
+    cnt.u += (uint32_t)(nprod * nrt);
     cnt.r += (uint32_t)nprod;
+    cnt.x += (uint32_t)(nprod - 1);
     return true;
 }
 
@@ -1728,16 +1791,27 @@ __global__ void __launch_bounds__(NT, 1) k_mixed_pass(MixedArgs a, int mode, int
         for (int s = 0; s < PB; ++s) { tc::mbar_init(&p.fullB[s], 1); tc::mbar_init(&p.emptyB[s], 1); }
         for (int s = 0; s < 2; ++s) { tc::mbar_init(&p.accFull[s], 1); tc::mbar_init(&p.accEmpty[s], 4); }
         tc::mbar_init(p.bReady, 1);
+        tc::mbar_init(p.maxReady, 1);
+        tc::mbar_init(p.convReady, 1);
     }
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
+    // a.cpj CTAs (one cluster) per job, as in the sweep: each computes its share
+    // of the row tiles of every product
+    const int cpj = a.cpj, rank = (int)(blockIdx.x % cpj), slot = (int)(blockIdx.x / cpj);
+    const int nslot = (int)(gridDim.x / cpj);
+    if (cpj > 1) cluster_sync();  // both CTAs' barriers exist before either arrives on the other's
+    __shared__ int ok_slots[2];
+    Team team{rank, cpj, nullptr, ok_slots, 0u};
+    const int rt0 = L.ntr * rank / cpj, rt1 = L.ntr * (rank + 1) / cpj;
+    const PassPart pt{rt0, rt1, min(L.nkc, rt0 * (TM / KB)), min(L.nkc, rt1 * (TM / KB)), cpj > 1 ? 1 - rank : -1};
     const uint32_t tbase = *p.tslot;
-    PassCnt cnt{0, 0, 0, 0};
-    unsigned char *bscr = a.scratch + (size_t)blockIdx.x * L.scratch_bytes;
+    PassCnt cnt{0, 0, 0, 0, 0};
+    unsigned char *bscr = a.scratch + (size_t)slot * L.scratch_bytes;
     const size_t sl = (size_t)L.ncap * N;  // float2 per slice of a vector array
     bool ok = true;
-    for (int w = blockIdx.x; w < a.njobs && ok; w += gridDim.x) {
+    for (int w = slot; w < a.njobs && ok; w += nslot) {
         if (a.status[w] != 0) continue;
         unsigned char *jm = a.jobmem + (size_t)w * L.job_bytes;
         const int nopen = ((const int *)(jm + L.off_oc))[L.ncap];
@@ -1746,8 +1820,11 @@ __global__ void __launch_bounds__(NT, 1) k_mixed_pass(MixedArgs a, int mode, int
         // unless this is the last iteration, CORR folds d into x(b) for b < Nz-1
         // on the way (the last slice is kept so that tau is formed from x + d in FP64)
         ok = pass_run(L, p, jm, bscr, mode, x, rc, d, (mode == PASS_CORR && !last) ? x : nullptr, nopen, npad,
-                      tbase, cnt);
-        if (mode == PASS_CORR) {
+                      tbase, cnt, pt);
+        // the same outcome in both CTAs of a team; the barrier also makes each
+        // CTA's rows of the vectors visible to the other
+        if (cpj > 1) ok = !team_or(team, !ok);
+        if (mode == PASS_CORR && rank == 0) {
             if (ok) {
                 // tau of x0 + d at the last slice, FP64
                 const negf::Geo &g = a.g;
@@ -1816,11 +1893,13 @@ __global__ void __launch_bounds__(NT, 1) k_mixed_pass(MixedArgs a, int mode, int
                 __syncthreads();
             }
         }
-        if (!ok && tid == 0) a.status[w] = -2;
+        if (!ok && tid == 0 && rank == 0) a.status[w] = -2;
     }
     tc::fence_before_sync();
     __syncthreads();
     if (tid < 32) tc::tmem_dealloc(tbase, ncols);
+    // no CTA leaves while the other may still write its shared memory
+    if (cpj > 1) cluster_sync();
 }
 
 // FP64 residual of the block-tridiagonal system for x0, one CTA per (job,
@@ -2082,6 +2161,23 @@ double kinetic(const negf_ctx *c, int ik, int i) {
     return (ax * ax + ay * ay) / 2;
 }
 
+// k_mixed_pass on nw jobs of cpj CTAs each (a cluster per job)
+cudaError_t launch_pass(const MixedArgs &a, int nw, int cpj, size_t smem, cudaStream_t st, int mode, int it, int last) {
+    cudaLaunchConfig_t lc = {};
+    cudaLaunchAttribute la[1];
+    la[0].id = cudaLaunchAttributeClusterDimension;
+    la[0].val.clusterDim.x = cpj;
+    la[0].val.clusterDim.y = 1;
+    la[0].val.clusterDim.z = 1;
+    lc.gridDim = dim3(nw * cpj);
+    lc.blockDim = dim3(NT);
+    lc.dynamicSmemBytes = smem;
+    lc.stream = st;
+    lc.attrs = la;
+    lc.numAttrs = 1;
+    return cudaLaunchKernelEx(&lc, k_mixed_pass, a, mode, it, last);
+}
+
 template <typename K>
 int set_smem(K kern, size_t bytes) {
     CKM(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
@@ -2173,9 +2269,10 @@ int negf_internal_mixed(negf_ctx *c, const double *h_E, const double *d_E, int n
         // a basis whose sweep state does not fit one SM's shared memory (about
         // N > 900) runs in FP64 like a job that does not fit device memory
         // the deepest factor ring of the passes that shared memory allows
+        // (1 KB kept for the pass kernel's static shared memory)
         int pa = PA_MAX;
-        while (pa > PA_MIN && pass_smem_bytes(N, ncap, pa) > (size_t)smem_optin) --pa;
-        if (sm_sweep > (size_t)smem_optin || pass_smem_bytes(N, ncap, pa) > (size_t)smem_optin) W = 0;
+        while (pa > PA_MIN && pass_smem_bytes(N, ncap, pa) + 1024 > (size_t)smem_optin) --pa;
+        if (sm_sweep > (size_t)smem_optin || pass_smem_bytes(N, ncap, pa) + 1024 > (size_t)smem_optin) W = 0;
         if (cpj == 2 && W >= 1) {
             CKM(cudaFuncSetAttribute(k_mixed_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_sweep));
             cudaLaunchConfig_t qc = {};
@@ -2262,17 +2359,14 @@ int negf_internal_mixed(negf_ctx *c, const double *h_E, const double *d_E, int n
                     lc.numAttrs = 1;
                     CKM(cudaLaunchKernelEx(&lc, k_mixed_sweep, a, tmC));
                 }
-                k_mixed_pass<<<nw, NT, sm_pass, st>>>(a, PASS_X0, 0, 0);
-                CKM(cudaGetLastError());
+                CKM(launch_pass(a, nw, cpj, sm_pass, st, PASS_X0, 0, 0));
                 // refinement steps; converged jobs (MIX_DONE) are skipped by the next ones
                 for (int it = 1; it <= pol.max_refinements; ++it) {
                     const int last = it == pol.max_refinements;
                     k_mixed_residual<<<dim3(nw, Nz), NT, sm_res, st>>>(a);
                     CKM(cudaGetLastError());
-                    k_mixed_pass<<<nw, NT, sm_pass, st>>>(a, PASS_BACK, it, last);
-                    CKM(cudaGetLastError());
-                    k_mixed_pass<<<nw, NT, sm_pass, st>>>(a, PASS_CORR, it, last);
-                    CKM(cudaGetLastError());
+                    CKM(launch_pass(a, nw, cpj, sm_pass, st, PASS_BACK, it, last));
+                    CKM(launch_pass(a, nw, cpj, sm_pass, st, PASS_CORR, it, last));
                 }
                 CKM(cudaEventRecord(c->ev1, st));
                 CKM(cudaMemcpyAsync(tau.data(), a.tau, sizeof(double) * nw, cudaMemcpyDeviceToHost, st));
