@@ -81,7 +81,7 @@ typedef struct negf_mixed_policy {
                               * contraction (|d_1| / |x| after one step, |d_k| / |d_k-1|
                               * after more).  Default 1e-7.                             */
     int32_t max_refinements; /* refinement steps before a job that has not met the
-                              * tolerance is re-run in FP64 (1..8, default 5)           */
+                              * tolerance is re-run in FP64 (1..16, default 8)          */
     int32_t ctas_per_job;    /* CTAs that sweep one job: 1, 2 (a thread-block cluster
                               * on two SMs), or 0 = automatic (2 when one CTA per job
                               * would leave at least half of the SMs idle, e.g. when

@@ -29,7 +29,7 @@ struct negf_ctx {
     int *d_info = nullptr;
     int cap_E = 0, cap_jobs = 0;
     // mixed-precision path
-    negf_mixed_policy mixed_policy{0.0, 0.0, 1e-7, 5, 0};
+    negf_mixed_policy mixed_policy{0.0, 0.0, 1e-7, 8, 0};
     negf_mixed_stats mixed_stats{};
     void *d_mixed = nullptr;  // per-wave factor storage and scratch
     size_t mixed_bytes = 0;

@@ -1373,7 +1373,7 @@ int negf_internal_fp64_jobs(negf_ctx *c, const double *d_E, const int *ie, const
 
 extern "C" int negf_set_mixed_policy(negf_ctx *c, const negf_mixed_policy *p) {
     if (!c || !p || !(p->threshold_window >= 0) || !(p->eta_fp64_below >= 0) || !(p->tau_tolerance > 0) ||
-        p->max_refinements < 1 || p->max_refinements > 8 || p->ctas_per_job < 0 || p->ctas_per_job > 2)
+        p->max_refinements < 1 || p->max_refinements > 16 || p->ctas_per_job < 0 || p->ctas_per_job > 2)
         return NEGF_ERR_ARG;
     c->mixed_policy = *p;
     return NEGF_OK;

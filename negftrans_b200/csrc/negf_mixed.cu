@@ -1876,7 +1876,10 @@ __global__ void __launch_bounds__(NT, 1) k_mixed_pass(MixedArgs a, int mode, int
                     // remaining error after this correction: |d_k| times the contraction,
                     // estimated as |d_1| / |x| after the first step and |d_k| / |d_k-1| later
                     const double dn = a.dnorm[w], xnv = sqrt(X);
-                    const double corr = xnv > 0 ? dn / xnv : INFINITY;
+                    // no trace term (no open channel of the left lead, e.g. E at the
+                    // band bottom): tau = 0 exactly, whatever the solution; an exactly
+                    // zero solution with a zero correction has converged as well
+                    const double corr = xnv > 0 ? dn / xnv : (dn > 0 ? INFINITY : 0.0);
                     const double rho = iter == 1 ? corr : (a.dprev[w] > 0 ? dn / a.dprev[w] : INFINITY);
                     const double est = 2.0 * fmax(a.tau[w], 1.0) * corr * rho;
                     a.dprev[w] = dn;

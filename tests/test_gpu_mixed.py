@@ -193,3 +193,25 @@ def test_mixed_one_and_two_ctas_per_job(name, nz, ne):
             assert np.max(np.abs(tau - ref)) <= TOL_MIXED, (cpj, np.abs(tau - ref), st)
             out[cpj] = tau
     assert np.max(np.abs(out[1] - out[2])) <= TOL_MIXED
+
+
+def test_mixed_accepts_energies_without_a_trace_term():
+    """At the band bottom (E = 0, flat leads at V = 0) no channel of the left
+    lead is open, so every gamma_L vanishes and tau is exactly 0 (grid.f90:355-383)
+    whatever G_{Nz,1} holds.  The mixed path accepts such a job at once instead of
+    sending it to an FP64 re-run."""
+    from negftrans_b200 import prepare as P
+    from negftrans_b200._lib import NEGF_MIXED
+    from negftrans_b200.negf import Engine
+    w, pr = _prepared("qpc_n69", nz=40)
+    grid = P.transmission_energies(pr.atomic, w.n_energy)
+    E = np.ascontiguousarray(np.concatenate([[0.0], grid[1::64]]))
+    ref = _oracle(pr, E)
+    assert ref[0] == 0.0
+    with Engine(*pr.engine_args()) as eng:
+        tau, info = eng.transmission(E, precision=NEGF_MIXED)
+        st = eng.mixed_stats()
+    assert info == 0
+    assert tau[0] == 0.0
+    assert st["n_fp64_rejected"] == 0 and st["n_mixed"] == len(E), st
+    assert np.max(np.abs(tau - ref)) <= TOL_MIXED
