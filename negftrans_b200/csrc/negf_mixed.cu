@@ -2382,7 +2382,7 @@ int negf_internal_mixed(negf_ctx *c, const double *h_E, const double *d_E, int n
                 mixed_ms += ms;
                 for (int w = 0; w < nw; ++w) {
                     const int q = m_jobs[w0 + w];
-                    const double corr = xn[w] > 0 ? dn[w] / xn[w] : INFINITY;
+                    const double corr = xn[w] > 0 ? dn[w] / xn[w] : (dn[w] > 0 ? INFINITY : 0.0);
                     if (status[w] == MIX_DONE) {
                         h_tau_jobs[q] = tau[w];
                         h_info[q] = 0;
