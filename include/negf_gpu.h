@@ -164,18 +164,21 @@ int negf_transmission(negf_ctx *ctx, const double *energies, int32_t nE, int32_t
 
 /* The NEGF_MIXED path of negf_transmission / negf_transmission_device.
  * Per job: the Schur complements D_k - gR(k) are formed in FP64 and rounded
- * to complex FP32; their inverses use FP32 Gauss-Jordan panels with partial
- * pivoting and rank-32 trailing updates on the tcgen05 tensor cores in split
- * fp16 (FP32 accumulation); every generator is kept in device memory.  Then
- * one refinement step on the open channels of the right lead: x0 = first
- * block column of G from the stored factors, the residual of the whole
- * block-tridiagonal system in FP64, the correction d from the stored
- * factors, and tau (grid.f90:362-383) from x0 + d in FP64.  Jobs rejected by
- * the check of negf_mixed_policy, and jobs the policy sends to FP64, are
- * re-run by the FP64 path; tau and stats then cover all jobs.  Jobs are
- * processed in waves sized to the free device memory (about 8 N^2 N_z bytes
- * per job).  negf_transmission_device with NEGF_MIXED synchronises `stream`
- * once per wave (to schedule the re-runs).  N <= 1023. */
+ * to complex FP32.  Their inverses use FP32 Gauss-Jordan with pivoting inside
+ * each 32 x 32 diagonal block, and trailing updates (rank 32, or rank 64
+ * above N = 256) on the tcgen05 tensor cores in split fp16 with FP32
+ * accumulation.  Every generator is kept in device memory.  Then refinement
+ * steps on the open channels of the right lead: x0 = first block column of G
+ * from the stored factors; the residual of the whole block-tridiagonal system
+ * in FP64; the correction d from the stored factors; tau (grid.f90:362-383)
+ * from x0 + d in FP64.  Jobs rejected by the check of negf_mixed_policy, and
+ * jobs the policy sends to FP64, are re-run by the FP64 path, so tau and
+ * stats cover all jobs.  Jobs are processed in waves sized to the free device
+ * memory (about 7 N^2 N_z bytes per job), one SM per job or, when that would
+ * leave half of the SMs idle, a two-SM cluster per job.  With NEGF_MIXED,
+ * negf_transmission_device synchronises `stream` once per wave, to schedule
+ * the re-runs.  N <= 1023; bases whose sweep state does not fit one SM's
+ * shared memory (about N > 890) run in FP64. */
 int negf_set_mixed_policy(negf_ctx *ctx, const negf_mixed_policy *policy);
 int negf_get_mixed_policy(const negf_ctx *ctx, negf_mixed_policy *policy);
 int negf_get_mixed_stats(const negf_ctx *ctx, negf_mixed_stats *stats);
