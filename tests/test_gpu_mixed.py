@@ -215,3 +215,37 @@ def test_mixed_accepts_energies_without_a_trace_term():
     assert tau[0] == 0.0
     assert st["n_fp64_rejected"] == 0 and st["n_mixed"] == len(E), st
     assert np.max(np.abs(tau - ref)) <= TOL_MIXED
+
+
+def test_mixed_device_entry_matches_host_entry():
+    """negf_transmission_device with NEGF_MIXED on device buffers and the
+    caller's stream gives the host entry's tau bit for bit (the mixed path is
+    deterministic: fixed-order reductions, order-free column maxima), and the
+    per-job tau in k-major order sums to it with the k weights."""
+    import torch
+    from negftrans_b200 import prepare as P
+    from negftrans_b200._lib import NEGF_MIXED
+    from negftrans_b200.negf import Engine
+    w, pr = _prepared("small:1.2:16")
+    E = P.transmission_energies(pr.atomic, 16)
+    nE = len(E)
+    kpt = np.asarray(pr.kpoint, np.float64).reshape(-1, 3)
+    nk = len(kpt)
+    dev = torch.device("cuda", 0)
+    d_E = torch.from_numpy(np.ascontiguousarray(E)).to(dev)
+    d_tau = torch.full((nE,), float("nan"), dtype=torch.float64, device=dev)
+    d_tj = torch.full((nk * nE,), float("nan"), dtype=torch.float64, device=dev)
+    d_info = torch.full((nk * nE,), -7, dtype=torch.int32, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    with Engine(*pr.engine_args()) as eng:
+        tau_host, info_host = eng.transmission(E, precision=NEGF_MIXED)
+        eng.transmission_device(d_E.data_ptr(), nE, d_tau.data_ptr(), d_tj.data_ptr(), d_info.data_ptr(),
+                                stream.cuda_stream, precision=NEGF_MIXED)
+        stream.synchronize()
+    assert info_host == 0
+    np.testing.assert_array_equal(d_tau.cpu().numpy(), tau_host)
+    assert (d_info.cpu().numpy() == 0).all()
+    tj = d_tj.cpu().numpy().reshape(nk, nE)
+    np.testing.assert_allclose(kpt[:, 2] @ tj, tau_host, rtol=1e-14, atol=1e-15)
+    ref = _oracle(pr, E)
+    assert np.max(np.abs(tau_host - ref)) <= TOL_MIXED
